@@ -1,0 +1,186 @@
+"""ctypes mirror of include/epp.h (the C ABI of libepp.so).
+
+Every struct and constant here has the same name, field order and meaning as in the header;
+the header cites the reference interface each entry point replaces.
+"""
+import ctypes as C
+
+EPP_ABI_VERSION = 1
+EPP_MAX_TAGS = 16
+
+# epp_status
+EPP_OK = 0
+EPP_ERR_INVALID_ARGUMENT = 1
+EPP_ERR_CUDA = 2
+EPP_ERR_OUT_OF_MEMORY = 3
+EPP_ERR_UNSUPPORTED_ACTION = 4
+EPP_ERR_UNSUPPORTED_CRITERION = 5
+EPP_ERR_STATE = 6
+EPP_ERR_DEVICE_STATUS = 7
+EPP_ERR_BUDGET = 8
+EPP_ERR_NO_DEVICE = 9
+EPP_ERR_CAPACITY = 10
+
+STATUS_NAMES = {
+    EPP_OK: "EPP_OK",
+    EPP_ERR_INVALID_ARGUMENT: "EPP_ERR_INVALID_ARGUMENT",
+    EPP_ERR_CUDA: "EPP_ERR_CUDA",
+    EPP_ERR_OUT_OF_MEMORY: "EPP_ERR_OUT_OF_MEMORY",
+    EPP_ERR_UNSUPPORTED_ACTION: "EPP_ERR_UNSUPPORTED_ACTION",
+    EPP_ERR_UNSUPPORTED_CRITERION: "EPP_ERR_UNSUPPORTED_CRITERION",
+    EPP_ERR_STATE: "EPP_ERR_STATE",
+    EPP_ERR_DEVICE_STATUS: "EPP_ERR_DEVICE_STATUS",
+    EPP_ERR_BUDGET: "EPP_ERR_BUDGET",
+    EPP_ERR_NO_DEVICE: "EPP_ERR_NO_DEVICE",
+    EPP_ERR_CAPACITY: "EPP_ERR_CAPACITY",
+}
+
+# device status bits
+EPP_STATUS_KILLED = 1 << 0
+EPP_STATUS_NEIGHBOUR_OVERFLOW = 1 << 1
+EPP_STATUS_CELL_OVERFLOW = 1 << 2
+EPP_STATUS_NONFINITE = 1 << 3
+EPP_STATUS_SPIN_TIMEOUT = 1 << 4
+EPP_STATUS_BAD_TAG = 1 << 5
+EPP_STATUS_QUEUE = 1 << 6
+
+EPP_CRITERION_DEFAULT = 0
+EPP_CRITERION_SYMMETRY = 1
+
+EPP_ACTION_NONE = 0
+EPP_ACTION_DAMBREAK_CONTINUITY = 1
+EPP_ACTION_DAMBREAK_DENSITY = 2
+EPP_ACTION_DAMBREAK_MOMENTUM = 3
+EPP_ACTION_DAMBREAK_INTEGRATE = 4
+EPP_ACTION_ZERO_DVELOCITY = 5
+EPP_ACTION_COUNT_NEIGHBOURS = 6
+
+EPP_SEARCH_EMIT_LIST = 1
+
+EPP_VISCOSITY_REFERENCE = 0
+EPP_VISCOSITY_MONAGHAN = 1
+
+
+class epp_domain(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32),
+        ("gap", C.c_float),
+        ("first", C.c_float * 3),
+        ("last", C.c_float * 3),
+    ]
+
+
+class epp_physics(C.Structure):
+    _fields_ = [
+        ("dt", C.c_float),
+        ("rho0", C.c_float),
+        ("c0", C.c_float),
+        ("p0", C.c_float),
+        ("gamma", C.c_int32),
+        ("gravity", C.c_float * 3),
+        ("alpha", C.c_float),
+        ("beta", C.c_float),
+        ("viscosity", C.c_int32),
+        ("fluid_tag", C.c_int32),
+        ("wall_tag", C.c_int32),
+        ("kahan", C.c_int32),
+    ]
+
+
+class epp_config(C.Structure):
+    _fields_ = [
+        ("domain", epp_domain),
+        ("n_capacity", C.c_int32),
+        ("max_neighbour_number", C.c_int32),
+        ("max_cell_particles", C.c_int32),
+        ("n_tags", C.c_int32),
+        ("adjacency", C.c_int32 * (EPP_MAX_TAGS * EPP_MAX_TAGS)),
+        ("device", C.c_int32),
+        ("hbm_budget_bytes", C.c_int64),
+    ]
+
+
+_COLUMN_FIELDS = [
+    "tag", "is_movable", "n_count", "n_index",
+    "position", "velocity", "dvelocity", "mass", "volume", "density", "ddensity", "pressure",
+    "gap", "h", "n_rvec", "n_r", "n_w", "n_dw", "n_hinv",
+]
+
+
+class epp_column_map(C.Structure):
+    _fields_ = [(f, C.c_int32) for f in _COLUMN_FIELDS]
+
+    @classmethod
+    def empty(cls):
+        m = cls()
+        for f in _COLUMN_FIELDS:
+            setattr(m, f, -1)
+        return m
+
+
+class epp_integrals(C.Structure):
+    _fields_ = [
+        ("mass_total", C.c_double),
+        ("mass_fluid", C.c_double),
+        ("kinetic", C.c_double),
+        ("potential", C.c_double),
+        ("internal", C.c_double),
+        ("max_speed", C.c_double),
+        ("cfl_dt", C.c_double),
+        ("n_alive", C.c_int64),
+        ("n_pairs", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+def make_domain(dim, gap, first, last):
+    d = epp_domain()
+    d.dim = dim
+    d.gap = gap
+    for a in range(3):
+        d.first[a] = first[a] if a < len(first) else 0.0
+        d.last[a] = last[a] if a < len(last) else 0.0
+    return d
+
+
+def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81, 0.0),
+                 alpha=0.1, beta=0.1, viscosity=EPP_VISCOSITY_REFERENCE, fluid_tag=1,
+                 wall_tag=2, kahan=1):
+    p = epp_physics()
+    p.dt = dt
+    p.rho0 = rho0
+    p.c0 = c0
+    p.p0 = p0
+    p.gamma = gamma
+    for a in range(3):
+        p.gravity[a] = gravity[a] if a < len(gravity) else 0.0
+    p.alpha = alpha
+    p.beta = beta
+    p.viscosity = viscosity
+    p.fluid_tag = fluid_tag
+    p.wall_tag = wall_tag
+    p.kahan = kahan
+    return p
+
+
+def make_config(domain, n_capacity, adjacency, max_neighbour_number=50, max_cell_particles=0,
+                device=0, hbm_budget_bytes=0):
+    c = epp_config()
+    c.domain = domain
+    c.n_capacity = n_capacity
+    c.max_neighbour_number = max_neighbour_number
+    c.max_cell_particles = max_cell_particles
+    n_tags = len(adjacency)
+    if n_tags < 1 or n_tags > EPP_MAX_TAGS:
+        raise ValueError("adjacency must be 1..%d square" % EPP_MAX_TAGS)
+    c.n_tags = n_tags
+    for i in range(n_tags):
+        if len(adjacency[i]) != n_tags:
+            raise ValueError("adjacency must be square")
+        for j in range(n_tags):
+            c.adjacency[i * EPP_MAX_TAGS + j] = int(adjacency[i][j])
+    c.device = device
+    c.hbm_budget_bytes = hbm_budget_bytes
+    return c

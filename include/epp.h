@@ -1,0 +1,192 @@
+/*
+ * epp.h -- C ABI of libepp.so, the B200 (sm_100a) SPH time-step backend for
+ * EtherParallelParticles.jl.
+ *
+ * The reference reaches its device through three Julia entry points that take a
+ * particle system, a domain, a neighbour system and a user closure:
+ *   Algorithm.search!       src/Algorithm/NeighbourSearch.jl:323-347 (static_search! :349-377)
+ *   Algorithm.interaction!  src/Algorithm/Action.jl:140-152 (static_interaction! :154-181)
+ *   Algorithm.selfaction!   src/Algorithm/Action.jl:53-67 (static_selfaction! :69-93)
+ * plus the host<->device mirror Class.syncto!/asyncto!
+ *   src/Class/ParticleSystem/ParticleSystem.jl:275-307, ParticleSystemBase.jl:33-50.
+ * Closures cannot cross a C ABI, so the actions are named bundles (EPP_ACTION_*)
+ * and the search criteria are named (EPP_CRITERION_*).  The property matrices keep
+ * the reference's layout: column-major, leading dimension = capacity, one column per
+ * scalar (vectors take dim consecutive columns), 1-based particle and cell ids.
+ *
+ * Conventions: every function returns an epp_status (0 = EPP_OK).  Nothing throws,
+ * aborts or traps.  Errors detected on the device set bits of a status word that
+ * epp_synchronize returns.  A context is not thread-safe; use one per host thread.
+ * All work is queued on the context's own CUDA stream; host buffers are borrowed
+ * only for the duration of the call.  The library owns all device memory.
+ */
+#ifndef EPP_H
+#define EPP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EPP_ABI_VERSION 1
+#define EPP_MAX_TAGS 16
+
+typedef enum epp_status {
+    EPP_OK = 0,
+    EPP_ERR_INVALID_ARGUMENT = 1,
+    EPP_ERR_CUDA = 2,
+    EPP_ERR_OUT_OF_MEMORY = 3,
+    EPP_ERR_UNSUPPORTED_ACTION = 4,
+    EPP_ERR_UNSUPPORTED_CRITERION = 5,
+    EPP_ERR_STATE = 6,          /* call order: e.g. interaction! before any search! */
+    EPP_ERR_DEVICE_STATUS = 7,  /* a device-side check failed; see the status word */
+    EPP_ERR_BUDGET = 8,         /* HBM budget of the context or server exceeded */
+    EPP_ERR_NO_DEVICE = 9,
+    EPP_ERR_CAPACITY = 10       /* more particles than the context's capacity */
+} epp_status;
+
+/* Bits of the device status word (accumulated until read by epp_synchronize). */
+#define EPP_STATUS_KILLED             (1u << 0) /* particles left the domain (info, as reference) */
+#define EPP_STATUS_NEIGHBOUR_OVERFLOW (1u << 1) /* a list exceeded max_neighbour_number */
+#define EPP_STATUS_CELL_OVERFLOW      (1u << 2) /* a cell exceeded max_cell_particles */
+#define EPP_STATUS_NONFINITE          (1u << 3) /* NaN/Inf in density or velocity */
+#define EPP_STATUS_SPIN_TIMEOUT       (1u << 4) /* a bounded device wait gave up */
+#define EPP_STATUS_BAD_TAG            (1u << 5) /* tag outside 1..n_tags */
+#define EPP_STATUS_QUEUE              (1u << 6) /* persistent work queue inconsistency */
+
+/* Search criteria: src/Algorithm/NeighbourSearch.jl:141-164 */
+#define EPP_CRITERION_DEFAULT  0 /* dr^2 <= gap^2                       (:141-151) */
+#define EPP_CRITERION_SYMMETRY 1 /* dr^2 <= (2 harmonic(h_i, h_j))^2    (:153-164) */
+
+/* Named actions.  The dam-break bundle restates example/collapse_dry/same/main.jl:74-126
+ * with the physics substitutions of the benchmark cases (Wendland C2, Tait EOS,
+ * artificial viscosity, symplectic Euler). */
+#define EPP_ACTION_NONE                  0 /* defaultSelfaction!  Action.jl:27-35 */
+#define EPP_ACTION_DAMBREAK_CONTINUITY   1 /* search! action: kernel cache + continuity  main.jl:74-90 */
+#define EPP_ACTION_DAMBREAK_DENSITY      2 /* selfaction!: rho += drho dt, V = m/rho, p = eos  main.jl:92-105 */
+#define EPP_ACTION_DAMBREAK_MOMENTUM     3 /* interaction!: pressure + artificial viscosity  main.jl:107-118 */
+#define EPP_ACTION_DAMBREAK_INTEGRATE    4 /* selfaction!: gravity, sAccelerate!, sMove!  main.jl:120-126 */
+#define EPP_ACTION_ZERO_DVELOCITY        5 /* selfaction!: dVelocity = 0 (test helper, ActionTest.jl:66-69) */
+#define EPP_ACTION_COUNT_NEIGHBOURS      6 /* interaction!: dVelocity += 1 per neighbour (ActionTest.jl:71-75) */
+
+/* epp_search flags */
+#define EPP_SEARCH_EMIT_LIST 1 /* keep per-particle neighbour lists for epp_download */
+
+/* Artificial-viscosity forms */
+#define EPP_VISCOSITY_REFERENCE 0 /* Viscosity.jl:28-52 as written: extra 1/(rho_i rho_j) */
+#define EPP_VISCOSITY_MONAGHAN  1 /* textbook Monaghan: divide by the mean density only */
+
+typedef struct epp_domain {
+    int32_t dim;      /* 2 (Domain2D, src/Class/Domain/Domain2D.jl:28-67) or 3 (new) */
+    float gap;        /* cell size; the reference uses 2h */
+    float first[3];   /* lower corner */
+    float last[3];    /* upper corner */
+} epp_domain;
+
+typedef struct epp_physics {
+    float dt;             /* time step (fixed, as the reference: main.jl:68) */
+    float rho0;           /* reference density */
+    float c0;             /* speed of sound */
+    float p0;             /* background pressure added by the EOS */
+    int32_t gamma;        /* Tait exponent, integer (7) */
+    float gravity[3];
+    float alpha;          /* artificial viscosity alpha (Viscosity.jl:36) */
+    float beta;           /* artificial viscosity beta (reference default 0.1, Viscosity.jl:37) */
+    int32_t viscosity;    /* EPP_VISCOSITY_* */
+    int32_t fluid_tag;    /* 1 in the reference example */
+    int32_t wall_tag;     /* 2 in the reference example */
+    int32_t kahan;        /* 1: compensated (Kahan) position update; 0: sMove! as written */
+} epp_physics;
+
+typedef struct epp_config {
+    epp_domain domain;
+    int32_t n_capacity;            /* rows of the property matrices */
+    int32_t max_neighbour_number;  /* list capacity for EPP_SEARCH_EMIT_LIST (reference: 50) */
+    int32_t max_cell_particles;    /* reference bucket capacity; only checked (0 = unchecked) */
+    int32_t n_tags;                /* adjacency matrix is n_tags x n_tags, tags are 1-based */
+    int32_t adjacency[EPP_MAX_TAGS * EPP_MAX_TAGS]; /* row-major [tag_i-1][tag_j-1] */
+    int32_t device;                /* CUDA ordinal */
+    int64_t hbm_budget_bytes;      /* 0 = unlimited; creation fails with EPP_ERR_BUDGET above it */
+} epp_config;
+
+/* 0-based column indices into the caller's property matrices; -1 = absent.
+ * Vector properties occupy dim consecutive columns starting at the index. */
+typedef struct epp_column_map {
+    /* int_properties_ */
+    int32_t tag, is_movable, n_count, n_index;
+    /* float_properties_ */
+    int32_t position, velocity, dvelocity, mass, volume, density, ddensity, pressure, gap, h;
+    int32_t n_rvec, n_r, n_w, n_dw, n_hinv;
+} epp_column_map;
+
+typedef struct epp_integrals {
+    double mass_total;      /* sum m over alive particles */
+    double mass_fluid;      /* sum m over alive fluid particles */
+    double kinetic;         /* sum 1/2 m |v|^2 (fluid) */
+    double potential;       /* sum -m g.x (fluid) */
+    double internal;        /* sum m e(rho), Tait internal energy (fluid) */
+    double max_speed;       /* max |v| (fluid) */
+    double cfl_dt;          /* 0.1 h_min / (c0 + max|v|) -- the CFL bound of the step */
+    int64_t n_alive;
+    int64_t n_pairs;        /* directed active neighbour pairs of the last search */
+} epp_integrals;
+
+typedef struct epp_ctx epp_ctx;
+
+/* Library */
+int32_t epp_abi_version(void);
+int32_t epp_device_count(int32_t* count);
+
+/* Context lifetime */
+int32_t epp_create(const epp_config* config, epp_ctx** out);
+int32_t epp_destroy(epp_ctx* ctx);
+const char* epp_last_error(const epp_ctx* ctx);
+
+/* Host <-> device in the reference layout (Class.asyncto!, ParticleSystem.jl:292-307).
+ * int_props / float_props are column-major with leading dimension ld_int / ld_float.
+ * is_alive and cell_index are the base_.is_alive_ / base_.cell_index_ vectors (cell ids
+ * 1-based, 0 = not binned).  Download writes only mapped columns; neighbour columns are
+ * written when the last search used EPP_SEARCH_EMIT_LIST. */
+int32_t epp_upload(epp_ctx* ctx, int32_t n_particles, const int32_t* is_alive,
+                   const int32_t* cell_index, const int32_t* int_props, int64_t ld_int,
+                   const float* float_props, int64_t ld_float, const epp_column_map* map);
+int32_t epp_download(epp_ctx* ctx, int32_t* is_alive, int32_t* cell_index, int32_t* int_props,
+                     int64_t ld_int, float* float_props, int64_t ld_float,
+                     const epp_column_map* map);
+
+/* Algorithm layer.  Each call is asynchronous on the context stream.
+ *   epp_search      replaces Algorithm.search!       (NeighbourSearch.jl:323-347)
+ *   epp_interaction replaces Algorithm.interaction!  (Action.jl:140-152)
+ *   epp_selfaction  replaces Algorithm.selfaction!   (Action.jl:53-67) */
+int32_t epp_search(epp_ctx* ctx, int32_t criterion, int32_t action, const epp_physics* phys,
+                   int32_t flags);
+int32_t epp_interaction(epp_ctx* ctx, int32_t action, const epp_physics* phys);
+int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys);
+
+/* The whole dam-break time step of main.jl:166-182 (density update, momentum,
+ * integrate, search + continuity), fused into 5 kernels and replayed as a CUDA graph.
+ * Requires one prior epp_search with EPP_ACTION_DAMBREAK_CONTINUITY (main.jl:157-164). */
+int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys);
+
+/* FP64 reductions of the current state. */
+int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out);
+
+/* Parity access to the cell list: counts[n_cells] per cell, offsets[n_cells+1] exclusive
+ * scan, sorted_ids[n_alive] 1-based particle ids in cell order (within a cell by id).
+ * Any pointer may be NULL. */
+int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t* sorted_ids,
+                       int32_t* n_cells);
+
+/* Waits for the context stream; returns EPP_ERR_DEVICE_STATUS when a device check failed
+ * (bits in *device_status, which is then cleared). device_status may be NULL. */
+int32_t epp_synchronize(epp_ctx* ctx, uint32_t* device_status);
+
+/* Per-stage device times of the last epp_step call (ms, CUDA events); n <= 8. */
+int32_t epp_last_step_timing(epp_ctx* ctx, float* ms_total);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EPP_H */

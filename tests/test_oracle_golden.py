@@ -1,0 +1,134 @@
+"""The CPU oracle against the reference's own known-answer tests (read from its test files into
+tests/golden/reference_kat.json by tests/golden/make_golden.py)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from epp import abi
+from epp.classes import ActivePair, Domain2D, NeighbourSystem, ParticleSystem
+from helpers import config_for, kat, neighbour_sets, nine_particle_system
+from oracle_lib import Oracle, load
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_domain_kat(precision):
+    """test/Class/DomainTest.jl:16-39"""
+    k = kat()["domain"]
+    lib = load()
+    d = abi.make_domain(2, k["gap"], k["first"], k["last"])
+    n = (C.c_int32 * 3)()
+    lib.orc_domain_info(C.byref(d), precision, n, None, None)
+    assert (n[0], n[1]) == (k["n_x"], k["n_y"])
+    cart = (C.c_int32 * 3)()
+    lin = C.c_int32()
+    ins = C.c_int32()
+    x = (C.c_float * 3)(k["point"][0], k["point"][1], 0.0)
+    lib.orc_cell_of(C.byref(d), precision, x, cart, C.byref(lin), C.byref(ins))
+    assert (cart[0], cart[1]) == tuple(k["cartesian"])
+    assert lin.value == k["linear"]
+    assert ins.value == 1
+
+
+def test_domain_host_mirror_kat():
+    """The host Domain2D mirror reproduces test/Class/DomainTest.jl:16-39."""
+    k = kat()["domain"]
+    d = Domain2D(k["gap"], k["first"][0], k["first"][1], k["last"][0], k["last"][1])
+    assert (d.get_n_x(), d.get_n_y(), d.get_n()) == (k["n_x"], k["n_y"], k["n_x"] * k["n_y"])
+    assert d.indexCartesianFromPosition(*k["point"]) == tuple(k["cartesian"])
+    assert d.indexLinearFromPosition(*k["point"]) == k["linear"]
+    assert d.indexCartesianToLinear(*k["to_linear"]["ij"]) == k["to_linear"]["value"]
+    assert d.indexLinearToCartesian(k["to_linear"]["value"]) == tuple(k["to_linear"]["ij"])
+    assert d.inside(*k["point"])
+    assert d.get_gap_x() == pytest.approx((k["last"][0] - k["first"][0]) / k["n_x"], rel=1e-6)
+
+
+def test_neighbour_cell_table_kat():
+    """test/Class/NeighbourSystem/NeighbourSystemBaseTest.jl:10-25"""
+    k = kat()["neighbour_cells"]
+    lib = load()
+    d = abi.make_domain(2, k["domain"]["gap"], k["domain"]["first"], k["domain"]["last"])
+    n = len(k["counts"])
+    counts = np.zeros(n, np.int32)
+    lists = np.zeros(n * 9, np.int32)
+    lib.orc_neighbour_cell_table(C.byref(d), counts.ctypes.data_as(C.POINTER(C.c_int32)),
+                                 lists.ctypes.data_as(C.POINTER(C.c_int32)))
+    assert counts.tolist() == k["counts"]
+    assert [n, 9] == k["list_shape"]
+    # host mirror
+    dom = Domain2D(k["domain"]["gap"], *k["domain"]["first"], *k["domain"]["last"])
+    ns = NeighbourSystem(dom, [(1, 1), (1, 2), (2, 1)])
+    assert ns.neighbour_cell_counts().tolist() == k["counts"]
+
+
+def test_active_pair_kat():
+    """test/Class/NeighbourSystem/ActivePairTest.jl:10-19 and NeighbourSystemTest.jl:32-36"""
+    for case in kat()["adjacency"]:
+        ap = ActivePair([tuple(p) for p in case["pairs"]])
+        assert ap.adjacency_matrix.tolist() == case["matrix"]
+
+
+def test_column_offsets_kat():
+    """test/Class/ParticleSystem/ParticleSystemTest.jl:86-93"""
+    k = kat()["columns"]
+    dim, nb = k["dim"], k["neighbour_count"]
+    ev = lambda s: eval(s, {"dim": dim, "neighbour_count": nb})  # noqa: E731 (arithmetic only)
+    ints = {name: ev(v) for name, v in k["int_named_tuple"]}
+    floats = {name: ev(v) for name, v in k["float_named_tuple"]}
+    dom = Domain2D(0.15, 0.1, 0.2, 0.9, 0.9)
+    ps = ParticleSystem(dom, 100, ints, floats, {"c_0": 340.0}, capacityExpand=lambda n: n + 100)
+    for key in ["Tag", "IsMovable", "nCount", "nIndex", "nR", "PositionVec", "nRVec"]:
+        assert ps.basic_index[key] == k[key], key
+    assert ps.get_n_capacity() == 200
+    assert ps.get_n_int_capacity() == 1 + 1 + 1 + nb
+
+
+def _nine_oracle(precision):
+    ps, ns, k = nine_particle_system()
+    cfg = config_for(ps, ns)
+    o = Oracle(cfg, precision)
+    cmap = ps.column_map()
+    o.upload(ps.n_particles, ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, cmap)
+    return o, ps, ns, k, cmap
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_neighbour_search_kat(precision):
+    """test/Algorithm/NeighbourSearchTest.jl:67-152: nCount and the neighbour sets."""
+    o, ps, ns, k, cmap = _nine_oracle(precision)
+    o.search(abi.EPP_CRITERION_DEFAULT, abi.EPP_ACTION_NONE)
+    o.search(abi.EPP_CRITERION_DEFAULT, abi.EPP_ACTION_NONE)  # search! then dynamic_search!
+    o.download(ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, cmap)
+    assert ps["nCount"].tolist() == k["ncount"]
+    assert neighbour_sets(ps) == k["neighbour_sets"]
+    assert o.status() == 0
+
+
+def test_action_kat():
+    """test/Algorithm/ActionTest.jl:60-85: zero a vector, add 1 per neighbour -> nCount."""
+    o, ps, ns, k, cmap = _nine_oracle(32)
+    o.search(abi.EPP_CRITERION_DEFAULT, abi.EPP_ACTION_NONE)
+    for _ in range(2):  # static then dynamic variants in the reference
+        o.selfaction(abi.EPP_ACTION_ZERO_DVELOCITY)
+        o.interaction(abi.EPP_ACTION_COUNT_NEIGHBOURS)
+    o.download(ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, cmap)
+    dv = ps["dVelocityVec"]
+    assert dv[:, 0].tolist() == kat()["action"]["counts"]
+    assert dv[:, 1].tolist() == kat()["action"]["counts"]
+
+
+def test_cell_stats_nine():
+    """Counts per cell and the sorted membership of the 9-particle case."""
+    o, ps, ns, k, cmap = _nine_oracle(32)
+    o.search(abi.EPP_CRITERION_DEFAULT, abi.EPP_ACTION_NONE)
+    counts, offsets, ids = o.cell_stats(9)
+    assert counts.sum() == 9
+    assert offsets[-1] == 9
+    # particles 1,2,4,5 are in cell 1; 3,6 in cell 2; 7,8 in cell 6; 9 in cell 7 (5 x 4 grid)
+    dom = ps.domain
+    expect = {}
+    for i, (x, y) in enumerate(k["positions"], 1):
+        expect.setdefault(dom.indexLinearFromPosition(x, y), []).append(i)
+    for c, members in expect.items():
+        s, e = offsets[c - 1], offsets[c]
+        assert ids[s:e].tolist() == sorted(members)
