@@ -1,0 +1,346 @@
+"""Benchmark of the SPH time step (pair-interactions/s) on B200.
+
+Default workload (N=1): the 2D dam break at dx = 0.002 m -- 500,000 fluid particles plus the
+3-layer walls (15,018 particles), cell gap 2h, re-sorted every step, Wendland C2, Tait EOS,
+artificial viscosity, symplectic Euler with Kahan positions.  A step is one full time step of
+example/collapse_dry/same/main.jl:166-182 (density update, momentum, integrate, search +
+continuity).  The metric counts the directed active neighbour pairs of each step's search once.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl epp|reference] [--case 2d|3d|2d-small]
+
+N > 1 (torchrun): the plain path does not shard, so every rank runs an independent replica
+("replicas only"), no collective on the data path; value = pairs of all ranks / max time.
+
+--impl reference times the CPU restatement of the reference algorithm (the oracle: stored
+neighbour lists, bucket cell list, one pass per reference launch) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "etherparallelparticles.jl_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import numpy as np  # noqa: E402
+
+# Algorithmic bytes per particle per step (FP32 state, Int32 ids, compulsory traffic of a fused
+# design with neighbours served on chip, counted once).
+B_ALG_STEP = {2: 189.0, 3: 245.0}
+B_ALG_MOMENTUM = {2: 64.0, 3: 88.0}   # dominant kernel: momentum + integrate + bin
+STAGES = ["momentum_integrate_bin", "scan", "scatter", "rank_gather", "search_continuity"]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="epp", choices=["epp", "reference"])
+    ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small"])
+    ap.add_argument("--no-flush", action="store_true")
+    return ap.parse_args()
+
+
+def make_case(name):
+    from epp import casegen
+    if name == "2d":
+        return casegen.dam_break_2d(dx=0.002, max_neighbour_number=1), "2D dam break dx=0.002 (500k fluid)"
+    if name == "2d-small":
+        return casegen.dam_break_2d(dx=0.02, max_neighbour_number=1), "2D dam break dx=0.02 (5k fluid)"
+    return casegen.dam_break_3d(dx=0.005, max_neighbour_number=1), "3D dam break dx=0.005 (4.8M fluid)"
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(case, steps_budget_s=20.0, max_steps=3):
+    """The oracle (C++ restatement of the reference's CPU algorithm) on all host cores."""
+    from epp import abi
+    from epp.classes import NeighbourSystem
+    from epp import casegen
+    import oracle_lib
+    ps, phys = case.ps, case.physics
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=40 if case.meta["dim"] == 2 else 100)
+    cfg = abi.make_config(case.domain.to_abi(), ps.n_capacity, ns.active_pair.adjacency_matrix.tolist(),
+                          max_neighbour_number=ns.max_neighbour_number, max_cell_particles=64 if case.meta["dim"] == 2 else 128)
+    threads = os.cpu_count() or 1
+    oracle_lib.set_threads(threads)
+    o = oracle_lib.Oracle(cfg, 32)
+    o.lib.orc_set_deterministic(o.h, 0)   # threaded atomic insert, as the reference's CPU backend
+    cm = ps.column_map()
+    o.upload(ps.n_particles, ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, cm)
+    o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys)
+    pairs, t_total, steps = 0, 0.0, 0
+    while steps < max_steps and (steps == 0 or t_total < steps_budget_s):
+        t0 = time.perf_counter()
+        o.step(1, phys)
+        t_total += time.perf_counter() - t0
+        pairs += int(o.field(9, 0, ps.n_particles).sum())
+        steps += 1
+    return {"value": pairs / t_total, "unit": "pair-interactions/s", "cores": threads, "kind": "port",
+            "sample": "%d full steps of %s (%d particles), %.2f s" % (steps, case.meta.get("label", ""), ps.n_particles, t_total),
+            "seconds_per_step": t_total / steps}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement on the host cores, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    case, label = make_case(args.case)
+    case.meta["label"] = label
+    probe = cpu_reference(case, steps_budget_s=0.0, max_steps=1)      # cost of one step
+    k = max(1, min(args.steps, int(120.0 / max(probe["seconds_per_step"], 1e-3))))
+    res = cpu_reference(case, steps_budget_s=150.0, max_steps=k)
+    val = res["value"]
+    out = {"metric": "SPH pair-interactions/s", "value": val, "unit": "pair-interactions/s",
+           "impl": "reference", "n_gpus": args.gpus, "steps": k, "warmup": 1,
+           "ms_per_step": res["seconds_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (dam-break lattice generated in-process)",
+           "config": {"workload": label, "particles": case.n},
+           "cpu_baseline": {"value": val, "unit": "pair-interactions/s", "cores": res["cores"],
+                            "kind": "port", "sample": res["sample"]},
+           "e2e": {"value": val, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from epp import abi, casegen
+    from epp.algorithm import DeviceParticleSystem
+    from epp.classes import NeighbourSystem
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    case, label = make_case(args.case)
+    case.meta["label"] = label
+    ps, phys = case.ps, case.physics
+    dim = case.meta["dim"]
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    dps = DeviceParticleSystem(ps, ns, device=local)
+    ctx = dps.ctx
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    dps.syncto()
+    ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    ctx.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(stream):
+        ctx.step(max(args.warmup, 3), phys)
+    ctx.synchronize()
+    clocks = Clocks(local)
+    # ---- timed region: K steps, L2 flushed before each, device time by CUDA events ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    p0 = ctx.pairs_total()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            if not args.no_flush:
+                flush.fill_(float(k))
+            starts[k].record(stream)
+            ctx.step(1, phys)
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    st = ctx.synchronize(raise_on_status=False)
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    pairs = ctx.pairs_total() - p0
+    if world > 1:
+        t = torch.tensor([ms, float(pairs)], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms_max, pairs_all = float(tmax[0]), float(t[1])
+    else:
+        ms_max, pairs_all = ms, float(pairs)
+    value = pairs_all / (ms_max / 1e3)
+
+    # ---- per-kernel device times (instrumented step on the same state, same stream) ----
+    with torch.cuda.stream(stream):
+        stage = np.zeros(5)
+        nprof = 5
+        for _ in range(nprof):
+            if not args.no_flush:
+                flush.fill_(1.0)
+            stage += np.array(ctx.profile_step(phys))
+        stage /= nprof
+    dom_k = int(np.argmax(stage))
+    n = case.n
+    b_mom = B_ALG_MOMENTUM[dim] * n
+    achieved = b_mom / (stage[0] * 1e-3) / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            tr = json.load(f).get(args.case, {}).get("k_momentum_fused")
+            if tr:
+                traffic = tr["bytes_per_launch"]
+    except Exception:
+        pass
+
+    # ---- end to end through the C ABI with host buffers (pinned) ----
+    e2e = run_e2e(dps, case, args, stream)
+
+    integ = ctx.integrals(phys)
+    if rank == 0:
+        step_bytes = B_ALG_STEP[dim] * n
+        out = {
+            "metric": "SPH pair-interactions/s",
+            "value": value,
+            "unit": "pair-interactions/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (dam-break lattice generated in-process, hydrostatic density)",
+            "config": {"workload": label, "particles": n, "fluid": case.meta["n_fluid"],
+                       "walls": case.meta["n_wall"], "cells": case.meta["n_cells"],
+                       "pairs_per_step": pairs_all / args.steps / world, "resort": "every step",
+                       "l2": "flushed (256 MB write) before every timed step" if not args.no_flush else "not flushed",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "step_hbm_gbs_algorithmic": step_bytes / (ms_max / args.steps * 1e-3) / 1e9},
+            "gpu_launches": 5 * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "k_momentum_fused", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback",
+                         "algorithmic_bytes_per_particle": B_ALG_MOMENTUM[dim],
+                         "stage_ms": dict(zip(STAGES, [round(x, 5) for x in stage])),
+                         "dominant_stage": STAGES[dom_k]},
+            "clocks": clk,
+            "e2e": e2e,
+            "device_status": st,
+            "integrals": {k: integ[k] for k in ("mass_total", "kinetic", "potential", "internal", "max_speed")},
+        }
+        if world == 1:
+            try:
+                cb = cpu_reference(case, steps_budget_s=20.0, max_steps=2)
+                out["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            except Exception as exc:  # reported, not fatal
+                out["cpu_baseline"] = {"value": None, "error": str(exc)}
+        print(json.dumps(out))
+    dps.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(dps, case, args, stream):
+    """Same metric through the public C ABI with host (pinned) buffers: upload of the reference-
+    layout matrices, K x (epp_step + FP64 integrals read back), download; host wall clock."""
+    import torch
+    ps = dps.host
+    ctx = dps.ctx
+    phys = case.physics
+    ip = torch.from_numpy(np.asfortranarray(ps.int_properties)).pin_memory().numpy()
+    fp = torch.from_numpy(np.asfortranarray(ps.float_properties)).pin_memory().numpy()
+    ip = np.asfortranarray(ip)
+    fp = np.asfortranarray(fp)
+    alive = torch.from_numpy(ps.is_alive.copy()).pin_memory().numpy()
+    cell = torch.from_numpy(ps.cell_index.copy()).pin_memory().numpy()
+    # download once so the host matrices hold the current state, then time a full run
+    ctx.download(alive, cell, ip, fp, dps.cmap)
+    K = args.steps
+    p0 = ctx.pairs_total()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.upload(ps.n_particles, alive, cell, ip, fp, dps.cmap)
+    ctx.search(1, 1, phys, 0)
+    for _ in range(K):
+        ctx.step(1, phys)
+        ctx.integrals(phys)
+    ctx.download(alive, cell, ip, fp, dps.cmap)
+    t1 = time.perf_counter()
+    pairs = ctx.pairs_total() - p0
+    cm = dps.cmap
+    ncols_f = sum(w for c, w in [(cm.position, case.meta["dim"]), (cm.velocity, case.meta["dim"]),
+                                 (cm.dvelocity, case.meta["dim"]), (cm.mass, 1), (cm.volume, 1), (cm.density, 1),
+                                 (cm.ddensity, 1), (cm.pressure, 1), (cm.h, 1)] if c >= 0)
+    ncols_i = 2 + sum(1 for c in (cm.tag, cm.is_movable, cm.n_count) if c >= 0)
+    n = ps.n_particles
+    h2d = (n * 4 * (ncols_f + ncols_i)) / K + 64
+    d2h = (n * 4 * (ncols_f + ncols_i)) / K + 72
+    return {"value": pairs / (t1 - t0), "unit": "pair-interactions/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "seconds": t1 - t0,
+            "note": "upload + initial search + K x (step + integrals readback) + download, host clock"}
+
+
+if __name__ == "__main__":
+    main()

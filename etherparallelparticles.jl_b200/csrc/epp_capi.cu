@@ -1,0 +1,957 @@
+// epp_capi.cu -- the C ABI of libepp.so (include/epp.h): context, device arena, reference-layout
+// upload/download, the search! / interaction! / selfaction! entry points and the fused,
+// graph-captured dam-break step.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "epp_self.cuh"
+
+using namespace epp;
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kIntegralBlocks = 592;   // 4 x 148 SMs
+
+inline int blocks_for(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
+
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, off = 0;
+    template <class T>
+    T* take(size_t count) {
+        size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+        if (off + bytes > size) return nullptr;
+        T* p = reinterpret_cast<T*>(base + off);
+        off += bytes;
+        return p;
+    }
+};
+
+DevPhys to_dev(const epp_physics& p) {
+    DevPhys d;
+    d.dt = p.dt;
+    d.rho0 = p.rho0;
+    d.c0 = p.c0;
+    d.p0 = p.p0;
+    d.B = (float)((double)p.rho0 * (double)p.c0 * (double)p.c0 / (double)p.gamma);
+    for (int a = 0; a < 3; ++a) d.g[a] = p.gravity[a];
+    d.alpha = p.alpha;
+    d.beta = p.beta;
+    d.gamma = p.gamma;
+    d.visc = p.viscosity;
+    d.fluid = p.fluid_tag;
+    d.wall = p.wall_tag;
+    d.kahan = p.kahan;
+    return d;
+}
+
+bool same_phys(const epp_physics& a, const epp_physics& b) { return std::memcmp(&a, &b, sizeof a) == 0; }
+
+}  // namespace
+
+struct epp_ctx {
+    epp_config cfg{};
+    int D = 2;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    DevDomain dom{};
+    int n = 0;        // particles uploaded (rows)
+    int cap = 0;
+    int n_cells = 0;
+    int n_tiles = 0;
+    Arena arena;
+    State S[2]{};
+    int* start[2]{};
+    int cur = 0;
+    FusedOut tmp{};       // xh/vm/comp of the fused momentum pass
+    int* count = nullptr;
+    int2* cs = nullptr;
+    int2* perm = nullptr;
+    unsigned long long* scan_state = nullptr;
+    unsigned* status = nullptr;
+    unsigned long long* pairs = nullptr;
+    int* ncount = nullptr;
+    float* stage_f = nullptr;
+    int* stage_i = nullptr;
+    double* ipartial = nullptr;
+    double* iresult = nullptr;
+    unsigned* iticket = nullptr;
+    double* ihpart = nullptr;
+    double* ihmin = nullptr;
+    float4* accel = nullptr;   // optional dv/dt output of the fused momentum pass
+    // lazily allocated neighbour lists (EPP_SEARCH_EMIT_LIST)
+    NeighbourList L{};
+    void* list_mem = nullptr;
+    void* list_stage = nullptr;
+    // host state flags
+    bool searched = false;      // cells match the current positions
+    bool sorted_once = false;   // the state is cell-ordered with a valid alive count
+    bool lists_valid = false;
+    bool dv_dirty = true;       // dVelocity may be non-zero (fused step assumes zero)
+    bool rpn_valid = false;     // density preview matches rho, drho and rpn_phys
+    epp_physics rpn_phys{};
+    int last_crit = EPP_CRITERION_SYMMETRY;
+    unsigned adj[kMaxTags]{};
+    // fused step graphs, one per ping-pong parity
+    cudaGraphExec_t graph[2]{};
+    epp_physics graph_phys{};
+    bool graph_accel = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;
+    std::string err;
+};
+
+namespace {
+
+int fail(epp_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, EPP_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                               \
+    } while (0)
+
+#define CK_LAUNCH() CK(cudaGetLastError())
+
+size_t state_bytes(int cap) {
+    // xh, vm, dv, comp (float4) + rho, drho, vol, p, tagm, id, cell (4 B) + rpn (8 B), aligned
+    return (size_t)cap * (4 * 16 + 7 * 4 + 8) + 12 * 256;
+}
+
+size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
+    size_t b = 2 * state_bytes(cap);
+    b += (size_t)cap * 3 * 16 + 3 * 256;                 // fused temp
+    b += (size_t)(n_cells + 2) * 4 + 256;                // count
+    b += 2 * ((size_t)(n_cells + 2) * 4 + 256);          // start[2]
+    b += (size_t)cap * 8 * 2 + 512;                      // cs, perm
+    b += (size_t)(n_tiles + 1) * 8 + 256;                // scan state
+    b += 256 * 3;                                        // status, pairs
+    b += (size_t)cap * 4 + 256;                          // ncount
+    b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
+    b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
+    b += (size_t)kIntegralBlocks * 8 * 7 + 8 * 8 + 4 * 256;
+    return b + (1 << 20);
+}
+
+template <int D>
+int run_search(epp_ctx* ctx, int crit, int action, const epp_physics* phys, bool emit);
+
+void fill_state(Arena& a, State& s, int cap) {
+    s.xh = a.take<float4>(cap);
+    s.vm = a.take<float4>(cap);
+    s.dv = a.take<float4>(cap);
+    s.comp = a.take<float4>(cap);
+    s.rho = a.take<float>(cap);
+    s.drho = a.take<float>(cap);
+    s.vol = a.take<float>(cap);
+    s.p = a.take<float>(cap);
+    s.tagm = a.take<int>(cap);
+    s.id = a.take<int>(cap);
+    s.cell = a.take<int>(cap);
+    s.rpn = a.take<float2>(cap);
+}
+
+PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
+    PairArgs A;
+    A.dom = ctx->dom;
+    A.s = ctx->S[set];
+    A.start = ctx->start[set];
+    for (int t = 0; t < kMaxTags; ++t) A.adj[t] = ctx->adj[t];
+    A.n_tags = ctx->cfg.n_tags;
+    A.crit = crit;
+    A.n_max = ctx->n;
+    A.status = ctx->status;
+    return A;
+}
+
+// clean! + insert (bin, count, scan, scatter, rank-by-id gather) from set `from` into 1-from.
+template <int D>
+int sort_cells(epp_ctx* ctx) {
+    const int from = ctx->cur, to = 1 - ctx->cur;
+    const int n = ctx->n;
+    k_bin_count<D><<<blocks_for(n), kThreads, 0, ctx->stream>>>(
+        n, ctx->dom, ctx->S[from], ctx->count, ctx->cs, ctx->cfg.max_cell_particles, ctx->status,
+        ctx->scan_state, ctx->n_tiles + 1);
+    CK_LAUNCH();
+    k_scan<<<ctx->n_tiles, kScanThreads, 0, ctx->stream>>>(ctx->n_cells + 1, ctx->count, ctx->start[to],
+                                                          ctx->scan_state, ctx->status);
+    CK_LAUNCH();
+    k_scatter<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->cs, ctx->start[to], ctx->S[from].id,
+                                                           ctx->perm, ctx->status);
+    CK_LAUNCH();
+    MoverAll mv{ctx->S[from], ctx->S[to]};
+    k_rank_gather<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->perm, ctx->cs,
+                                                               ctx->start[to], mv, ctx->status);
+    CK_LAUNCH();
+    ctx->cur = to;
+    return EPP_OK;
+}
+
+int ensure_lists(epp_ctx* ctx) {
+    if (ctx->list_mem) return EPP_OK;
+    const size_t cap = ctx->cap, nb = ctx->cfg.max_neighbour_number, D = ctx->D;
+    const size_t words = cap * nb * (1 + D + 4);
+    CK(cudaMalloc(&ctx->list_mem, words * 4));
+    CK(cudaMemsetAsync(ctx->list_mem, 0, words * 4, ctx->stream));
+    CK(cudaMalloc(&ctx->list_stage, words * 4));
+    char* p = (char*)ctx->list_mem;
+    ctx->L.idx = (int*)p; p += cap * nb * 4;
+    ctx->L.rvec = (float*)p; p += cap * nb * D * 4;
+    ctx->L.r = (float*)p; p += cap * nb * 4;
+    ctx->L.w = (float*)p; p += cap * nb * 4;
+    ctx->L.dw = (float*)p; p += cap * nb * 4;
+    ctx->L.hinv = (float*)p;
+    ctx->L.max_nb = (int)nb;
+    ctx->L.cap = (int)cap;
+    return EPP_OK;
+}
+
+template <int D>
+int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_physics* phys, bool emit,
+                       bool fused) {
+    PairArgs A = pair_args(ctx, set, crit);
+    DevPhys P = phys ? to_dev(*phys) : DevPhys{};
+    const int grid = blocks_for(ctx->n);
+    const bool cont = action == EPP_ACTION_DAMBREAK_CONTINUITY;
+#define EPP_SEARCH_LAUNCH(E, C, F)                                                              \
+    do {                                                                                        \
+        ActSearch<D, E, C, F> act{ctx->S[set], ctx->L, P, ctx->ncount, ctx->status};            \
+        k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, ctx->pairs);                      \
+    } while (0)
+    if (fused) EPP_SEARCH_LAUNCH(false, true, true);
+    else if (emit && cont) EPP_SEARCH_LAUNCH(true, true, false);
+    else if (emit) EPP_SEARCH_LAUNCH(true, false, false);
+    else if (cont) EPP_SEARCH_LAUNCH(false, true, false);
+    else EPP_SEARCH_LAUNCH(false, false, false);
+#undef EPP_SEARCH_LAUNCH
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+template <int D>
+int run_search(epp_ctx* ctx, int crit, int action, const epp_physics* phys, bool emit) {
+    if (emit) {
+        int rc = ensure_lists(ctx);
+        if (rc) return rc;
+    }
+    int rc = sort_cells<D>(ctx);
+    if (rc) return rc;
+    rc = launch_search_pass<D>(ctx, ctx->cur, crit, action, phys, emit, false);
+    if (rc) return rc;
+    ctx->searched = true;
+    ctx->sorted_once = true;
+    ctx->lists_valid = emit;
+    ctx->last_crit = crit;
+    if (action == EPP_ACTION_DAMBREAK_CONTINUITY) {
+        ctx->rpn_valid = true;
+        ctx->rpn_phys = *phys;
+    } else {
+        ctx->rpn_valid = false;
+    }
+    return EPP_OK;
+}
+
+// One fused step from set c to 1 - c (captured into a graph by the caller).  With `ev`, an
+// event is recorded before the first and after every kernel (profiling, no graph).
+template <int D>
+int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t* ev = nullptr) {
+#define EPP_MARK(k) do { if (ev) CK(cudaEventRecord(ev[k], ctx->stream)); } while (0)
+    EPP_MARK(0);
+    const int to = 1 - c;
+    const int n = ctx->n;
+    PairArgs A = pair_args(ctx, c, EPP_CRITERION_SYMMETRY);
+    ActMomentum<D, true> mom;
+    mom.s = ctx->S[c];
+    mom.P = to_dev(phys);
+    mom.dom = ctx->dom;
+    mom.F = ctx->tmp;
+    mom.F.n = n;
+    mom.F.accel = ctx->graph_accel ? ctx->accel : nullptr;
+    mom.status = ctx->status;
+    k_momentum_fused<D><<<blocks_for(n), kThreads, 0, ctx->stream>>>(A, mom);
+    CK_LAUNCH();
+    EPP_MARK(1);
+    k_scan<<<ctx->n_tiles, kScanThreads, 0, ctx->stream>>>(ctx->n_cells + 1, ctx->count, ctx->start[to],
+                                                          ctx->scan_state, ctx->status);
+    CK_LAUNCH();
+    EPP_MARK(2);
+    k_scatter<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->cs, ctx->start[to], ctx->S[c].id,
+                                                           ctx->perm, ctx->status);
+    CK_LAUNCH();
+    EPP_MARK(3);
+    MoverFused mv{ctx->S[c], ctx->S[to], mom.F, ctx->start[c], ctx->n_cells, phys.fluid_tag, phys.wall_tag};
+    k_rank_gather<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->perm, ctx->cs,
+                                                               ctx->start[to], mv, ctx->status);
+    CK_LAUNCH();
+    EPP_MARK(4);
+    int rc = launch_search_pass<D>(ctx, to, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys,
+                                   false, true);
+    if (rc) return rc;
+    EPP_MARK(5);
+#undef EPP_MARK
+    return EPP_OK;
+}
+
+template <int D>
+int build_graphs(epp_ctx* ctx, const epp_physics& phys) {
+    for (int c = 0; c < 2; ++c) {
+        if (ctx->graph[c]) {
+            cudaGraphExecDestroy(ctx->graph[c]);
+            ctx->graph[c] = nullptr;
+        }
+    }
+    for (int c = 0; c < 2; ++c) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_fused_step<D>(ctx, c, phys);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail(ctx, EPP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&ctx->graph[c], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(ctx, EPP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    ctx->graph_phys = phys;
+    return EPP_OK;
+}
+
+template <int D>
+int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
+    DevPhys P = phys ? to_dev(*phys) : DevPhys{};
+    k_self<D><<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(action, ctx->start[ctx->cur], ctx->n_cells,
+                                                                ctx->n, ctx->S[ctx->cur], P, ctx->status);
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+template <int D>
+int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
+    PairArgs A = pair_args(ctx, ctx->cur, ctx->last_crit);
+    const int grid = blocks_for(ctx->n);
+    if (action == EPP_ACTION_DAMBREAK_MOMENTUM) {
+        ActMomentum<D, false> act;
+        act.s = ctx->S[ctx->cur];
+        act.P = to_dev(*phys);
+        act.dom = ctx->dom;
+        act.F = FusedOut{};
+        act.status = ctx->status;
+        k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, nullptr);
+    } else {
+        ActCount<D> act{ctx->S[ctx->cur]};
+        k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, nullptr);
+    }
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+template <int D>
+int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
+    int rc;
+    if (ctx->dv_dirty) {
+        // the first step goes through the per-call kernels, which honour a non-zero dVelocity
+        rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_DENSITY, &phys);
+        if (!rc) rc = run_interaction<D>(ctx, EPP_ACTION_DAMBREAK_MOMENTUM, &phys);
+        if (!rc) rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_INTEGRATE, &phys);
+        if (!rc) rc = run_search<D>(ctx, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false);
+        if (rc) return rc;
+        CK(cudaMemsetAsync(ctx->S[0].dv, 0, sizeof(float4) * ctx->cap, ctx->stream));
+        CK(cudaMemsetAsync(ctx->S[1].dv, 0, sizeof(float4) * ctx->cap, ctx->stream));
+        ctx->dv_dirty = false;
+        --n_steps;
+        if (n_steps == 0) return EPP_OK;
+    }
+    if (!ctx->rpn_valid || !same_phys(ctx->rpn_phys, phys)) {
+        k_density_preview<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], to_dev(phys));
+        CK_LAUNCH();
+    }
+    if (!ctx->graph[0] || !same_phys(ctx->graph_phys, phys) || ctx->graph_accel != accel) {
+        ctx->graph_accel = accel;
+        rc = build_graphs<D>(ctx, phys);
+        if (rc) return rc;
+    }
+    for (int s = 0; s < n_steps; ++s) {
+        CK(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+        ctx->cur = 1 - ctx->cur;
+    }
+    ctx->rpn_valid = true;
+    ctx->rpn_phys = phys;
+    ctx->searched = true;
+    ctx->lists_valid = false;
+    ctx->last_crit = EPP_CRITERION_SYMMETRY;
+    return EPP_OK;
+}
+
+}  // namespace
+
+// =========================================================================================
+extern "C" {
+
+int32_t epp_abi_version(void) { return EPP_ABI_VERSION; }
+
+int32_t epp_device_count(int32_t* count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (count) *count = e == cudaSuccess ? n : 0;
+    return e == cudaSuccess && n > 0 ? EPP_OK : EPP_ERR_NO_DEVICE;
+}
+
+const char* epp_last_error(const epp_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
+    if (!cfg || !out) return EPP_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    const int D = cfg->domain.dim;
+    if ((D != 2 && D != 3) || cfg->n_capacity < 1 || cfg->n_tags < 1 || cfg->n_tags > EPP_MAX_TAGS ||
+        !(cfg->domain.gap > 0.0f))
+        return EPP_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return EPP_ERR_NO_DEVICE;
+    if (cfg->device < 0 || cfg->device >= ndev) return EPP_ERR_INVALID_ARGUMENT;
+    epp_ctx* ctx = new (std::nothrow) epp_ctx();
+    if (!ctx) return EPP_ERR_OUT_OF_MEMORY;
+    ctx->cfg = *cfg;
+    if (ctx->cfg.max_neighbour_number <= 0) ctx->cfg.max_neighbour_number = 50;
+    ctx->D = D;
+    ctx->dev = cfg->device;
+    ctx->cap = cfg->n_capacity;
+    // domain in FP32 exactly as Domain2D (Domain2D.jl:34-66)
+    DevDomain& d = ctx->dom;
+    d.dim = D;
+    const float gap = cfg->domain.gap;
+    d.gap_square = gap * gap;
+    long long ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        d.n[a] = 1;
+        d.first[a] = d.last[a] = 0.0f;
+        d.gap_inv[a] = 1.0f;
+    }
+    for (int a = 0; a < D; ++a) {
+        d.first[a] = cfg->domain.first[a];
+        d.last[a] = cfg->domain.last[a];
+        const float span = d.last[a] - d.first[a];
+        volatile float q = span / gap;
+        const int na = (int)floorf(q);
+        if (na < 1) {
+            delete ctx;
+            return EPP_ERR_INVALID_ARGUMENT;
+        }
+        d.n[a] = na;
+        volatile float ga = span / (float)na;
+        d.gap_inv[a] = 1.0f / ga;
+        ncell *= na;
+    }
+    if (ncell > (1ll << 30)) {
+        delete ctx;
+        return EPP_ERR_INVALID_ARGUMENT;
+    }
+    d.n_cells = (int)ncell;
+    ctx->n_cells = (int)ncell;
+    ctx->n_tiles = (ctx->n_cells + 1 + kScanTile - 1) / kScanTile;
+    for (int a = 0; a < cfg->n_tags; ++a) {
+        unsigned m = 0;
+        for (int b = 0; b < cfg->n_tags; ++b)
+            if (cfg->adjacency[a * EPP_MAX_TAGS + b] == 1) m |= 1u << b;
+        ctx->adj[a] = m;
+    }
+    const size_t need = arena_bytes(ctx->cap, ctx->n_cells, D, ctx->n_tiles);
+    if (cfg->hbm_budget_bytes > 0 && (long long)need > cfg->hbm_budget_bytes) {
+        delete ctx;
+        return EPP_ERR_BUDGET;
+    }
+    if (cudaSetDevice(ctx->dev) != cudaSuccess) {
+        delete ctx;
+        return EPP_ERR_CUDA;
+    }
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->arena.base, need) != cudaSuccess) {
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+        cudaGetLastError();
+        return EPP_ERR_OUT_OF_MEMORY;
+    }
+    ctx->stream = ctx->own_stream;
+    ctx->arena.size = need;
+    Arena& a = ctx->arena;
+    fill_state(a, ctx->S[0], ctx->cap);
+    fill_state(a, ctx->S[1], ctx->cap);
+    ctx->tmp.xh = a.take<float4>(ctx->cap);
+    ctx->tmp.vm = a.take<float4>(ctx->cap);
+    ctx->tmp.comp = a.take<float4>(ctx->cap);
+    ctx->count = a.take<int>(ctx->n_cells + 2);
+    ctx->start[0] = a.take<int>(ctx->n_cells + 2);
+    ctx->start[1] = a.take<int>(ctx->n_cells + 2);
+    ctx->cs = a.take<int2>(ctx->cap);
+    ctx->perm = a.take<int2>(ctx->cap);
+    ctx->scan_state = a.take<unsigned long long>(ctx->n_tiles + 1);
+    ctx->status = a.take<unsigned>(1);
+    ctx->pairs = a.take<unsigned long long>(1);
+    ctx->ncount = a.take<int>(ctx->cap);
+    ctx->stage_f = a.take<float>((size_t)ctx->cap * (3 * D + 6));
+    ctx->stage_i = a.take<int>((size_t)ctx->cap * SI_COUNT);
+    ctx->ipartial = a.take<double>(kIntegralBlocks * 7);
+    ctx->iresult = a.take<double>(8);
+    ctx->iticket = a.take<unsigned>(1);
+    ctx->ihpart = a.take<double>(kIntegralBlocks);
+    ctx->ihmin = a.take<double>(1);
+    ctx->tmp.count = ctx->count;
+    ctx->tmp.cs = ctx->cs;
+    ctx->tmp.scan_state = ctx->scan_state;
+    ctx->tmp.n_scan_words = ctx->n_tiles + 1;
+    ctx->tmp.accel = nullptr;
+    if (!ctx->ihmin) {
+        epp_destroy(ctx);
+        return EPP_ERR_OUT_OF_MEMORY;
+    }
+    if (cudaMemsetAsync(ctx->arena.base, 0, need, ctx->stream) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        epp_destroy(ctx);
+        return EPP_ERR_CUDA;
+    }
+    *out = ctx;
+    return EPP_OK;
+}
+
+int32_t epp_destroy(epp_ctx* ctx) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int c = 0; c < 2; ++c)
+        if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
+    if (ctx->accel) cudaFree(ctx->accel);
+    if (ctx->list_mem) cudaFree(ctx->list_mem);
+    if (ctx->list_stage) cudaFree(ctx->list_stage);
+    if (ctx->arena.base) cudaFree(ctx->arena.base);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return EPP_OK;
+}
+
+int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32_t* cell_index,
+                   const int32_t* ip, int64_t ldi, const float* fp, int64_t ldf,
+                   const epp_column_map* m) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (!is_alive || !ip || !fp || !m || n < 0) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "null argument");
+    if (n > ctx->cap) return fail(ctx, EPP_ERR_CAPACITY, "%d particles > capacity %d", n, ctx->cap);
+    if (m->tag < 0 || m->position < 0)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "Tag and PositionVec columns are required");
+    if (ldi < n || ldf < n) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "leading dimension < n");
+    cudaSetDevice(ctx->dev);
+    const int D = ctx->D;
+    ctx->n = n;
+    if (n == 0) {
+        ctx->searched = false;
+        return EPP_OK;
+    }
+    auto fcol = [&](int stage_col, int user_col, int width, float fill) -> int {
+        for (int k = 0; k < width; ++k) {
+            float* dst = ctx->stage_f + (size_t)(stage_col + k) * n;
+            if (user_col >= 0) {
+                CK(cudaMemcpyAsync(dst, fp + (size_t)(user_col + k) * ldf, (size_t)n * 4,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+            } else if (fill == 0.0f) {
+                CK(cudaMemsetAsync(dst, 0, (size_t)n * 4, ctx->stream));
+            } else {
+                std::vector<float> h(n, fill);
+                CK(cudaMemcpyAsync(dst, h.data(), (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+                CK(cudaStreamSynchronize(ctx->stream));
+            }
+        }
+        return EPP_OK;
+    };
+    auto icol = [&](int stage_col, const int32_t* src, int fill) -> int {
+        int* dst = ctx->stage_i + (size_t)stage_col * n;
+        if (src) {
+            CK(cudaMemcpyAsync(dst, src, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+        } else if (fill == 0) {
+            CK(cudaMemsetAsync(dst, 0, (size_t)n * 4, ctx->stream));
+        } else {
+            std::vector<int> h(n, fill);
+            CK(cudaMemcpyAsync(dst, h.data(), (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        return EPP_OK;
+    };
+    int rc = 0;
+    rc |= fcol(0, m->position, D, 0.0f);
+    rc |= fcol(sf_vel(D), m->velocity, D, 0.0f);
+    rc |= fcol(sf_dvel(D), m->dvelocity, D, 0.0f);
+    rc |= fcol(sf_mass(D), m->mass, 1, 0.0f);
+    rc |= fcol(sf_vol(D), m->volume, 1, 0.0f);
+    rc |= fcol(sf_rho(D), m->density, 1, 0.0f);
+    rc |= fcol(sf_drho(D), m->ddensity, 1, 0.0f);
+    rc |= fcol(sf_p(D), m->pressure, 1, 0.0f);
+    rc |= fcol(sf_h(D), m->h, 1, 0.0f);
+    rc |= icol(SI_TAG, ip + (size_t)m->tag * ldi, 0);
+    rc |= icol(SI_MOV, m->is_movable >= 0 ? ip + (size_t)m->is_movable * ldi : nullptr, 1);
+    rc |= icol(SI_NCOUNT, m->n_count >= 0 ? ip + (size_t)m->n_count * ldi : nullptr, 0);
+    rc |= icol(SI_ALIVE, is_alive, 0);
+    rc |= icol(SI_CELL, cell_index, 0);
+    if (rc) return rc;
+    ctx->cur = 0;
+    auto launch = [&](auto Dt) {
+        constexpr int DD = decltype(Dt)::value;
+        k_unpack<DD><<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->stage_f, ctx->stage_i,
+                                                                  ctx->S[0], ctx->ncount);
+    };
+    if (D == 2) launch(std::integral_constant<int, 2>{});
+    else launch(std::integral_constant<int, 3>{});
+    CK_LAUNCH();
+    ctx->searched = false;
+    ctx->sorted_once = false;
+    ctx->lists_valid = false;
+    ctx->rpn_valid = false;
+    ctx->dv_dirty = true;
+    return EPP_OK;
+}
+
+int32_t epp_download(epp_ctx* ctx, int32_t* is_alive, int32_t* cell_index, int32_t* ip, int64_t ldi,
+                     float* fp, int64_t ldf, const epp_column_map* m) {
+    if (!ctx || !m) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    const int D = ctx->D, n = ctx->n;
+    if (n == 0) return EPP_OK;
+    if ((ip && ldi < n) || (fp && ldf < n)) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "leading dimension < n");
+    auto launch = [&](auto Dt) {
+        constexpr int DD = decltype(Dt)::value;
+        k_pack<DD><<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->stage_f, ctx->stage_i,
+                                                                ctx->S[ctx->cur], ctx->ncount);
+    };
+    if (D == 2) launch(std::integral_constant<int, 2>{});
+    else launch(std::integral_constant<int, 3>{});
+    CK_LAUNCH();
+    auto fget = [&](int stage_col, int user_col, int width) -> int {
+        if (!fp || user_col < 0) return EPP_OK;
+        for (int k = 0; k < width; ++k)
+            CK(cudaMemcpyAsync(fp + (size_t)(user_col + k) * ldf, ctx->stage_f + (size_t)(stage_col + k) * n,
+                               (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        return EPP_OK;
+    };
+    auto iget = [&](int stage_col, int32_t* dst) -> int {
+        if (!dst) return EPP_OK;
+        CK(cudaMemcpyAsync(dst, ctx->stage_i + (size_t)stage_col * n, (size_t)n * 4, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        return EPP_OK;
+    };
+    int rc = 0;
+    rc |= fget(0, m->position, D);
+    rc |= fget(sf_vel(D), m->velocity, D);
+    rc |= fget(sf_dvel(D), m->dvelocity, D);
+    rc |= fget(sf_mass(D), m->mass, 1);
+    rc |= fget(sf_vol(D), m->volume, 1);
+    rc |= fget(sf_rho(D), m->density, 1);
+    rc |= fget(sf_drho(D), m->ddensity, 1);
+    rc |= fget(sf_p(D), m->pressure, 1);
+    rc |= fget(sf_h(D), m->h, 1);
+    rc |= iget(SI_ALIVE, is_alive);
+    rc |= iget(SI_CELL, cell_index);
+    if (ip) {
+        if (m->tag >= 0) rc |= iget(SI_TAG, ip + (size_t)m->tag * ldi);
+        if (m->is_movable >= 0) rc |= iget(SI_MOV, ip + (size_t)m->is_movable * ldi);
+        if (m->n_count >= 0) rc |= iget(SI_NCOUNT, ip + (size_t)m->n_count * ldi);
+    }
+    if (rc) return rc;
+    const bool want_lists = ctx->lists_valid && ((ip && m->n_index >= 0) ||
+                            (fp && (m->n_rvec >= 0 || m->n_r >= 0 || m->n_w >= 0 || m->n_dw >= 0 || m->n_hinv >= 0)));
+    if (want_lists) {
+        const size_t nb = ctx->L.max_nb;
+        int* nidx = (int*)ctx->list_stage;
+        float* nrvec = (float*)(nidx + nb * n);
+        float* nr = nrvec + nb * D * n;
+        float* nw = nr + nb * n;
+        float* ndw = nw + nb * n;
+        float* nh = ndw + nb * n;
+        auto launch2 = [&](auto Dt) {
+            constexpr int DD = decltype(Dt)::value;
+            k_pack_lists<DD><<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->L, ctx->S[ctx->cur].id,
+                                                                          ctx->ncount, nidx, nrvec, nr, nw, ndw, nh);
+        };
+        if (D == 2) launch2(std::integral_constant<int, 2>{});
+        else launch2(std::integral_constant<int, 3>{});
+        CK_LAUNCH();
+        auto cols = [&](const void* src, void* dstbase, int user_col, int64_t ld, int ncols) -> int {
+            if (user_col < 0 || !dstbase) return EPP_OK;
+            for (int k = 0; k < ncols; ++k)
+                CK(cudaMemcpyAsync((char*)dstbase + ((size_t)(user_col + k) * ld) * 4,
+                                   (const char*)src + (size_t)k * n * 4, (size_t)n * 4,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+            return EPP_OK;
+        };
+        rc |= cols(nidx, ip, ip ? m->n_index : -1, ldi, (int)nb);
+        rc |= cols(nrvec, fp, fp ? m->n_rvec : -1, ldf, (int)(nb * D));
+        rc |= cols(nr, fp, fp ? m->n_r : -1, ldf, (int)nb);
+        rc |= cols(nw, fp, fp ? m->n_w : -1, ldf, (int)nb);
+        rc |= cols(ndw, fp, fp ? m->n_dw : -1, ldf, (int)nb);
+        rc |= cols(nh, fp, fp ? m->n_hinv : -1, ldf, (int)nb);
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return EPP_OK;
+}
+
+int32_t epp_search(epp_ctx* ctx, int32_t criterion, int32_t action, const epp_physics* phys, int32_t flags) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (criterion != EPP_CRITERION_DEFAULT && criterion != EPP_CRITERION_SYMMETRY)
+        return fail(ctx, EPP_ERR_UNSUPPORTED_CRITERION, "criterion %d", criterion);
+    if (action != EPP_ACTION_NONE && action != EPP_ACTION_DAMBREAK_CONTINUITY)
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "search action %d", action);
+    if (action == EPP_ACTION_DAMBREAK_CONTINUITY && !phys)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
+    cudaSetDevice(ctx->dev);
+    if (ctx->n == 0) return EPP_OK;
+    const bool emit = (flags & EPP_SEARCH_EMIT_LIST) != 0;
+    return ctx->D == 2 ? run_search<2>(ctx, criterion, action, phys, emit)
+                       : run_search<3>(ctx, criterion, action, phys, emit);
+}
+
+int32_t epp_interaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (action == EPP_ACTION_NONE) return EPP_OK;
+    if (action != EPP_ACTION_DAMBREAK_MOMENTUM && action != EPP_ACTION_COUNT_NEIGHBOURS)
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "interaction action %d", action);
+    if (action == EPP_ACTION_DAMBREAK_MOMENTUM && !phys)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
+    if (!ctx->searched)
+        return fail(ctx, EPP_ERR_STATE, "interaction! needs a search! at the current positions");
+    cudaSetDevice(ctx->dev);
+    if (ctx->n == 0) return EPP_OK;
+    ctx->dv_dirty = true;
+    return ctx->D == 2 ? run_interaction<2>(ctx, action, phys) : run_interaction<3>(ctx, action, phys);
+}
+
+int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (action == EPP_ACTION_NONE) return EPP_OK;
+    if (action != EPP_ACTION_DAMBREAK_DENSITY && action != EPP_ACTION_DAMBREAK_INTEGRATE &&
+        action != EPP_ACTION_ZERO_DVELOCITY)
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "selfaction action %d", action);
+    if (action != EPP_ACTION_ZERO_DVELOCITY && !phys)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
+    if (!ctx->sorted_once)
+        return fail(ctx, EPP_ERR_STATE, "selfaction! runs on the cell-sorted state: call search! first");
+    cudaSetDevice(ctx->dev);
+    if (ctx->n == 0) return EPP_OK;
+    int rc = ctx->D == 2 ? run_selfaction<2>(ctx, action, phys) : run_selfaction<3>(ctx, action, phys);
+    if (action == EPP_ACTION_DAMBREAK_INTEGRATE) {
+        ctx->searched = false;   // positions moved: the next pass needs a search!
+        ctx->rpn_valid = false;
+    }
+    if (action == EPP_ACTION_DAMBREAK_DENSITY) ctx->rpn_valid = false;
+    if (action == EPP_ACTION_ZERO_DVELOCITY) ctx->dv_dirty = true;
+    ctx->lists_valid = ctx->lists_valid && action != EPP_ACTION_DAMBREAK_INTEGRATE;
+    return rc;
+}
+
+int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (!phys || n_steps < 0) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (!ctx->searched)
+        return fail(ctx, EPP_ERR_STATE, "epp_step needs an initial search! (main.jl:157-164)");
+    cudaSetDevice(ctx->dev);
+    if (n_steps == 0 || ctx->n == 0) return EPP_OK;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    int rc = ctx->D == 2 ? run_step<2>(ctx, n_steps, *phys, ctx->accel != nullptr)
+                         : run_step<3>(ctx, n_steps, *phys, ctx->accel != nullptr);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->timed = true;
+    return EPP_OK;
+}
+
+int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out) {
+    if (!ctx || !phys || !out) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    std::memset(out, 0, sizeof *out);
+    if (ctx->n == 0) return EPP_OK;
+    if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
+    IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket, ctx->ihpart, ctx->ihmin};
+    DevPhys P = to_dev(*phys);
+    auto launch = [&](auto Dt) {
+        constexpr int DD = decltype(Dt)::value;
+        k_integrals<DD><<<kIntegralBlocks, 256, 0, ctx->stream>>>(
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], P, phys->rho0, phys->c0, phys->gamma, phys->p0,
+            phys->gravity[0], phys->gravity[1], phys->gravity[2], O);
+    };
+    if (ctx->D == 2) launch(std::integral_constant<int, 2>{});
+    else launch(std::integral_constant<int, 3>{});
+    CK_LAUNCH();
+    double r[8];
+    int n_alive = 0;
+    CK(cudaMemcpyAsync(r, ctx->iresult, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&r[6], ctx->ihmin, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&n_alive, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    std::vector<int> nc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    out->mass_total = r[0];
+    out->mass_fluid = r[1];
+    out->kinetic = r[2];
+    out->potential = r[3];
+    out->internal = r[4];
+    out->max_speed = r[5];
+    out->cfl_dt = r[6] < 1e300 ? 0.1 * r[6] / ((double)phys->c0 + r[5]) : 0.0;
+    out->n_alive = n_alive;
+    // directed pairs of the last search = sum of nCount over alive particles
+    nc.resize(n_alive);
+    if (n_alive > 0) {
+        CK(cudaMemcpy(nc.data(), ctx->ncount, sizeof(int) * n_alive, cudaMemcpyDeviceToHost));
+        long long s = 0;
+        for (int v : nc) s += v;
+        out->n_pairs = s;
+    }
+    return EPP_OK;
+}
+
+int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t* sorted_ids, int32_t* n_cells) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (n_cells) *n_cells = ctx->n_cells;
+    if (!counts && !offsets && !sorted_ids) return EPP_OK;
+    if (!ctx->searched) return fail(ctx, EPP_ERR_STATE, "no cell list: call search! first");
+    cudaSetDevice(ctx->dev);
+    std::vector<int> st(ctx->n_cells + 2);
+    CK(cudaMemcpyAsync(st.data(), ctx->start[ctx->cur], sizeof(int) * (ctx->n_cells + 1), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int n_alive = st[ctx->n_cells];
+    if (counts)
+        for (int c = 0; c < ctx->n_cells; ++c) counts[c] = st[c + 1] - st[c];
+    if (offsets)
+        for (int c = 0; c <= ctx->n_cells; ++c) offsets[c] = st[c];
+    if (sorted_ids && n_alive > 0) {
+        CK(cudaMemcpy(sorted_ids, ctx->S[ctx->cur].id, sizeof(int) * n_alive, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n_alive; ++k) sorted_ids[k] += 1;
+    }
+    return EPP_OK;
+}
+
+int32_t epp_synchronize(epp_ctx* ctx, uint32_t* device_status) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned st = 0;
+    CK(cudaMemcpy(&st, ctx->status, sizeof st, cudaMemcpyDeviceToHost));
+    CK(cudaMemset(ctx->status, 0, sizeof st));
+    if (device_status) *device_status = st;
+    if (st & ~(unsigned)EPP_STATUS_KILLED)
+        return fail(ctx, EPP_ERR_DEVICE_STATUS, "device status 0x%x", st);
+    return EPP_OK;
+}
+
+int32_t epp_last_step_timing(epp_ctx* ctx, float* ms_total) {
+    if (!ctx || !ms_total) return EPP_ERR_INVALID_ARGUMENT;
+    if (!ctx->timed) return fail(ctx, EPP_ERR_STATE, "no timed step");
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(ms_total, ctx->ev0, ctx->ev1));
+    return EPP_OK;
+}
+
+int32_t epp_pairs_total(epp_ctx* ctx, int64_t* out) {
+    if (!ctx || !out) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    unsigned long long v = 0;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(&v, ctx->pairs, sizeof v, cudaMemcpyDeviceToHost));
+    *out = (int64_t)v;
+    return EPP_OK;
+}
+
+int32_t epp_set_stream(epp_ctx* ctx, void* stream) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return EPP_OK;
+}
+
+int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms) {
+    if (!ctx || !phys || !stage_ms) return EPP_ERR_INVALID_ARGUMENT;
+    if (!ctx->searched) return fail(ctx, EPP_ERR_STATE, "epp_profile_step needs an initial search!");
+    cudaSetDevice(ctx->dev);
+    if (ctx->n == 0) return EPP_OK;
+    if (ctx->dv_dirty) {
+        int rc = epp_step(ctx, 1, phys);   // settles dVelocity through the per-call path
+        if (rc) return rc;
+    }
+    if (!ctx->rpn_valid || !same_phys(ctx->rpn_phys, *phys)) {
+        k_density_preview<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], to_dev(*phys));
+        CK_LAUNCH();
+    }
+    cudaEvent_t ev[6];
+    for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
+    int rc = ctx->D == 2 ? enqueue_fused_step<2>(ctx, ctx->cur, *phys, ev)
+                         : enqueue_fused_step<3>(ctx, ctx->cur, *phys, ev);
+    if (!rc) {
+        ctx->cur = 1 - ctx->cur;
+        ctx->rpn_valid = true;
+        ctx->rpn_phys = *phys;
+        ctx->lists_valid = false;
+        cudaError_t e = cudaEventSynchronize(ev[5]);
+        for (int k = 0; k < 5 && e == cudaSuccess; ++k) e = cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
+        if (e != cudaSuccess) rc = fail(ctx, EPP_ERR_CUDA, "profile events: %s", cudaGetErrorString(e));
+    }
+    for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
+    return rc;
+}
+
+int32_t epp_set_accel_output(epp_ctx* ctx, int32_t enable) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    if (enable && !ctx->accel) {
+        CK(cudaMalloc(&ctx->accel, sizeof(float4) * ctx->cap));
+        CK(cudaMemsetAsync(ctx->accel, 0, sizeof(float4) * ctx->cap, ctx->stream));
+    } else if (!enable && ctx->accel) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->accel);
+        ctx->accel = nullptr;
+    }
+    return EPP_OK;
+}
+
+int32_t epp_get_accel(epp_ctx* ctx, float* out, int32_t n) {
+    // dv/dt (momentum + gravity) of the last fused step, per particle row, dim components each
+    // stored as out[a * n + row]; rows of non-fluid particles are 0.
+    if (!ctx || !out || n != ctx->n) return EPP_ERR_INVALID_ARGUMENT;
+    if (!ctx->accel) return fail(ctx, EPP_ERR_STATE, "accel output disabled");
+    cudaSetDevice(ctx->dev);
+    // accel is indexed by the order before the last gather; the permutation is cs/perm.  Copy
+    // with the id array of that order (the other ping-pong set).
+    std::vector<float4> a(ctx->n);
+    std::vector<int> ids(ctx->n);
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(a.data(), ctx->accel, sizeof(float4) * ctx->n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ids.data(), ctx->S[1 - ctx->cur].id, sizeof(int) * ctx->n, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < ctx->n; ++k) {
+        const int i = ids[k];
+        out[i] = a[k].x;
+        out[(size_t)n + i] = a[k].y;
+        if (ctx->D == 3) out[(size_t)2 * n + i] = a[k].z;
+    }
+    return EPP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,157 @@
+// epp_math.cuh -- device-side state layout, constants and SPH formulas.
+//
+// Formulas follow the reference's Julia sources (paths relative to the EtherParallelParticles.jl
+// root); the operation order is kept so that FP32 results agree with a literal evaluation:
+//   Wendland C2           src/SPH/Kernel/WendlandC2.jl:10-49
+//   power                 src/Math/OptimizedFunction.jl:10-42
+//   Mean                  src/Math/Mean.jl:12-34
+//   criteria              src/Algorithm/NeighbourSearch.jl:141-164 (IEEE, no contraction: exact)
+//   cell arithmetic       src/Class/Domain/Domain2D.jl:110-137, AbstractDomain.jl:12-19 (exact)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/epp.h"
+
+namespace epp {
+
+constexpr int kMaxTags = EPP_MAX_TAGS;
+
+// Domain in FP32 (as Domain2D{Int32, Float32}); n[a] cells per axis, x fastest.
+struct DevDomain {
+    int dim;
+    int n[3];
+    int n_cells;
+    float gap_square;
+    float first[3], last[3], gap_inv[3];
+};
+
+// Physics constants rounded to FP32 the way `parallel(x)` converts them (Parallel.jl:62-74).
+struct DevPhys {
+    float dt, rho0, c0, p0, B;
+    float g[3];
+    float alpha, beta;
+    int gamma, visc, fluid, wall, kahan;
+};
+
+// Cell-sorted particle state.  Positions and velocities carry h and m in their w lanes so that
+// one 16-byte load gives what the neighbour filter (x, h) or the pair term (v, m) needs.
+struct State {
+    float4* xh;      // (x, y, z, h)      z = 0 in 2D
+    float4* vm;      // (vx, vy, vz, m)
+    float4* dv;      // dVelocity accumulator (interaction! / selfaction! calls)
+    float4* comp;    // Kahan compensation of x
+    float* rho;
+    float* drho;
+    float* vol;
+    float* p;
+    int* tagm;       // tag | movable << 16
+    int* id;         // 0-based row of the particle in the caller's matrices
+    int* cell;       // 0-based cell (n_cells = dead bin)
+    float2* rpn;     // (rho, p) after the next density update -- input of the fused momentum pass
+};
+
+struct NeighbourList {   // EPP_SEARCH_EMIT_LIST output, column-major [k * cap + i]
+    int* idx;            // sorted index of the neighbour
+    float* rvec;         // [(D*k + a) * cap + i]
+    float* r;
+    float* w;
+    float* dw;
+    float* hinv;
+    int max_nb;
+    int cap;
+};
+
+__host__ __device__ inline int tag_of(int tm) { return tm & 0xffff; }
+__host__ __device__ inline int movable_of(int tm) { return (tm >> 16) & 1; }
+
+// power(x, Val(N)) of OptimizedFunction.jl:10-42, same association.
+__device__ __forceinline__ float powi(float x, int n) {
+    float t;
+    switch (n) {
+        case 0: return 1.0f;
+        case 1: return x;
+        case 2: return x * x;
+        case 3: return x * x * x;
+        case 4: t = x * x; return t * t;
+        case 5: t = x * x; return t * t * x;
+        case 6: t = x * x * x; return t * t;
+        case 7: t = x * x * x; return t * t * x;
+        case 8: t = x * x; t = t * t; return t * t;
+        default: {
+            float e = x;
+            for (int i = 2; i <= n; ++i) e = e * x;
+            return e;
+        }
+    }
+}
+
+// Division used by the physics terms.  The reference's pair functions use IEEE division; the
+// fast form differs by at most 2 ulp and stays well inside the 1e-5 parity tolerance.
+__device__ __forceinline__ float fdiv(float a, float b) {
+#ifdef EPP_IEEE_DIV
+    return __fdiv_rn(a, b);
+#else
+    return __fdividef(a, b);
+#endif
+}
+
+// Mean.harmonic(a, b) * 2 with IEEE operations, as the symmetric criterion evaluates it.
+__device__ __forceinline__ float harmonic2_exact(float a, float b) {
+    return __fmul_rn(__fdiv_rn(__fmul_rn(__fmul_rn(2.0f, a), b), __fadd_rn(a, b)), 2.0f);
+}
+// Mean.invharmonic(a, b) = (a + b) / (2 a b), IEEE (it is cached per particle when h_i == h_j).
+__device__ __forceinline__ float invharmonic_exact(float a, float b) {
+    return __fdiv_rn(__fadd_rn(a, b), __fmul_rn(__fmul_rn(2.0f, a), b));
+}
+
+template <int D>
+__device__ __forceinline__ float wc2_sigma() {
+    return D == 2 ? 0.55704230082163f /* 7/(4 pi) */ : 0.41778172561623f /* 21/(16 pi) */;
+}
+
+// _value(r, hinv), WendlandC2.jl:17-28
+template <int D>
+__device__ __forceinline__ float wc2_value(float r, float hinv) {
+    float q = r * hinv;
+    if (q < 2.0f)
+        return wc2_sigma<D>() * powi(2.0f - q, 4) * powi(hinv, D) * (1.0f + 2.0f * q) * 0.0625f;
+    return 0.0f;
+}
+
+// _gradient(r, hinv), WendlandC2.jl:38-49
+template <int D>
+__device__ __forceinline__ float wc2_gradient(float r, float hinv) {
+    float q = r * hinv;
+    if (q < 2.0f) return -wc2_sigma<D>() * powi(hinv, D + 1) * 0.625f * q * powi(2.0f - q, 3);
+    return 0.0f;
+}
+
+// Tait EOS: p = B ((rho / rho0)^gamma - 1) + p0 (replaces the linear eos of main.jl:64).
+__device__ __forceinline__ float eos(const DevPhys& P, float rho) {
+    return P.B * (powi(__fdiv_rn(rho, P.rho0), P.gamma) - 1.0f) + P.p0;
+}
+
+// Cell of a position: indexCartesianFromPosition + indexCartesianToLinear (Domain2D.jl:92-137),
+// 0-based.  Returns -1 when the position is outside the domain (the particle is then killed,
+// NeighbourSearch.jl:41-43).
+template <int D>
+__device__ __forceinline__ int cell_of(const DevDomain& dom, float4 x) {
+    float xs[3] = {x.x, x.y, x.z};
+#pragma unroll
+    for (int a = 0; a < D; ++a)
+        if (!(dom.first[a] <= xs[a] && xs[a] <= dom.last[a])) return -1;
+    int lin = 0, stride = 1;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        float f = floorf(__fmul_rn(__fsub_rn(xs[a], dom.first[a]), dom.gap_inv[a]));
+        int i = (int)f;   // unsafe_trunc(Int32, floor(.)), 0-based here
+        i = min(dom.n[a] - 1, i);
+        i = max(0, i);
+        lin += i * stride;
+        stride *= dom.n[a];
+    }
+    return lin;
+}
+
+}  // namespace epp

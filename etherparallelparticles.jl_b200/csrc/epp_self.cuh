@@ -1,0 +1,279 @@
+// epp_self.cuh -- per-particle passes: selfaction! actions, the fused-step gather, FP64
+// integrals, and the pack/unpack kernels between the reference layout and the sorted state.
+#pragma once
+#include "epp_pair.cuh"
+
+namespace epp {
+
+// selfaction! (Action.jl:39-51) bodies.  Alive particles are the first start[n_cells] rows.
+// DAMBREAK_DENSITY: sContinuity! wrapper of main.jl:92-105 (Continuity.jl:10-21, State.jl:10-19).
+// DAMBREAK_INTEGRATE: sMomentum! of main.jl:120-126 with sAccelerate! + sMove! (Motion.jl:17-51).
+template <int D>
+__global__ void k_self(int action, const int* start, int n_cells, int n_max, State s, DevPhys P,
+                       unsigned* status) {
+    const int n_alive = min(start[n_cells], n_max);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_alive) return;
+    const int ti = tag_of(s.tagm[i]);
+    if (action == EPP_ACTION_ZERO_DVELOCITY) {
+        s.dv[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else if (action == EPP_ACTION_DAMBREAK_DENSITY) {
+        if (ti == P.fluid || ti == P.wall) {
+            const float rho = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt));
+            s.rho[i] = rho;
+            s.drho[i] = 0.0f;
+            s.vol[i] = __fdiv_rn(s.vm[i].w, rho);
+            s.p[i] = eos(P, rho);
+            if (!isfinite(rho)) atomicOr(status, EPP_STATUS_NONFINITE);
+        }
+    } else if (action == EPP_ACTION_DAMBREAK_INTEGRATE) {
+        if (ti == P.fluid) {
+            float4 d = s.dv[i], v = s.vm[i], x = s.xh[i], c = s.comp[i];
+            float du[3] = {d.x, d.y, d.z}, vv[3] = {v.x, v.y, v.z}, xx[3] = {x.x, x.y, x.z};
+            float cc[3] = {c.x, c.y, c.z};
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                du[k] = __fadd_rn(du[k], P.g[k]);
+                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], P.dt));
+            }
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                if (P.kahan) {
+                    const float y = __fsub_rn(__fmul_rn(vv[k], P.dt), cc[k]);
+                    const float t = __fadd_rn(xx[k], y);
+                    cc[k] = __fsub_rn(__fsub_rn(t, xx[k]), y);
+                    xx[k] = t;
+                } else {
+                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], P.dt));
+                }
+            }
+            s.dv[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            s.vm[i] = make_float4(vv[0], vv[1], vv[2], v.w);
+            s.xh[i] = make_float4(xx[0], xx[1], xx[2], x.w);
+            s.comp[i] = make_float4(cc[0], cc[1], cc[2], 0.0f);
+            if (!(isfinite(vv[0]) && isfinite(vv[1]) && isfinite(vv[2])))
+                atomicOr(status, EPP_STATUS_NONFINITE);
+        }
+    }
+}
+
+// Density preview used when the fused step starts from a state whose rpn is not current.
+__global__ void k_density_preview(const int* start, int n_cells, int n_max, State s, DevPhys P) {
+    const int n_alive = min(start[n_cells], n_max);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_alive) return;
+    const int ti = tag_of(s.tagm[i]);
+    float2 rp;
+    if (ti == P.fluid || ti == P.wall) {
+        rp.x = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt));
+        rp.y = eos(P, rp.x);
+    } else {
+        rp.x = s.rho[i];
+        rp.y = s.p[i];
+    }
+    s.rpn[i] = rp;
+}
+
+// Gather of the fused step: positions / velocities / compensation from the momentum pass's
+// output, density and pressure from the preview (what sContinuity! left), volume = m / rho.
+// Particles that were dead before this step keep their stored values.
+struct MoverFused {
+    State a, b;
+    FusedOut F;
+    const int* start_old;
+    int n_cells;
+    int fluid, wall;
+    __device__ __forceinline__ void operator()(int src, int dst, int c) const {
+        const float4 vm = F.vm[src];
+        b.xh[dst] = F.xh[src];
+        b.vm[dst] = vm;
+        b.comp[dst] = F.comp[src];
+        const int tm = a.tagm[src];
+        b.tagm[dst] = tm;
+        b.id[dst] = a.id[src];
+        b.cell[dst] = c;
+        const int t = tag_of(tm);
+        if (src < start_old[n_cells] && (t == fluid || t == wall)) {
+            const float2 rp = a.rpn[src];
+            b.rho[dst] = rp.x;
+            b.p[dst] = rp.y;
+            b.vol[dst] = __fdiv_rn(vm.w, rp.x);
+        } else {
+            b.rho[dst] = a.rho[src];
+            b.p[dst] = a.p[src];
+            b.vol[dst] = a.vol[src];
+        }
+    }
+};
+
+// FP64 integrals: per-block partials, the last block folds them in block order (deterministic).
+struct IntegralsOut {
+    double* partial;       // [n_blocks * 6]
+    double* result;        // [6]: mass_total, mass_fluid, kinetic, potential, internal, max|v|
+    unsigned* ticket;
+    double* hmin_partial;  // [n_blocks]
+    double* hmin;          // [1]
+};
+
+template <int D>
+__global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells, int n_max, State s,
+                                                   DevPhys P, double rho0, double c0,
+                                                   double gam, double p0, double g0, double g1,
+                                                   double g2, IntegralsOut O) {
+    __shared__ double sh[6][256 / 32];
+    __shared__ double shh[256 / 32];
+    __shared__ bool last;
+    const int n_alive = min(start[n_cells], n_max);
+    const double B = rho0 * c0 * c0 / gam;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    double hmin = 1e300;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_alive; i += gridDim.x * blockDim.x) {
+        const float4 vm = s.vm[i];
+        const double m = (double)vm.w;
+        v[0] += m;
+        if (tag_of(s.tagm[i]) != P.fluid) continue;
+        const float4 xh = s.xh[i];
+        v[1] += m;
+        const double u2 = (double)vm.x * vm.x + (double)vm.y * vm.y + (D == 3 ? (double)vm.z * vm.z : 0.0);
+        v[2] += 0.5 * m * u2;
+        v[3] += -m * (g0 * xh.x + g1 * xh.y + (D == 3 ? g2 * xh.z : 0.0));
+        const double r = (double)s.rho[i];
+        v[4] += m * ((B / rho0) * (pow(r / rho0, gam - 1.0) / (gam - 1.0) + rho0 / r - gam / (gam - 1.0)) +
+                     p0 * (1.0 / rho0 - 1.0 / r));
+        v[5] = fmax(v[5], sqrt(u2));
+        hmin = fmin(hmin, (double)xh.w);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_down_sync(0xffffffffu, v[k], o);
+            v[k] = k == 5 ? fmax(v[k], t) : v[k] + t;
+        }
+        if (lane == 0) sh[k][warp] = v[k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) hmin = fmin(hmin, __shfl_down_sync(0xffffffffu, hmin, o));
+    if (lane == 0) shh[warp] = hmin;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 6; ++k) {
+            double a = sh[k][0];
+            for (int w = 1; w < 256 / 32; ++w) a = k == 5 ? fmax(a, sh[k][w]) : a + sh[k][w];
+            O.partial[blockIdx.x * 6 + k] = a;
+        }
+        double hm = shh[0];
+        for (int w = 1; w < 256 / 32; ++w) hm = fmin(hm, shh[w]);
+        O.hmin_partial[blockIdx.x] = hm;
+        __threadfence();
+        last = atomicAdd(O.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        for (int k = 0; k < 6; ++k) {
+            double a = k == 5 ? 0.0 : 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b) {
+                const double t = ((volatile double*)O.partial)[b * 6 + k];
+                a = k == 5 ? fmax(a, t) : a + t;
+            }
+            O.result[k] = a;
+        }
+        double hm = 1e300;
+        for (unsigned b = 0; b < gridDim.x; ++b) hm = fmin(hm, ((volatile double*)O.hmin_partial)[b]);
+        O.hmin[0] = hm;
+        *O.ticket = 0;
+    }
+}
+
+// Staging columns (by particle row), used by upload and download:
+//   float: position[D], velocity[D], dvelocity[D], mass, volume, density, ddensity, pressure, h
+//   int:   tag, movable, ncount, alive, cell
+enum { SF_POS = 0 };
+__host__ __device__ inline int sf_vel(int D) { return D; }
+__host__ __device__ inline int sf_dvel(int D) { return 2 * D; }
+__host__ __device__ inline int sf_mass(int D) { return 3 * D; }
+__host__ __device__ inline int sf_vol(int D) { return 3 * D + 1; }
+__host__ __device__ inline int sf_rho(int D) { return 3 * D + 2; }
+__host__ __device__ inline int sf_drho(int D) { return 3 * D + 3; }
+__host__ __device__ inline int sf_p(int D) { return 3 * D + 4; }
+__host__ __device__ inline int sf_h(int D) { return 3 * D + 5; }
+__host__ __device__ inline int sf_count(int D) { return 3 * D + 6; }
+enum { SI_TAG = 0, SI_MOV = 1, SI_NCOUNT = 2, SI_ALIVE = 3, SI_CELL = 4, SI_COUNT = 5 };
+
+// Rows of the caller's matrices -> state in row order (a search sorts it afterwards).
+template <int D>
+__global__ void k_unpack(int n, int n_cells, const float* sf, const int* si, State s, int* ncount) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    auto F = [&](int col) { return sf[(size_t)col * n + i]; };
+    auto I = [&](int col) { return si[(size_t)col * n + i]; };
+    s.xh[i] = make_float4(F(0), F(1), D == 3 ? F(2) : 0.0f, F(sf_h(D)));
+    s.vm[i] = make_float4(F(sf_vel(D)), F(sf_vel(D) + 1), D == 3 ? F(sf_vel(D) + 2) : 0.0f, F(sf_mass(D)));
+    s.dv[i] = make_float4(F(sf_dvel(D)), F(sf_dvel(D) + 1), D == 3 ? F(sf_dvel(D) + 2) : 0.0f, 0.0f);
+    s.comp[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    s.rho[i] = F(sf_rho(D));
+    s.drho[i] = F(sf_drho(D));
+    s.vol[i] = F(sf_vol(D));
+    s.p[i] = F(sf_p(D));
+    s.tagm[i] = (I(SI_TAG) & 0xffff) | ((I(SI_MOV) != 0) << 16);
+    s.id[i] = i;
+    const int cell1 = I(SI_CELL);
+    s.cell[i] = I(SI_ALIVE) == 1 ? (cell1 >= 1 && cell1 <= n_cells ? cell1 - 1 : -1) : n_cells;
+    ncount[i] = I(SI_NCOUNT);
+}
+
+// Sorted state -> staging columns by particle row.
+template <int D>
+__global__ void k_pack(int n, int n_cells, float* sf, int* si, State s, const int* ncount) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = s.id[k];
+    auto F = [&](int col, float v) { sf[(size_t)col * n + i] = v; };
+    auto I = [&](int col, int v) { si[(size_t)col * n + i] = v; };
+    const float4 x = s.xh[k], v = s.vm[k], d = s.dv[k];
+    F(0, x.x); F(1, x.y); if (D == 3) F(2, x.z);
+    F(sf_vel(D), v.x); F(sf_vel(D) + 1, v.y); if (D == 3) F(sf_vel(D) + 2, v.z);
+    F(sf_dvel(D), d.x); F(sf_dvel(D) + 1, d.y); if (D == 3) F(sf_dvel(D) + 2, d.z);
+    F(sf_mass(D), v.w);
+    F(sf_vol(D), s.vol[k]);
+    F(sf_rho(D), s.rho[k]);
+    F(sf_drho(D), s.drho[k]);
+    F(sf_p(D), s.p[k]);
+    F(sf_h(D), x.w);
+    const int tm = s.tagm[k];
+    I(SI_TAG, tag_of(tm));
+    I(SI_MOV, movable_of(tm));
+    I(SI_NCOUNT, ncount[k]);
+    const int c = s.cell[k];
+    const bool alive = c != n_cells;
+    I(SI_ALIVE, alive ? 1 : 0);
+    I(SI_CELL, alive && c >= 0 ? c + 1 : 0);
+}
+
+// Emitted neighbour lists -> reference columns by particle row: nIndex (1-based ids), nRVec,
+// nR, nW, nDW, nHInv.  Staging blocks are [max_nb * n] (nRVec [D * max_nb * n]).
+template <int D>
+__global__ void k_pack_lists(int n, NeighbourList L, const int* sorted_id, const int* ncount,
+                             int* nidx, float* nrvec, float* nr, float* nw, float* ndw,
+                             float* nhinv) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = sorted_id[k];
+    const int cnt = min(ncount[k], L.max_nb);
+    for (int q = 0; q < L.max_nb; ++q) {
+        const bool on = q < cnt;
+        const size_t src = (size_t)q * L.cap + k;
+        const size_t dst = (size_t)q * n + i;
+        nidx[dst] = on ? sorted_id[L.idx[src]] + 1 : 0;
+        nr[dst] = on ? L.r[src] : 0.0f;
+        nw[dst] = on ? L.w[src] : 0.0f;
+        ndw[dst] = on ? L.dw[src] : 0.0f;
+        nhinv[dst] = on ? L.hinv[src] : 0.0f;
+        for (int a = 0; a < D; ++a)
+            nrvec[((size_t)D * q + a) * n + i] = on ? L.rvec[((size_t)D * q + a) * L.cap + k] : 0.0f;
+    }
+}
+
+}  // namespace epp

@@ -1,0 +1,191 @@
+"""ctypes binding of libepp.so (include/epp.h).
+
+The library is built in-tree (csrc/Makefile) next to this file.  There is no CPU fallback:
+loading fails loudly when the library is missing, and every entry point raises EppError on a
+non-zero status.
+"""
+import ctypes as C
+import os
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libepp.so")
+
+EXPORTS = [
+    "epp_abi_version", "epp_device_count", "epp_create", "epp_destroy", "epp_last_error",
+    "epp_upload", "epp_download", "epp_search", "epp_interaction", "epp_selfaction", "epp_step",
+    "epp_get_integrals", "epp_cell_stats", "epp_synchronize", "epp_last_step_timing",
+    "epp_pairs_total", "epp_set_accel_output", "epp_get_accel", "epp_set_stream",
+    "epp_profile_step",
+]
+
+
+class EppError(RuntimeError):
+    def __init__(self, code, what, detail=""):
+        self.code = code
+        super().__init__("%s -> %s %s" % (what, abi.STATUS_NAMES.get(code, code), detail))
+
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError("libepp.so is not built (%s); run __graft_entry__.build() or make -C "
+                          "etherparallelparticles.jl_b200/csrc" % path)
+    lib = C.CDLL(path)
+    P = C.POINTER
+    i32p, f32p = P(C.c_int32), P(C.c_float)
+    ctx = C.c_void_p
+    lib.epp_abi_version.restype = C.c_int32
+    lib.epp_device_count.argtypes = [i32p]
+    lib.epp_create.argtypes = [P(abi.epp_config), P(C.c_void_p)]
+    lib.epp_destroy.argtypes = [ctx]
+    lib.epp_last_error.restype = C.c_char_p
+    lib.epp_last_error.argtypes = [ctx]
+    lib.epp_upload.argtypes = [ctx, C.c_int32, i32p, i32p, i32p, C.c_int64, f32p, C.c_int64,
+                               P(abi.epp_column_map)]
+    lib.epp_download.argtypes = [ctx, i32p, i32p, i32p, C.c_int64, f32p, C.c_int64,
+                                 P(abi.epp_column_map)]
+    lib.epp_search.argtypes = [ctx, C.c_int32, C.c_int32, P(abi.epp_physics), C.c_int32]
+    lib.epp_interaction.argtypes = [ctx, C.c_int32, P(abi.epp_physics)]
+    lib.epp_selfaction.argtypes = [ctx, C.c_int32, P(abi.epp_physics)]
+    lib.epp_step.argtypes = [ctx, C.c_int32, P(abi.epp_physics)]
+    lib.epp_get_integrals.argtypes = [ctx, P(abi.epp_physics), P(abi.epp_integrals)]
+    lib.epp_cell_stats.argtypes = [ctx, i32p, i32p, i32p, i32p]
+    lib.epp_synchronize.argtypes = [ctx, P(C.c_uint32)]
+    lib.epp_last_step_timing.argtypes = [ctx, f32p]
+    lib.epp_pairs_total.argtypes = [ctx, P(C.c_int64)]
+    lib.epp_set_accel_output.argtypes = [ctx, C.c_int32]
+    lib.epp_get_accel.argtypes = [ctx, f32p, C.c_int32]
+    lib.epp_set_stream.argtypes = [ctx, C.c_void_p]
+    lib.epp_profile_step.argtypes = [ctx, P(abi.epp_physics), f32p]
+    for name in EXPORTS:
+        if name not in ("epp_last_error", "epp_abi_version"):
+            getattr(lib, name).restype = C.c_int32
+    if lib.epp_abi_version() != abi.EPP_ABI_VERSION:
+        raise ImportError("libepp ABI %d != %d" % (lib.epp_abi_version(), abi.EPP_ABI_VERSION))
+    _lib = lib
+    return lib
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(C.POINTER(t)) if a is not None else None
+
+
+class Context:
+    """One device context (epp_ctx) holding a particle system's state on a GPU."""
+
+    def __init__(self, config):
+        self.lib = load()
+        self.config = config
+        h = C.c_void_p()
+        rc = self.lib.epp_create(C.byref(config), C.byref(h))
+        if rc != abi.EPP_OK:
+            raise EppError(rc, "epp_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.epp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc, what):
+        if rc != abi.EPP_OK:
+            detail = self.lib.epp_last_error(self.h).decode() if self.h else ""
+            raise EppError(rc, what, detail)
+
+    def upload(self, n, is_alive, cell_index, int_props, float_props, cmap):
+        self._ck(self.lib.epp_upload(self.h, n, _ptr(is_alive, C.c_int32), _ptr(cell_index, C.c_int32),
+                                     _ptr(int_props, C.c_int32), int_props.shape[0],
+                                     _ptr(float_props, C.c_float), float_props.shape[0], C.byref(cmap)),
+                 "epp_upload")
+
+    def download(self, is_alive, cell_index, int_props, float_props, cmap):
+        self._ck(self.lib.epp_download(self.h, _ptr(is_alive, C.c_int32), _ptr(cell_index, C.c_int32),
+                                       _ptr(int_props, C.c_int32),
+                                       int_props.shape[0] if int_props is not None else 0,
+                                       _ptr(float_props, C.c_float),
+                                       float_props.shape[0] if float_props is not None else 0,
+                                       C.byref(cmap)), "epp_download")
+
+    def search(self, criterion, action, phys=None, flags=0):
+        self._ck(self.lib.epp_search(self.h, criterion, action,
+                                     C.byref(phys) if phys is not None else None, flags), "epp_search")
+
+    def interaction(self, action, phys=None):
+        self._ck(self.lib.epp_interaction(self.h, action, C.byref(phys) if phys is not None else None),
+                 "epp_interaction")
+
+    def selfaction(self, action, phys=None):
+        self._ck(self.lib.epp_selfaction(self.h, action, C.byref(phys) if phys is not None else None),
+                 "epp_selfaction")
+
+    def step(self, n_steps, phys):
+        self._ck(self.lib.epp_step(self.h, n_steps, C.byref(phys)), "epp_step")
+
+    def integrals(self, phys):
+        out = abi.epp_integrals()
+        self._ck(self.lib.epp_get_integrals(self.h, C.byref(phys), C.byref(out)), "epp_get_integrals")
+        return out.as_dict()
+
+    def cell_stats(self):
+        import numpy as np
+        nc = C.c_int32(0)
+        self._ck(self.lib.epp_cell_stats(self.h, None, None, None, C.byref(nc)), "epp_cell_stats")
+        counts = np.zeros(nc.value, np.int32)
+        offsets = np.zeros(nc.value + 1, np.int32)
+        self._ck(self.lib.epp_cell_stats(self.h, _ptr(counts, C.c_int32), _ptr(offsets, C.c_int32), None,
+                                         C.byref(nc)), "epp_cell_stats")
+        ids = np.zeros(max(int(offsets[-1]), 1), np.int32)
+        self._ck(self.lib.epp_cell_stats(self.h, None, None, _ptr(ids, C.c_int32), C.byref(nc)),
+                 "epp_cell_stats")
+        return counts, offsets, ids[: int(offsets[-1])]
+
+    def synchronize(self, raise_on_status=True):
+        st = C.c_uint32(0)
+        rc = self.lib.epp_synchronize(self.h, C.byref(st))
+        if rc == abi.EPP_ERR_DEVICE_STATUS and not raise_on_status:
+            return st.value
+        self._ck(rc, "epp_synchronize")
+        return st.value
+
+    def last_step_ms(self):
+        v = C.c_float(0)
+        self._ck(self.lib.epp_last_step_timing(self.h, C.byref(v)), "epp_last_step_timing")
+        return v.value
+
+    def pairs_total(self):
+        v = C.c_int64(0)
+        self._ck(self.lib.epp_pairs_total(self.h, C.byref(v)), "epp_pairs_total")
+        return v.value
+
+    def set_accel_output(self, enable):
+        self._ck(self.lib.epp_set_accel_output(self.h, 1 if enable else 0), "epp_set_accel_output")
+
+    def set_stream(self, stream_handle):
+        """Queue work on a caller-owned cudaStream_t (integer handle); None restores the own stream."""
+        self._ck(self.lib.epp_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None),
+                 "epp_set_stream")
+
+    def profile_step(self, phys):
+        """One step kernel by kernel; returns the 5 stage times in ms."""
+        out = (C.c_float * 5)()
+        self._ck(self.lib.epp_profile_step(self.h, C.byref(phys), out), "epp_profile_step")
+        return list(out)
+
+    def accel(self, n, dim):
+        import numpy as np
+        out = np.zeros(dim * n, np.float32)
+        self._ck(self.lib.epp_get_accel(self.h, _ptr(out, C.c_float), n), "epp_get_accel")
+        return out.reshape(dim, n).T.copy()

@@ -182,8 +182,26 @@ int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t*
  * (bits in *device_status, which is then cleared). device_status may be NULL. */
 int32_t epp_synchronize(epp_ctx* ctx, uint32_t* device_status);
 
-/* Per-stage device times of the last epp_step call (ms, CUDA events); n <= 8. */
+/* Device time of the last epp_step call (ms, CUDA events on the context stream). */
 int32_t epp_last_step_timing(epp_ctx* ctx, float* ms_total);
+
+/* Directed active pairs found by all searches of this context so far (the numerator of the
+ * pair-interactions/s metric; each step's search counts its pairs once). */
+int32_t epp_pairs_total(epp_ctx* ctx, int64_t* out);
+
+/* Optional dv/dt output of the fused step (momentum sum + gravity, before integration), for
+ * per-step force comparisons.  epp_get_accel writes out[a * n + row] for a < dim. */
+int32_t epp_set_accel_output(epp_ctx* ctx, int32_t enable);
+int32_t epp_get_accel(epp_ctx* ctx, float* out, int32_t n);
+
+/* Queue the context's work on a caller-owned cudaStream_t (passed as void*; NULL restores the
+ * context's own stream).  Lets a host application order it with its own work and events. */
+int32_t epp_set_stream(epp_ctx* ctx, void* stream);
+
+/* One dam-break step launched kernel by kernel (no graph) with CUDA events between the
+ * kernels; stage_ms[0..4] = momentum+integrate+bin, scan, scatter, rank+gather,
+ * search+continuity.  Same results as epp_step(ctx, 1, phys). */
+int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,290 @@
+"""CUDA path (through the C ABI) against the CPU oracle and the reference's known answers.
+
+Bars: bit-exact for cell counts, offsets, sorted membership, neighbour counts and sets;
+1e-5 relative for FP32 physics (dρ/dt, dv/dt, state) with the error floors stated per test.
+"""
+import numpy as np
+import pytest
+
+from epp import abi, casegen
+from epp.algorithm import DeviceParticleSystem
+from epp.classes import NeighbourSystem
+from helpers import kat, neighbour_sets, nine_particle_system
+from oracle_lib import (ORC_FIELD_ACCEL, ORC_FIELD_DDENSITY, ORC_FIELD_DENSITY, ORC_FIELD_DVELOCITY,
+                        ORC_FIELD_POSITION, ORC_FIELD_PRESSURE, ORC_FIELD_VELOCITY, ORC_FIELD_VOLUME,
+                        Oracle)
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-5
+
+
+def rel_err(a, b, floor):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))) if a.size else 0.0
+
+
+def make_case(dim, dx, max_nb=None):
+    if dim == 2:
+        return casegen.dam_break_2d(dx=dx, max_neighbour_number=max_nb or 40)
+    return casegen.dam_break_3d(dx=dx, tank=(0.6, 0.3, 0.4), column=(0.2, 0.3, 0.24),
+                                max_neighbour_number=max_nb or 100)
+
+
+def pair(case, max_nb):
+    """(device system, oracle) loaded with the same case."""
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=max_nb)
+    dps = DeviceParticleSystem(case.ps, ns)
+    dps.physics = case.physics
+    dps.syncto()
+    o = Oracle(dps.config, 32)
+    ps = case.ps
+    o.upload(ps.n_particles, ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, dps.cmap)
+    return dps, o
+
+
+def gpu_fields(dps):
+    dps.asyncto()
+    ps = dps.host
+    return {
+        "x": ps["PositionVec"], "v": ps["VelocityVec"], "dv": ps["dVelocityVec"],
+        "rho": ps["Density"], "drho": ps["dDensity"], "p": ps["Pressure"], "vol": ps["Volume"],
+        "ncount": ps["nCount"], "alive": ps.is_alive[: ps.n_particles].copy(),
+        "cell": ps.cell_index[: ps.n_particles].copy(),
+    }
+
+
+def oracle_fields(o, n, dim):
+    vec = lambda f: np.stack([o.field(f, a, n) for a in range(dim)], 1)  # noqa: E731
+    return {
+        "x": vec(ORC_FIELD_POSITION), "v": vec(ORC_FIELD_VELOCITY), "dv": vec(ORC_FIELD_DVELOCITY),
+        "rho": o.field(ORC_FIELD_DENSITY, 0, n), "drho": o.field(ORC_FIELD_DDENSITY, 0, n),
+        "p": o.field(ORC_FIELD_PRESSURE, 0, n), "vol": o.field(ORC_FIELD_VOLUME, 0, n),
+    }
+
+
+def test_neighbour_search_golden_gpu():
+    """test/Algorithm/NeighbourSearchTest.jl:67-152 through the C ABI."""
+    ps, ns, k = nine_particle_system()
+    dps = DeviceParticleSystem(ps, ns)
+    dps.syncto()
+    from epp import algorithm as A
+    A.search(dps, A.defaultSearchCriterion, A.defaultSelfaction)
+    A.dynamic_search(dps, A.defaultSearchCriterion, A.defaultSelfaction)
+    dps.asyncto()
+    assert ps["nCount"].tolist() == k["ncount"]
+    assert neighbour_sets(ps) == k["neighbour_sets"]
+
+
+def test_action_golden_gpu():
+    """test/Algorithm/ActionTest.jl:60-85 through the C ABI."""
+    ps, ns, k = nine_particle_system()
+    dps = DeviceParticleSystem(ps, ns)
+    dps.syncto()
+    from epp import algorithm as A
+    A.search(dps)
+    for _ in range(2):
+        A.selfaction(dps, abi.EPP_ACTION_ZERO_DVELOCITY)
+        A.interaction(dps, abi.EPP_ACTION_COUNT_NEIGHBOURS)
+    dps.asyncto()
+    dv = ps["dVelocityVec"]
+    assert dv[:, 0].tolist() == kat()["action"]["counts"]
+    assert dv[:, 1].tolist() == kat()["action"]["counts"]
+
+
+@pytest.mark.parametrize("dim,dx", [(2, 0.04), (3, 0.02)])
+def test_cell_list_bit_exact(dim, dx):
+    """Counts, offsets (exclusive scan) and per-cell membership sorted by id equal the oracle's."""
+    case = make_case(dim, dx)
+    dps, o = pair(case, 40 if dim == 2 else 100)
+    dps.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_NONE, case.physics, 0)
+    o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_NONE, case.physics)
+    dps.ctx.synchronize()
+    gc, go, gi = dps.ctx.cell_stats()
+    oc, oo, oi = o.cell_stats(case.n)
+    assert np.array_equal(gc, oc)
+    assert np.array_equal(go, oo)
+    assert np.array_equal(gi, oi)
+
+
+@pytest.mark.parametrize("dim,dx", [(2, 0.04), (3, 0.02)])
+def test_per_call_step_parity(dim, dx):
+    """main.jl:157-182 call by call: search+continuity, density, momentum, integrate, search."""
+    max_nb = 40 if dim == 2 else 100
+    case = make_case(dim, dx, max_nb)
+    phys = case.physics
+    dps, o = pair(case, max_nb)
+    n = case.n
+    c = dps.ctx
+    c.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, abi.EPP_SEARCH_EMIT_LIST)
+    o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys)
+    c.synchronize()
+    g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+    drho_scale = 1000.0 * phys.c0 / case.meta["h"] * 1e-6
+    assert rel_err(g["drho"], r["drho"], drho_scale) < REL
+    assert np.array_equal(g["ncount"], o.field(9, 0, n).astype(np.int32))
+    # neighbour sets bit-exact (emitted list)
+    ops = make_case(dim, dx, max_nb).ps
+    o.download(ops.is_alive, ops.cell_index, ops.int_properties, ops.float_properties, dps.cmap)
+    assert neighbour_sets(dps.host) == neighbour_sets(ops)
+    for _ in range(2):
+        c.selfaction(abi.EPP_ACTION_DAMBREAK_DENSITY, phys)
+        o.selfaction(abi.EPP_ACTION_DAMBREAK_DENSITY, phys)
+        c.interaction(abi.EPP_ACTION_DAMBREAK_MOMENTUM, phys)
+        o.interaction(abi.EPP_ACTION_DAMBREAK_MOMENTUM, phys)
+        c.synchronize()
+        g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+        assert np.array_equal(g["rho"], r["rho"].astype(np.float32))
+        assert rel_err(g["p"], r["p"], 1.0) < REL
+        assert rel_err(g["vol"], r["vol"], 1e-12) < REL
+        assert rel_err(g["dv"], r["dv"], 9.81) < REL
+        c.selfaction(abi.EPP_ACTION_DAMBREAK_INTEGRATE, phys)
+        o.selfaction(abi.EPP_ACTION_DAMBREAK_INTEGRATE, phys)
+        c.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+        o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys)
+        c.synchronize()
+        g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+        assert rel_err(g["v"], r["v"], 1e-3) < REL
+        assert rel_err(g["x"], r["x"], 1.0) < 1e-6
+        assert rel_err(g["drho"], r["drho"], drho_scale) < REL
+        assert np.array_equal(g["ncount"], o.field(9, 0, n).astype(np.int32))
+
+
+@pytest.mark.parametrize("dim,dx,steps", [(2, 0.04, 20), (3, 0.02, 10)])
+def test_fused_step_parity(dim, dx, steps):
+    """epp_step (fused kernels in a CUDA graph) against the oracle's main.jl loop, step by step."""
+    max_nb = 40 if dim == 2 else 100
+    case = make_case(dim, dx, max_nb)
+    phys = case.physics
+    dps, o = pair(case, max_nb)
+    n = case.n
+    c = dps.ctx
+    c.set_accel_output(True)
+    c.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys)
+    drho_scale = 1000.0 * phys.c0 / case.meta["h"] * 1e-6
+    worst = {}
+    for s in range(steps):
+        c.step(1, phys)
+        o.step(1, phys)
+        c.synchronize()
+        g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+        fluid = case.ps["Tag"] == casegen.FLUID_TAG
+        acc = c.accel(n, dim)
+        racc = np.stack([o.field(ORC_FIELD_ACCEL, a, n) for a in range(dim)], 1)
+        errs = {
+            "accel": rel_err(acc[fluid], racc[fluid], 9.81),
+            "drho": rel_err(g["drho"], r["drho"], drho_scale),
+            "rho": rel_err(g["rho"], r["rho"], 1.0),
+            "v": rel_err(g["v"], r["v"], 1e-2),
+            "x": rel_err(g["x"], r["x"], 1.0),
+        }
+        for k, v in errs.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+        assert np.array_equal(g["ncount"], o.field(9, 0, n).astype(np.int32)), "step %d" % s
+    assert worst["accel"] < REL, worst
+    assert worst["drho"] < REL, worst
+    assert worst["rho"] < REL, worst
+    assert worst["v"] < REL, worst
+    assert worst["x"] < 1e-6, worst
+
+
+def test_fused_matches_per_call():
+    """The fused graph step and the per-call sequence give the same state."""
+    case_a = make_case(2, 0.04)
+    case_b = make_case(2, 0.04)
+    phys = case_a.physics
+    ns = NeighbourSystem(case_a.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=40)
+    a = DeviceParticleSystem(case_a.ps, ns)
+    b = DeviceParticleSystem(case_b.ps, ns)
+    for d in (a, b):
+        d.syncto()
+        d.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    a.ctx.step(5, phys)
+    for _ in range(5):
+        b.ctx.selfaction(abi.EPP_ACTION_DAMBREAK_DENSITY, phys)
+        b.ctx.interaction(abi.EPP_ACTION_DAMBREAK_MOMENTUM, phys)
+        b.ctx.selfaction(abi.EPP_ACTION_DAMBREAK_INTEGRATE, phys)
+        b.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    a.ctx.synchronize()
+    b.ctx.synchronize()
+    ga, gb = gpu_fields(a), gpu_fields(b)
+    for k in ("x", "v", "rho", "drho", "p", "ncount"):
+        assert rel_err(ga[k], gb[k], 1e-3) < 1e-6, k
+
+
+def test_determinism():
+    """Two runs of the same case are bit-identical (within-cell order by particle id)."""
+    outs = []
+    for _ in range(2):
+        case = make_case(2, 0.04)
+        ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=40)
+        d = DeviceParticleSystem(case.ps, ns)
+        d.syncto()
+        d.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, case.physics, 0)
+        d.ctx.step(10, case.physics)
+        d.ctx.synchronize()
+        outs.append(gpu_fields(d))
+    for k in ("x", "v", "rho", "drho"):
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_integrals_fp64():
+    case = make_case(2, 0.04)
+    dps, o = pair(case, 40)
+    phys = case.physics
+    dps.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys)
+    dps.ctx.step(5, phys)
+    o.step(5, phys)
+    gi = dps.ctx.integrals(phys)
+    oi = o.integrals(phys)
+    assert gi["n_alive"] == oi["n_alive"]
+    assert gi["n_pairs"] == oi["n_pairs"]
+    for k in ("mass_total", "mass_fluid", "potential"):
+        assert abs(gi[k] - oi[k]) <= 1e-9 * abs(oi[k]), k
+    assert abs(gi["internal"] - oi["internal"]) <= 1e-4 * abs(oi["internal"]) + 1e-9
+    assert abs(gi["kinetic"] - oi["kinetic"]) <= 1e-4 * abs(oi["kinetic"]) + 1e-12
+
+
+def test_out_of_domain_killed():
+    """NeighbourSearch.jl:41-43: particles outside the domain are killed (is_alive = 0, cell 0)."""
+    case = make_case(2, 0.04)
+    ps = case.ps
+    x = ps["PositionVec"]
+    x[0] = [100.0, 100.0]
+    ps["PositionVec"] = x
+    dps, o = pair(case, 40)
+    dps.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, case.physics, 0)
+    st = dps.ctx.synchronize()
+    assert st & abi.EPP_STATUS_KILLED
+    g = gpu_fields(dps)
+    assert g["alive"][0] == 0 and g["cell"][0] == 0
+    assert g["alive"][1:].min() == 1
+
+
+def test_neighbour_overflow_status():
+    """The reference writes past its columns when a list overflows; the device reports it."""
+    case = make_case(2, 0.04, 40)
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=8)
+    dps = DeviceParticleSystem(case.ps, ns)
+    dps.syncto()
+    dps.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_NONE, case.physics, abi.EPP_SEARCH_EMIT_LIST)
+    st = dps.ctx.synchronize(raise_on_status=False)
+    assert st & abi.EPP_STATUS_NEIGHBOUR_OVERFLOW
+
+
+def test_empty_and_state_errors():
+    case = make_case(2, 0.04)
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS)
+    dps = DeviceParticleSystem(case.ps, ns)
+    from epp.lib import EppError
+    with pytest.raises(EppError):
+        dps.ctx.interaction(abi.EPP_ACTION_DAMBREAK_MOMENTUM, case.physics)
+    dps.ctx.upload(0, case.ps.is_alive, case.ps.cell_index, case.ps.int_properties,
+                   case.ps.float_properties, dps.cmap)
+    dps.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_NONE, case.physics, 0)
+    dps.ctx.synchronize()
+    with pytest.raises(EppError):
+        dps.ctx.search(7, abi.EPP_ACTION_NONE, case.physics, 0)
