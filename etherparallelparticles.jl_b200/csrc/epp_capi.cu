@@ -71,6 +71,9 @@ struct epp_ctx {
     Arena arena;
     State S[2]{};
     int* start[2]{};
+    int* occ[2]{};             // occupied cells of each buffer set (cell order)
+    int* meta[2]{};            // meta[set][0] = number of occupied cells
+    int sms = 148;
     int cur = 0;
     FusedOut tmp{};       // xh/vm/comp of the fused momentum pass
     int* count = nullptr;
@@ -101,6 +104,9 @@ struct epp_ctx {
     epp_physics rpn_phys{};
     int last_crit = EPP_CRITERION_SYMMETRY;
     unsigned adj[kMaxTags]{};
+    int lanes = 0;             // pair-pass family: 0 mask passes, 1 cell-centric, 2..32 lane groups
+    unsigned* mask = nullptr;  // neighbour masks of the last search ([NW * cap])
+    bool mask_valid = false;   // the mask matches the current order, positions and criterion
     // fused step graphs, one per ping-pong parity
     cudaGraphExec_t graph[2]{};
     epp_physics graph_phys{};
@@ -135,8 +141,8 @@ int fail(epp_ctx* c, int code, const char* fmt, ...) {
 #define CK_LAUNCH() CK(cudaGetLastError())
 
 size_t state_bytes(int cap) {
-    // xh, vm, dv, comp (float4) + rho, drho, vol, p, tagm, id, cell (4 B) + rpn (8 B), aligned
-    return (size_t)cap * (4 * 16 + 7 * 4 + 8) + 12 * 256;
+    // xh, vm, dv, comp, rp4 (float4) + rho, drho, vol, p, tagm, id, cell (4 B), aligned
+    return (size_t)cap * (5 * 16 + 7 * 4) + 12 * 256;
 }
 
 size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
@@ -146,11 +152,13 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += 2 * ((size_t)(n_cells + 2) * 4 + 256);          // start[2]
     b += (size_t)cap * 8 * 2 + 512;                      // cs, perm
     b += (size_t)(n_tiles + 1) * 8 + 256;                // scan state
+    b += 2 * ((size_t)(n_cells + 1) * 4 + 256 + 256);    // occ[2], meta[2]
     b += 256 * 3;                                        // status, pairs
     b += (size_t)cap * 4 + 256;                          // ncount
     b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
     b += (size_t)kIntegralBlocks * 8 * 7 + 8 * 8 + 4 * 256;
+    b += (size_t)cap * 4 * (D == 2 ? MaskConf<2>::NW : MaskConf<3>::NW) + 256;   // neighbour masks
     return b + (1 << 20);
 }
 
@@ -169,7 +177,7 @@ void fill_state(Arena& a, State& s, int cap) {
     s.tagm = a.take<int>(cap);
     s.id = a.take<int>(cap);
     s.cell = a.take<int>(cap);
-    s.rpn = a.take<float2>(cap);
+    s.rp4 = a.take<float4>(cap);
 }
 
 PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
@@ -185,6 +193,87 @@ PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
     return A;
 }
 
+int lanes_of(const epp_ctx* ctx) { return ctx->lanes; }
+
+// A mask pass (one thread per particle).  BUILD: filter (and store the mask if `store`).
+template <int D, bool BUILD, class Act, bool EPI = false>
+int launch_pass(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs, bool store) {
+    PairArgs A = pair_args(ctx, set, crit);
+    MaskArgs M{store || !BUILD ? ctx->mask : nullptr, ctx->cap};
+    k_pass<D, BUILD, Act, EPI><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
+                                                                          ctx->n_tiles + 1);
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+// Launch a G-lane pair pass over `groups` particles (G from the context's tuning).
+template <int D, class Act, bool EPI>
+int launch_pair_g(epp_ctx* ctx, const PairArgs& A, const Act& act, unsigned long long* pairs, long long groups) {
+    const int G = lanes_of(ctx);
+    const int nw = ctx->n_tiles + 1;
+#define EPP_G(GG)                                                                                 \
+    case GG:                                                                                      \
+        k_pair_g<D, GG, Act, EPI><<<blocks_for(groups * GG), kThreads, 0, ctx->stream>>>(          \
+            A, act, pairs, ctx->scan_state, nw);                                                  \
+        break;
+    switch (G) {
+        EPP_G(2)
+        EPP_G(4)
+        EPP_G(8)
+        EPP_G(16)
+        EPP_G(32)
+        default:
+            return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "lanes per particle %d not in {2,4,8,16,32}", G);
+    }
+#undef EPP_G
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+// Persistent grid of a cell-pair kernel: resident blocks per SM x SMs (computed once per
+// instantiation, with the dynamic shared memory opt-in set outside any graph capture).
+template <int D, class Act, bool EPI>
+int cellpair_grid(epp_ctx* ctx) {   // -1 on a CUDA error (recorded in the context)
+    static int grid = 0;
+    if (grid) return grid;
+    const size_t smem = sizeof(CPShared<D>) * kCPWarps;
+    cudaError_t e = cudaFuncSetAttribute(k_cellpair<D, Act, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    int per_sm = 0;
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cellpair<D, Act, EPI>, kCPWarps * 32, smem);
+    if (e != cudaSuccess) {
+        fail(ctx, EPP_ERR_CUDA, "cell-pair kernel setup: %s", cudaGetErrorString(e));
+        return -1;
+    }
+    grid = (per_sm > 0 ? per_sm : 1) * ctx->sms;
+    return grid;
+}
+
+template <int D, class Act, bool EPI = false>
+int launch_cellpair(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs) {
+    CellArgs CA{pair_args(ctx, set, crit), ctx->occ[set], ctx->meta[set]};
+    const int grid = cellpair_grid<D, Act, EPI>(ctx);
+    if (grid < 0) return EPP_ERR_CUDA;
+    const size_t smem = sizeof(CPShared<D>) * kCPWarps;
+    k_cellpair<D, Act, EPI><<<grid, kCPWarps * 32, smem, ctx->stream>>>(CA, act, pairs, ctx->scan_state,
+                                                                         ctx->n_tiles + 1);
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+template <int D>
+int prepare_kernels(epp_ctx* ctx) {
+    int g = 0;
+    g |= cellpair_grid<D, CPCont<D, true>, false>(ctx) < 0;
+    g |= cellpair_grid<D, CPCont<D, false>, false>(ctx) < 0;
+    g |= cellpair_grid<D, CPCount<D>, false>(ctx) < 0;
+    g |= cellpair_grid<D, CPCountDv<D>, false>(ctx) < 0;
+    g |= cellpair_grid<D, CPMom<D, true>, true>(ctx) < 0;
+    g |= cellpair_grid<D, CPMom<D, false>, false>(ctx) < 0;
+    return g ? EPP_ERR_CUDA : EPP_OK;
+}
+
 // clean! + insert (bin, count, scan, scatter, rank-by-id gather) from set `from` into 1-from.
 template <int D>
 int sort_cells(epp_ctx* ctx) {
@@ -195,11 +284,13 @@ int sort_cells(epp_ctx* ctx) {
         ctx->scan_state, ctx->n_tiles + 1);
     CK_LAUNCH();
     k_scan<<<ctx->n_tiles, kScanThreads, 0, ctx->stream>>>(ctx->n_cells + 1, ctx->count, ctx->start[to],
-                                                          ctx->scan_state, ctx->status);
+                                                          ctx->occ[to], ctx->meta[to], ctx->scan_state,
+                                                          ctx->status);
     CK_LAUNCH();
     k_scatter<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->cs, ctx->start[to], ctx->S[from].id,
                                                            ctx->perm, ctx->status);
     CK_LAUNCH();
+    ctx->mask_valid = false;
     MoverAll mv{ctx->S[from], ctx->S[to]};
     k_rank_gather<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->perm, ctx->cs,
                                                                ctx->start[to], mv, ctx->status);
@@ -232,21 +323,45 @@ int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_ph
                        bool fused) {
     PairArgs A = pair_args(ctx, set, crit);
     DevPhys P = phys ? to_dev(*phys) : DevPhys{};
-    const int grid = blocks_for(ctx->n);
     const bool cont = action == EPP_ACTION_DAMBREAK_CONTINUITY;
-#define EPP_SEARCH_LAUNCH(E, C, F)                                                              \
-    do {                                                                                        \
-        ActSearch<D, E, C, F> act{ctx->S[set], ctx->L, P, ctx->ncount, ctx->status};            \
-        k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, ctx->pairs);                      \
-    } while (0)
-    if (fused) EPP_SEARCH_LAUNCH(false, true, true);
-    else if (emit && cont) EPP_SEARCH_LAUNCH(true, true, false);
-    else if (emit) EPP_SEARCH_LAUNCH(true, false, false);
-    else if (cont) EPP_SEARCH_LAUNCH(false, true, false);
-    else EPP_SEARCH_LAUNCH(false, false, false);
-#undef EPP_SEARCH_LAUNCH
-    CK_LAUNCH();
-    return EPP_OK;
+    if (emit) {
+        ctx->mask_valid = false;
+        // the emitted list keeps the reference's neighbour order: one thread per particle
+        const int grid = blocks_for(ctx->n);
+        if (cont) {
+            ActSearch<D, true, true, false> act{ctx->S[set], ctx->L, P, ctx->ncount, ctx->status};
+            k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, ctx->pairs);
+        } else {
+            ActSearch<D, true, false, false> act{ctx->S[set], ctx->L, P, ctx->ncount, ctx->status};
+            k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, ctx->pairs);
+        }
+        CK_LAUNCH();
+        return EPP_OK;
+    }
+    if (ctx->lanes == 0) {
+        int rc;
+        if (fused) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs, true);
+        else if (cont) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncount}, ctx->pairs, true);
+        else rc = launch_pass<D, true>(ctx, set, crit, CPCount<D>{ctx->ncount}, ctx->pairs, true);
+        ctx->mask_valid = rc == EPP_OK;
+        return rc;
+    }
+    ctx->mask_valid = false;
+    if (ctx->lanes >= 2) {   // lane-group kernels (tuning alternative)
+        if (fused) {
+            ActContG<D, true, true> act{ctx->S[set], P, ctx->ncount};
+            return launch_pair_g<D, decltype(act), false>(ctx, A, act, ctx->pairs, ctx->n);
+        }
+        if (cont) {
+            ActContG<D, true, false> act{ctx->S[set], P, ctx->ncount};
+            return launch_pair_g<D, decltype(act), false>(ctx, A, act, ctx->pairs, ctx->n);
+        }
+        ActContG<D, false, false> act{ctx->S[set], P, ctx->ncount};
+        return launch_pair_g<D, decltype(act), false>(ctx, A, act, ctx->pairs, ctx->n);
+    }
+    if (fused) return launch_cellpair<D>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+    if (cont) return launch_cellpair<D>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+    return launch_cellpair<D>(ctx, set, crit, CPCount<D>{ctx->ncount}, ctx->pairs);
 }
 
 template <int D>
@@ -281,7 +396,7 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     const int to = 1 - c;
     const int n = ctx->n;
     PairArgs A = pair_args(ctx, c, EPP_CRITERION_SYMMETRY);
-    ActMomentum<D, true> mom;
+    ActMomG<D, true> mom;
     mom.s = ctx->S[c];
     mom.P = to_dev(phys);
     mom.dom = ctx->dom;
@@ -289,11 +404,18 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     mom.F.n = n;
     mom.F.accel = ctx->graph_accel ? ctx->accel : nullptr;
     mom.status = ctx->status;
-    k_momentum_fused<D><<<blocks_for(n), kThreads, 0, ctx->stream>>>(A, mom);
-    CK_LAUNCH();
+    {
+        int rc0 = ctx->lanes >= 2 ? launch_pair_g<D, ActMomG<D, true>, true>(ctx, A, mom, nullptr, n)
+                  : ctx->lanes == 1 ? launch_cellpair<D, CPMom<D, true>, true>(ctx, c, EPP_CRITERION_SYMMETRY,
+                                                                               CPMom<D, true>{mom}, nullptr)
+                                    : launch_pass<D, false, CPMom<D, true>, true>(ctx, c, EPP_CRITERION_SYMMETRY,
+                                                                                  CPMom<D, true>{mom}, nullptr, false);
+        if (rc0) return rc0;
+    }
     EPP_MARK(1);
     k_scan<<<ctx->n_tiles, kScanThreads, 0, ctx->stream>>>(ctx->n_cells + 1, ctx->count, ctx->start[to],
-                                                          ctx->scan_state, ctx->status);
+                                                          ctx->occ[to], ctx->meta[to], ctx->scan_state,
+                                                          ctx->status);
     CK_LAUNCH();
     EPP_MARK(2);
     k_scatter<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->cs, ctx->start[to], ctx->S[c].id,
@@ -311,6 +433,16 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     EPP_MARK(5);
 #undef EPP_MARK
     return EPP_OK;
+}
+
+// The fused momentum pass reads the neighbour mask of the last search: rebuild it (count-only
+// search pass at the current positions) when the last search did not leave one.
+template <int D>
+int ensure_mask(epp_ctx* ctx) {
+    if (ctx->lanes != 0 || ctx->mask_valid) return EPP_OK;
+    int rc = launch_pass<D, true>(ctx, ctx->cur, EPP_CRITERION_SYMMETRY, CPCount<D>{ctx->ncount}, nullptr, true);
+    if (rc == EPP_OK) ctx->mask_valid = true;
+    return rc;
 }
 
 template <int D>
@@ -340,7 +472,8 @@ template <int D>
 int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
     DevPhys P = phys ? to_dev(*phys) : DevPhys{};
     k_self<D><<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(action, ctx->start[ctx->cur], ctx->n_cells,
-                                                                ctx->n, ctx->S[ctx->cur], P, ctx->status);
+                                                                ctx->n, ctx->S[ctx->cur], P, ctx->status,
+                                                                ctx->accel);
     CK_LAUNCH();
     return EPP_OK;
 }
@@ -348,21 +481,30 @@ int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
 template <int D>
 int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
     PairArgs A = pair_args(ctx, ctx->cur, ctx->last_crit);
-    const int grid = blocks_for(ctx->n);
     if (action == EPP_ACTION_DAMBREAK_MOMENTUM) {
-        ActMomentum<D, false> act;
+        k_prep_rp4<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(ctx->start[ctx->cur], ctx->n_cells, ctx->n,
+                                                                      ctx->S[ctx->cur]);
+        CK_LAUNCH();
+        ActMomG<D, false> act;
         act.s = ctx->S[ctx->cur];
         act.P = to_dev(*phys);
         act.dom = ctx->dom;
         act.F = FusedOut{};
         act.status = ctx->status;
-        k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, nullptr);
-    } else {
-        ActCount<D> act{ctx->S[ctx->cur]};
-        k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, nullptr);
+        if (ctx->lanes >= 2) return launch_pair_g<D, decltype(act), false>(ctx, A, act, nullptr, ctx->n);
+        if (ctx->lanes == 1) return launch_cellpair<D>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false>{act}, nullptr);
+        if (ctx->mask_valid)
+            return launch_pass<D, false>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false>{act}, nullptr, false);
+        return launch_pass<D, true>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false>{act}, nullptr, false);
     }
-    CK_LAUNCH();
-    return EPP_OK;
+    if (ctx->lanes >= 2) {
+        ActCountG<D> act{ctx->S[ctx->cur]};
+        return launch_pair_g<D, decltype(act), false>(ctx, A, act, nullptr, ctx->n);
+    }
+    if (ctx->lanes == 1) return launch_cellpair<D>(ctx, ctx->cur, ctx->last_crit, CPCountDv<D>{ctx->S[ctx->cur]}, nullptr);
+    if (ctx->mask_valid)
+        return launch_pass<D, false>(ctx, ctx->cur, ctx->last_crit, CPCountDv<D>{ctx->S[ctx->cur]}, nullptr, false);
+    return launch_pass<D, true>(ctx, ctx->cur, ctx->last_crit, CPCountDv<D>{ctx->S[ctx->cur]}, nullptr, false);
 }
 
 template <int D>
@@ -386,6 +528,9 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
             ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], to_dev(phys));
         CK_LAUNCH();
     }
+    if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->mask_valid = false;
+    rc = ensure_mask<D>(ctx);
+    if (rc) return rc;
     if (!ctx->graph[0] || !same_phys(ctx->graph_phys, phys) || ctx->graph_accel != accel) {
         ctx->graph_accel = accel;
         rc = build_graphs<D>(ctx, phys);
@@ -400,6 +545,7 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     ctx->searched = true;
     ctx->lists_valid = false;
     ctx->last_crit = EPP_CRITERION_SYMMETRY;
+    ctx->mask_valid = ctx->lanes == 0;
     return EPP_OK;
 }
 
@@ -502,6 +648,10 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->count = a.take<int>(ctx->n_cells + 2);
     ctx->start[0] = a.take<int>(ctx->n_cells + 2);
     ctx->start[1] = a.take<int>(ctx->n_cells + 2);
+    ctx->occ[0] = a.take<int>(ctx->n_cells + 1);
+    ctx->occ[1] = a.take<int>(ctx->n_cells + 1);
+    ctx->meta[0] = a.take<int>(64);
+    ctx->meta[1] = a.take<int>(64);
     ctx->cs = a.take<int2>(ctx->cap);
     ctx->perm = a.take<int2>(ctx->cap);
     ctx->scan_state = a.take<unsigned long long>(ctx->n_tiles + 1);
@@ -515,6 +665,7 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->iticket = a.take<unsigned>(1);
     ctx->ihpart = a.take<double>(kIntegralBlocks);
     ctx->ihmin = a.take<double>(1);
+    ctx->mask = a.take<unsigned>((size_t)ctx->cap * (D == 2 ? MaskConf<2>::NW : MaskConf<3>::NW));
     ctx->tmp.count = ctx->count;
     ctx->tmp.cs = ctx->cs;
     ctx->tmp.scan_state = ctx->scan_state;
@@ -527,6 +678,11 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     if (cudaMemsetAsync(ctx->arena.base, 0, need, ctx->stream) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        epp_destroy(ctx);
+        return EPP_ERR_CUDA;
+    }
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->dev);
+    if ((D == 2 ? prepare_kernels<2>(ctx) : prepare_kernels<3>(ctx)) != EPP_OK) {
         epp_destroy(ctx);
         return EPP_ERR_CUDA;
     }
@@ -623,6 +779,7 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     CK_LAUNCH();
     ctx->searched = false;
     ctx->sorted_once = false;
+    ctx->mask_valid = false;
     ctx->lists_valid = false;
     ctx->rpn_valid = false;
     ctx->dv_dirty = true;
@@ -757,6 +914,7 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (ctx->n == 0) return EPP_OK;
     int rc = ctx->D == 2 ? run_selfaction<2>(ctx, action, phys) : run_selfaction<3>(ctx, action, phys);
     if (action == EPP_ACTION_DAMBREAK_INTEGRATE) {
+        ctx->mask_valid = false;
         ctx->searched = false;   // positions moved: the next pass needs a search!
         ctx->rpn_valid = false;
     }
@@ -879,6 +1037,23 @@ int32_t epp_pairs_total(epp_ctx* ctx, int64_t* out) {
     return EPP_OK;
 }
 
+int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    const int g = lanes_per_particle;
+    if (g != 0 && g != 1 && g != 2 && g != 4 && g != 8 && g != 16 && g != 32)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pair-pass family %d not in {0,1,2,4,8,16,32}", g);
+    if (g != ctx->lanes) {
+        ctx->lanes = g;
+        ctx->mask_valid = false;
+        for (int c = 0; c < 2; ++c)
+            if (ctx->graph[c]) {
+                cudaGraphExecDestroy(ctx->graph[c]);
+                ctx->graph[c] = nullptr;
+            }
+    }
+    return EPP_OK;
+}
+
 int32_t epp_set_stream(epp_ctx* ctx, void* stream) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
@@ -901,6 +1076,11 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
             ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], to_dev(*phys));
         CK_LAUNCH();
     }
+    if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->mask_valid = false;
+    {
+        int rc0 = ctx->D == 2 ? ensure_mask<2>(ctx) : ensure_mask<3>(ctx);
+        if (rc0) return rc0;
+    }
     cudaEvent_t ev[6];
     for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
     int rc = ctx->D == 2 ? enqueue_fused_step<2>(ctx, ctx->cur, *phys, ev)
@@ -910,6 +1090,7 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
         ctx->rpn_valid = true;
         ctx->rpn_phys = *phys;
         ctx->lists_valid = false;
+        ctx->mask_valid = ctx->lanes == 0;
         cudaError_t e = cudaEventSynchronize(ev[5]);
         for (int k = 0; k < 5 && e == cudaSuccess; ++k) e = cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
         if (e != cudaSuccess) rc = fail(ctx, EPP_ERR_CUDA, "profile events: %s", cudaGetErrorString(e));

@@ -1,0 +1,430 @@
+// epp_cellpair.cuh -- cell-centric pair passes: one warp per occupied cell.
+//
+// All particles of a cell share the same 3^D stencil, whose cells form 3 (2D) or 9 (3D) rows
+// that are contiguous in cell-sorted order.  A warp stages those candidates in shared memory
+// with coalesced 16-byte loads, filters every (target, candidate) pair of the cell with the
+// reference's IEEE criterion (so the neighbour sets stay bit-exact), and compacts the accepted
+// pairs into a per-warp queue.  The pair arithmetic then runs on full warps, 32 pairs at a time,
+// and each window is folded into the targets' accumulators by a segmented shuffle scan over runs
+// of the same target -- a fixed order, so results are deterministic.  This replaces the
+// thread-per-particle loop in which only about a third of the lanes had a neighbour at any time.
+#pragma once
+#include "epp_pair_g.cuh"
+
+namespace epp {
+
+constexpr int kCPWarps = 4;       // warps per block
+constexpr int kCPQueue = 64;      // queue ring (entries)
+
+template <int D>
+struct CPConf {
+    static constexpr int C = D == 2 ? 192 : 512;   // staged candidates per chunk
+    static constexpr int T = 64;                    // targets per batch
+};
+
+struct CellArgs {
+    PairArgs A;
+    const int* occ;      // occupied cells (cell order)
+    const int* meta;     // meta[0] = number of occupied cells
+};
+
+struct TargetConst {   // per target: h, invharmonic(h,h), dW/r factor, 1/hinv, (2 harmonic(h,h))^2
+    float h, hinv, kdw, hh;
+    float h2sq;
+};
+
+template <int D>
+struct CPShared {
+    float4 cx[CPConf<D>::C];     // staged candidate (x, h)
+    int cj[CPConf<D>::C];        // staged candidate index
+    int ct[CPConf<D>::C];        // staged candidate tag
+    int queue[kCPQueue];         // (t << 16) | k
+    float4 acc[CPConf<D>::T];    // per-target sums
+    int cnt[CPConf<D>::T];       // per-target accepted pairs
+    TargetConst tc[CPConf<D>::T];
+};
+
+template <int D>
+__device__ __forceinline__ TargetConst target_const(float h) {
+    TargetConst c;
+    c.h = h;
+    c.hinv = invharmonic_exact(h, h);
+    c.kdw = wc2_kdw<D>(c.hinv);
+    c.hh = __fdiv_rn(1.0f, c.hinv);
+    const float h2 = harmonic2_exact(h, h);
+    c.h2sq = __fmul_rn(h2, h2);
+    return c;
+}
+
+// Geometry of a pair for the contribution functions.
+struct PairGeo {
+    float dx, dy, dz, dr2;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Continuity (search! action of main.jl:74-90) as a per-pair contribution.
+template <int D, bool FUSED>
+struct CPCont {
+    State s;
+    DevPhys P;
+    int* ncount;
+    static constexpr int NC = 1;
+    __device__ __forceinline__ bool wants(int) const { return true; }
+    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
+                                              const PairGeo& g, const TargetConst& tc) const {
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const bool ff = ti == P.fluid && tj == P.fluid;
+        const bool fw = ti == P.fluid && tj == P.wall;
+        const bool wf = ti == P.wall && tj == P.fluid;
+        if (!(ff || fw || wf)) return out;
+        const float r = sqrtf(g.dr2);
+        float hinv, kdw;
+        if (xj.w == tc.h) {
+            hinv = tc.hinv;
+            kdw = tc.kdw;
+        } else {
+            hinv = invharmonic_exact(tc.h, xj.w);
+            kdw = wc2_kdw<D>(hinv);
+        }
+        const float q = r * hinv;
+        if (!(q < 2.0f)) return out;     // W = dW = 0 at q >= 2 (WendlandC2.jl:23,44)
+        const float u = 2.0f - q;
+        const float dwr = kdw * (u * u * u);
+        const float4 vi = s.vm[i];
+        const float4 vj = s.vm[j];
+        float vdx = g.dx * (vi.x - vj.x);
+        vdx += g.dy * (vi.y - vj.y);
+        if (D == 3) vdx += g.dz * (vi.z - vj.z);
+        if (ff) out.x = vj.w * vdx * dwr;                       // iClassicContinuity!
+        else out.x = s.rho[i] * s.vol[j] * vdx * dwr;           // iBalancedContinuity!
+        return out;
+    }
+    __device__ __forceinline__ void end(int i, int ti, float4 sum, int cnt) const {
+        ncount[i] = cnt;
+        const float rho_i = s.rho[i];
+        const float drho = FUSED ? sum.x : s.drho[i] + sum.x;
+        s.drho[i] = drho;
+        if (ti == P.fluid || ti == P.wall) {
+            const float rho = __fadd_rn(rho_i, __fmul_rn(drho, P.dt));
+            s.rp4[i] = make_rp4(rho, eos(P, rho));
+        } else {
+            s.rp4[i] = make_rp4(rho_i, s.p[i]);
+        }
+    }
+    __device__ __forceinline__ void end_idle(int i, int ti) const { end(i, ti, make_float4(0, 0, 0, 0), 0); }
+};
+
+// Count only (search! without an action).
+template <int D>
+struct CPCount {
+    int* ncount;
+    static constexpr int NC = 0;
+    __device__ __forceinline__ bool wants(int) const { return true; }
+    __device__ __forceinline__ float4 contrib(int, int, int, int, float4, float4, const PairGeo&,
+                                              const TargetConst&) const {
+        return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    __device__ __forceinline__ void end(int i, int, float4, int cnt) const { ncount[i] = cnt; }
+    __device__ __forceinline__ void end_idle(int i, int) const { ncount[i] = 0; }
+};
+
+// interaction! test action: dVelocity += 1 per neighbour (ActionTest.jl:71-75).
+template <int D>
+struct CPCountDv {
+    State s;
+    static constexpr int NC = 0;
+    __device__ __forceinline__ bool wants(int) const { return true; }
+    __device__ __forceinline__ float4 contrib(int, int, int, int, float4, float4, const PairGeo&,
+                                              const TargetConst&) const {
+        return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    __device__ __forceinline__ void end(int i, int, float4, int cnt) const {
+        float4 d = s.dv[i];
+        d.x += (float)cnt;
+        d.y += (float)cnt;
+        if (D == 3) d.z += (float)cnt;
+        s.dv[i] = d;
+    }
+    __device__ __forceinline__ void end_idle(int, int) const {}
+};
+
+// Momentum (interaction! of main.jl:107-118) as a per-pair contribution; FUSED adds the
+// integrate + bin epilogue of the fused step.
+template <int D, bool FUSED>
+struct CPMom {
+    ActMomG<D, FUSED> m;   // state, physics, fused outputs, integrate_and_bin
+    static constexpr int NC = 3;
+    __device__ __forceinline__ bool wants(int ti) const { return ti == m.P.fluid; }
+    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
+                                              const PairGeo& g, const TargetConst& tc) const {
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const DevPhys& P = m.P;
+        const bool ff = tj == P.fluid;
+        const bool fw = tj == P.wall;
+        if (!(ff || fw)) return out;
+        const float r = sqrtf(g.dr2);
+        float hinv, kdw, hh;
+        if (xj.w == tc.h) {
+            hinv = tc.hinv;
+            kdw = tc.kdw;
+            hh = tc.hh;
+        } else {
+            hinv = invharmonic_exact(tc.h, xj.w);
+            kdw = wc2_kdw<D>(hinv);
+            hh = __fdividef(1.0f, hinv);
+        }
+        const float q = r * hinv;
+        if (!(q < 2.0f)) return out;
+        const float u = 2.0f - q;
+        const float dwr = kdw * (u * u * u);
+        const float4 rpi = m.s.rp4[i];
+        const float4 rpj = m.s.rp4[j];
+        const float4 vi = m.s.vm[i];
+        const float4 vj = m.s.vm[j];
+        const float p_rho_2 = ff ? rpi.z + rpj.z : (rpi.y + rpj.y) * rpi.w * rpj.w;
+        const float fp = p_rho_2 * (-vj.w * dwr);
+        out.x = fp * g.dx;
+        out.y = fp * g.dy;
+        if (D == 3) out.z = fp * g.dz;
+        float vdx = g.dx * (vi.x - vj.x);
+        vdx += g.dy * (vi.y - vj.y);
+        if (D == 3) vdx += g.dz * (vi.z - vj.z);
+        if (vdx < 0.0f) {
+            const float rhob = 0.5f * (rpi.x + rpj.x);
+            const float az = g.dr2 + 0.01f * hh * hh;
+            const float phi = __fdividef(vdx, hinv * az);
+            float force = __fdividef((-P.alpha * P.c0 + P.beta * phi) * phi, rhob);
+            if (P.visc == EPP_VISCOSITY_REFERENCE) force *= (-vj.w * rpi.w * rpj.w) * dwr;
+            else force *= -vj.w * dwr;
+            out.x += force * g.dx;
+            out.y += force * g.dy;
+            if (D == 3) out.z += force * g.dz;
+        }
+        return out;
+    }
+    __device__ __forceinline__ void end(int i, int ti, float4 sum, int) const {
+        typename ActMomG<D, FUSED>::Acc a;
+        a.du[0] = sum.x;
+        a.du[1] = sum.y;
+        a.du[2] = sum.z;
+        m.end(i, ti, a);
+    }
+    __device__ __forceinline__ void end_idle(int i, int ti) const {
+        if (FUSED) m.integrate_and_bin(i, ti, nullptr);
+    }
+};
+
+// Segmented inclusive scan over runs of equal key (keys are non-decreasing across lanes).
+__device__ __forceinline__ float seg_scan(float v, int key, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float up = __shfl_up_sync(0xffffffffu, v, o);
+        const int kup = __shfl_up_sync(0xffffffffu, key, o);
+        if (lane >= o && kup == key) v += up;
+    }
+    return v;
+}
+
+template <int D, class Act>
+__device__ __forceinline__ void cp_window(const CellArgs& CA, const Act& act, CPShared<D>& S,
+                                          int qhead, int nq, int tbase, int lane) {
+    const int e = lane < nq ? S.queue[(qhead + lane) & (kCPQueue - 1)] : -1;
+    const int t = e >= 0 ? (e >> 16) : 0x7fffffff;
+    float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (e >= 0 && Act::NC > 0) {
+        const int k = e & 0xffff;
+        const int i = tbase + t;
+        const int j = S.cj[k];
+        const float4 xj = S.cx[k];
+        const int tj = S.ct[k];
+        const float4 xi = CA.A.s.xh[i];
+        const int ti = tag_of(CA.A.s.tagm[i]);
+        PairGeo g;
+        g.dx = __fsub_rn(xi.x, xj.x);
+        g.dy = __fsub_rn(xi.y, xj.y);
+        g.dz = D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f;
+        g.dr2 = __fadd_rn(__fmul_rn(g.dx, g.dx), __fmul_rn(g.dy, g.dy));
+        if (D == 3) g.dr2 = __fadd_rn(g.dr2, __fmul_rn(g.dz, g.dz));
+        c = act.contrib(i, j, ti, tj, xi, xj, g, S.tc[t]);
+    }
+    if (Act::NC > 0) {
+        const int key = t;
+        const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+        const bool last = e >= 0 && (lane == 31 || knext != key);
+        c.x = seg_scan(c.x, key, lane);
+        if (Act::NC > 1) {
+            c.y = seg_scan(c.y, key, lane);
+            c.z = seg_scan(c.z, key, lane);
+        }
+        if (last) {
+            float4 a = S.acc[t];
+            a.x += c.x;
+            if (Act::NC > 1) {
+                a.y += c.y;
+                a.z += c.z;
+            }
+            S.acc[t] = a;
+        }
+    }
+    __syncwarp();
+}
+
+// The cell-pair kernel.  Persistent: warps stride over the occupied cells.  EPI (fused momentum):
+// block 0 clears the scan state and the dead bin gets the integrate + bin epilogue.
+template <int D, class Act, bool EPI>
+__global__ void __launch_bounds__(kCPWarps * 32, 4) k_cellpair(CellArgs CA, Act act, unsigned long long* pairs,
+                                                            unsigned long long* scan_state,
+                                                            int n_scan_words) {
+    extern __shared__ __align__(16) unsigned char cp_smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    CPShared<D>& S = reinterpret_cast<CPShared<D>*>(cp_smem)[warp];
+    if (EPI && blockIdx.x == 0)
+        for (int t = threadIdx.x; t < n_scan_words; t += blockDim.x) scan_state[t] = 0ull;
+    const PairArgs& A = CA.A;
+    const int n_occ = CA.meta[0];
+    const int n_alive = min(A.start[A.dom.n_cells], A.n_max);
+    const int nwarps = gridDim.x * kCPWarps;
+    const int n0 = A.dom.n[0], n1 = A.dom.n[1];
+    unsigned long long my_pairs = 0;
+    unsigned st = 0;
+    for (int oc = blockIdx.x * kCPWarps + warp; oc < n_occ; oc += nwarps) {
+        const int c = CA.occ[oc];
+        const int cs0 = max(A.start[c], 0);
+        const int cs1 = min(A.start[c + 1], n_alive);
+        const int cx = c % n0, cy = (c / n0) % n1, cz = D == 3 ? c / (n0 * n1) : 0;
+        const int x0 = max(cx - 1, 0), x1 = min(cx + 1, n0 - 1);
+        const int y0 = max(cy - 1, 0), y1 = min(cy + 1, n1 - 1);
+        const int z0 = D == 3 ? max(cz - 1, 0) : 0, z1 = D == 3 ? min(cz + 1, A.dom.n[2] - 1) : 0;
+        for (int tb = cs0; tb < cs1; tb += CPConf<D>::T) {
+            const int TB = min(CPConf<D>::T, cs1 - tb);
+            for (int t = lane; t < TB; t += 32) {
+                S.acc[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                S.cnt[t] = 0;
+                S.tc[t] = target_const<D>(A.s.xh[tb + t].w);
+            }
+            __syncwarp();
+            int qhead = 0, qtail = 0;
+            int KC = 0;
+            // rows of the stencil, staged chunk by chunk
+            int zz = z0, yy = y0;
+            int pos = max(A.start[n0 * (yy + n1 * zz) + x0], 0);
+            int hi = min(A.start[n0 * (yy + n1 * zz) + x1 + 1], A.n_max);
+            bool rows_left = true;
+            while (rows_left) {
+                // fill the chunk
+                while (rows_left && KC < CPConf<D>::C) {
+                    const int piece = max(0, min(hi - pos, CPConf<D>::C - KC));
+                    for (int k = lane; k < piece; k += 32) {
+                        const int j = pos + k;
+                        S.cj[KC + k] = j;
+                        S.cx[KC + k] = A.s.xh[j];
+                        S.ct[KC + k] = tag_of(A.s.tagm[j]);
+                    }
+                    KC += piece;
+                    pos += piece;
+                    if (piece == 0 || pos >= hi) {
+                        if (++yy > y1) {
+                            yy = y0;
+                            if (++zz > z1) rows_left = false;
+                        }
+                        if (rows_left) {
+                            pos = max(A.start[n0 * (yy + n1 * zz) + x0], 0);
+                            hi = min(A.start[n0 * (yy + n1 * zz) + x1 + 1], A.n_max);
+                        }
+                    }
+                }
+                __syncwarp();
+                // filter every target of the batch against the chunk
+                for (int t = 0; t < TB; ++t) {
+                    const int i = tb + t;
+                    const float4 xi = A.s.xh[i];
+                    const int ti = tag_of(A.s.tagm[i]);
+                    if (ti < 1 || ti > A.n_tags) {
+                        st |= EPP_STATUS_BAD_TAG;
+                        continue;
+                    }
+                    if (!act.wants(ti)) continue;
+                    const unsigned amask = A.adj[ti - 1];
+                    const float h2sq = S.tc[t].h2sq;
+                    int added = 0;
+                    for (int k0 = 0; k0 < KC; k0 += 32) {
+                        const int k = k0 + lane;
+                        bool ok = false;
+                        if (k < KC) {
+                            const int j = S.cj[k];
+                            if (j != i) {
+                                const float4 xj = S.cx[k];
+                                const float dx = __fsub_rn(xi.x, xj.x);
+                                const float dy = __fsub_rn(xi.y, xj.y);
+                                float dr2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                                if (D == 3) {
+                                    const float dz = __fsub_rn(xi.z, xj.z);
+                                    dr2 = __fadd_rn(dr2, __fmul_rn(dz, dz));
+                                }
+                                if (A.crit == EPP_CRITERION_DEFAULT) {
+                                    ok = dr2 <= A.dom.gap_square;
+                                } else if (xj.w == xi.w) {
+                                    ok = dr2 <= h2sq;
+                                } else {
+                                    const float h2 = harmonic2_exact(xi.w, xj.w);
+                                    ok = dr2 <= __fmul_rn(h2, h2);
+                                }
+                                if (ok) {
+                                    const int tj = S.ct[k];
+                                    if (tj < 1 || tj > A.n_tags) {
+                                        st |= EPP_STATUS_BAD_TAG;
+                                        ok = false;
+                                    } else {
+                                        ok = (amask >> (tj - 1)) & 1u;
+                                    }
+                                }
+                            }
+                        }
+                        const unsigned mask = __ballot_sync(0xffffffffu, ok);
+                        if (ok) {
+                            const int slot = qtail + __popc(mask & ((1u << lane) - 1u));
+                            S.queue[slot & (kCPQueue - 1)] = (t << 16) | k;
+                        }
+                        const int nadd = __popc(mask);
+                        qtail += nadd;
+                        added += nadd;
+                        __syncwarp();
+                        if (qtail - qhead >= 32) {
+                            cp_window<D>(CA, act, S, qhead, 32, tb, lane);
+                            qhead += 32;
+                        }
+                    }
+                    if (lane == 0) S.cnt[t] += added;
+                    my_pairs += added;
+                }
+                // the queue refers to this chunk's staging: drain it before the next chunk
+                if (qtail > qhead) {
+                    cp_window<D>(CA, act, S, qhead, qtail - qhead, tb, lane);
+                    qhead = qtail;
+                }
+                KC = 0;
+                __syncwarp();
+            }
+            // epilogue per target
+            for (int t = lane; t < TB; t += 32) {
+                const int i = tb + t;
+                const int ti = tag_of(A.s.tagm[i]);
+                if (ti >= 1 && ti <= A.n_tags && act.wants(ti)) act.end(i, ti, S.acc[t], S.cnt[t]);
+                else act.end_idle(i, ti);
+            }
+            __syncwarp();
+        }
+    }
+    if (EPI) {
+        for (int i = n_alive + (blockIdx.x * kCPWarps + warp) * 32 + lane; i < A.n_max; i += nwarps * 32)
+            act.end_idle(i, tag_of(A.s.tagm[i]));
+    }
+    if (st) atomicOr(A.status, st);
+    if (pairs) {
+        // my_pairs is warp-uniform (sum of ballot counts)
+        if (lane == 0 && my_pairs) atomicAdd(pairs, my_pairs);
+    }
+}
+
+}  // namespace epp

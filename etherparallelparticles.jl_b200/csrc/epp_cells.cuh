@@ -49,66 +49,73 @@ __global__ void k_bin_count(int n, DevDomain dom, State s, int* count, int2* cs,
 }
 
 // Single-pass exclusive scan with decoupled look-back over m = n_cells + 1 counts (the last is
-// the dead bin).  Writes start[0..m] and clears the counts for the next binning pass.  Tiles
-// take a ticket in launch order so every predecessor is already running; the wait on a
-// predecessor is bounded and reports EPP_STATUS_SPIN_TIMEOUT instead of hanging.
-// scan_state layout: [0] ticket, [1 + t] status word of tile t: (flag << 32) | value,
-// flag 1 = tile aggregate, 2 = inclusive prefix.
-__global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count, int* start,
-                                                       unsigned long long* scan_state,
+// the dead bin).  Writes start[0..m], the list of occupied cells occ[0..n_occ) in cell order
+// (meta[0] = n_occ) and clears the counts for the next binning pass.  Tiles take a ticket in
+// launch order so every predecessor is already running; the wait on a predecessor is bounded
+// and reports EPP_STATUS_SPIN_TIMEOUT instead of hanging.
+// scan_state layout: [0] ticket, [1 + t] status word of tile t:
+//   (flag << 62) | (occupied cells << 31) | particles,  flag 1 = aggregate, 2 = inclusive prefix.
+__device__ __forceinline__ unsigned long long pack_status(unsigned long long flag,
+                                                          unsigned long long v) {
+    // v = (occ << 32) | count  ->  status word
+    return (flag << 62) | ((v >> 32) << 31) | (v & 0x7fffffffull);
+}
+__device__ __forceinline__ unsigned long long unpack_status(unsigned long long w) {
+    return (((w >> 31) & 0x7fffffffull) << 32) | (w & 0x7fffffffull);
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count, int* start, int* occ,
+                                                       int* meta, unsigned long long* scan_state,
                                                        unsigned* status) {
     __shared__ int s_tile;
-    __shared__ int s_warp[kScanThreads / 32];
-    __shared__ int s_prefix;
+    __shared__ unsigned long long s_warp[kScanThreads / 32];
+    __shared__ unsigned long long s_prefix;
     if (threadIdx.x == 0) s_tile = (int)atomicAdd(&scan_state[0], 1ull);
     __syncthreads();
     const int tile = s_tile;
     const int base = tile * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
-    int tsum = 0;
+    unsigned long long tsum = 0;   // (occupied << 32) | particles
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         int idx = base + k;
         v[k] = idx < m ? count[idx] : 0;
-        tsum += v[k];
+        tsum += (unsigned long long)v[k] + ((idx < m - 1 && v[k] > 0) ? (1ull << 32) : 0ull);
     }
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k)
         if (base + k < m) count[base + k] = 0;
-    // block exclusive scan of per-thread sums
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = tsum;
+    unsigned long long incl = tsum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
     if (lane == 31) s_warp[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        int w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
-        int wi = w;
+        unsigned long long w = lane < kScanThreads / 32 ? s_warp[lane] : 0ull;
+        unsigned long long wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, wi, o);
+            unsigned long long t = __shfl_up_sync(0xffffffffu, wi, o);
             if (lane >= o) wi += t;
         }
         if (lane < kScanThreads / 32) s_warp[lane] = wi - w;   // exclusive warp offsets
         if (lane == kScanThreads / 32 - 1) {
-            // lane 7 holds the block total
-            int total = wi;
+            const unsigned long long total = wi;   // block total (lane 7)
             volatile unsigned long long* st = scan_state + 1;
             unsigned long long prefix = 0;
             if (tile == 0) {
-                __threadfence();
-                atomicExch(&scan_state[1 + tile], (2ull << 32) | (unsigned)total);
+                atomicExch(&scan_state[1 + tile], pack_status(2, total));
             } else {
-                atomicExch(&scan_state[1 + tile], (1ull << 32) | (unsigned)total);
+                atomicExch(&scan_state[1 + tile], pack_status(1, total));
                 int p = tile - 1;
                 long long spins = 0;
                 while (p >= 0) {
-                    unsigned long long w2 = st[p];
-                    unsigned flag = (unsigned)(w2 >> 32);
+                    const unsigned long long w2 = st[p];
+                    const unsigned flag = (unsigned)(w2 >> 62);
                     if (flag == 0) {
                         if (++spins > kSpinLimit) {
                             atomicOr(status, EPP_STATUS_SPIN_TIMEOUT);
@@ -117,25 +124,30 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count, int* s
                         __nanosleep(32);
                         continue;
                     }
-                    prefix += (unsigned)(w2 & 0xffffffffu);
+                    prefix += unpack_status(w2);
                     if (flag == 2) break;
                     --p;
                 }
                 __threadfence();
-                atomicExch(&scan_state[1 + tile],
-                           (2ull << 32) | (unsigned)(prefix + (unsigned)total));
+                atomicExch(&scan_state[1 + tile], pack_status(2, prefix + total));
             }
-            s_prefix = (int)prefix;
+            s_prefix = prefix;
         }
     }
     __syncthreads();
-    int run = s_prefix + s_warp[warp] + incl - tsum;
+    unsigned long long run = s_prefix + s_warp[warp] + incl - tsum;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        int idx = base + k;
-        if (idx < m) start[idx] = run;
-        run += v[k];
-        if (idx == m - 1) start[m] = run;
+        const int idx = base + k;
+        const int cnt = (int)(run & 0xffffffffull);
+        const int oc = (int)(run >> 32);
+        if (idx < m) start[idx] = cnt;
+        if (idx < m - 1 && v[k] > 0) occ[oc] = idx;
+        run += (unsigned long long)v[k] + ((idx < m - 1 && v[k] > 0) ? (1ull << 32) : 0ull);
+        if (idx == m - 1) {
+            start[m] = (int)(run & 0xffffffffull);
+            meta[0] = (int)(run >> 32);
+        }
     }
 }
 

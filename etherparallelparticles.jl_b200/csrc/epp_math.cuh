@@ -48,7 +48,7 @@ struct State {
     int* tagm;       // tag | movable << 16
     int* id;         // 0-based row of the particle in the caller's matrices
     int* cell;       // 0-based cell (n_cells = dead bin)
-    float2* rpn;     // (rho, p) after the next density update -- input of the fused momentum pass
+    float4* rp4;     // (rho, p, p/rho^2, 1/rho) that the next momentum pass reads
 };
 
 struct NeighbourList {   // EPP_SEARCH_EMIT_LIST output, column-major [k * cap + i]
@@ -130,6 +130,11 @@ __device__ __forceinline__ float wc2_gradient(float r, float hinv) {
 // Tait EOS: p = B ((rho / rho0)^gamma - 1) + p0 (replaces the linear eos of main.jl:64).
 __device__ __forceinline__ float eos(const DevPhys& P, float rho) {
     return P.B * (powi(__fdiv_rn(rho, P.rho0), P.gamma) - 1.0f) + P.p0;
+}
+
+// (rho, p, p / rho^2, 1 / rho): what a momentum pass needs of a neighbour (Pressure.jl:24-60).
+__device__ __forceinline__ float4 make_rp4(float rho, float p) {
+    return make_float4(rho, p, __fdiv_rn(p, __fmul_rn(rho, rho)), __fdiv_rn(1.0f, rho));
 }
 
 // Cell of a position: indexCartesianFromPosition + indexCartesianToLinear (Domain2D.jl:92-137),

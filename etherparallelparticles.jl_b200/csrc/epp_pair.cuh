@@ -118,7 +118,7 @@ struct HCache {
 };
 
 // ------------------------------------------------------------------------------------------
-// search! action: neighbour count, optional list (nIndex, nRVec, nR, nW, nDW, nHInv), and the
+// search! action (exact reference order; used when the list is emitted): neighbour count, list (nIndex, nRVec, nR, nW, nDW, nHInv), and the
 // dam-break continuity of main.jl:74-90 (iValueGradient! SPH/Library/Kernel.jl:114-128,
 // iClassicContinuity! / iBalancedContinuity! Continuity.jl:23-47).
 // FUSED: drho starts from 0 (sContinuity! zeroed it) and the density preview (rho + drho dt,
@@ -190,27 +190,18 @@ struct ActSearch {
         if (CONT) {
             s.drho[i] = a.drho;
             // density preview of sContinuity! (Continuity.jl:10-21) + eos, exact FP32 order
-            float2 rp;
             if (ti == P.fluid || ti == P.wall) {
-                rp.x = __fadd_rn(a.rho_i, __fmul_rn(a.drho, P.dt));
-                rp.y = eos(P, rp.x);
+                const float rho = __fadd_rn(a.rho_i, __fmul_rn(a.drho, P.dt));
+                s.rp4[i] = make_rp4(rho, eos(P, rho));
             } else {
-                rp.x = a.rho_i;
-                rp.y = s.p[i];
+                s.rp4[i] = make_rp4(a.rho_i, s.p[i]);
             }
-            s.rpn[i] = rp;
         }
     }
     __device__ __forceinline__ int count(const Acc& a) const { return a.cnt; }
 };
 
-// ------------------------------------------------------------------------------------------
-// interaction! action: dam-break momentum of main.jl:107-118 with the benchmark's artificial
-// viscosity: fluid-fluid iClassicPressure! (Pressure.jl:24-41), fluid-wall iBalancedPressure!
-// (:43-60), each followed by sArtificialViscosity! (Viscosity.jl:28-52).  Walls receive nothing.
-// FUSED: rho and p come from the density preview (rpn) of the previous search, du starts at 0
-// (sAccelerate! zeroed it) and the epilogue integrates (sGravity!, sAccelerate!, sMove!,
-// Motion.jl:17-51) and bins the new position.
+// Outputs of the fused momentum pass (integrate + bin epilogue).
 struct FusedOut {
     float4* xh;          // new (x, h)   in the current (old) order
     float4* vm;          // new (v, m)
@@ -221,183 +212,6 @@ struct FusedOut {
     unsigned long long* scan_state;   // cleared by block 0 for the scan that follows
     int n_scan_words;
     int n;               // all particles (alive first, dead bin last)
-};
-
-template <int D, bool FUSED>
-struct ActMomentum {
-    State s;
-    DevPhys P;
-    DevDomain dom;
-    FusedOut F;
-    unsigned* status;
-
-    struct Acc {
-        float du[3];
-        float rho_i, p_i, pr_i;
-        float4 vi;
-        HCache hc;
-    };
-    __device__ __forceinline__ bool wants(int ti) const { return ti == P.fluid; }
-    __device__ __forceinline__ void begin(int i, int ti, float4 xi, Acc& a) const {
-        if (FUSED) {
-            a.du[0] = a.du[1] = a.du[2] = 0.0f;
-            const float2 rp = s.rpn[i];
-            a.rho_i = rp.x;
-            a.p_i = rp.y;
-        } else {
-            const float4 d = s.dv[i];
-            a.du[0] = d.x; a.du[1] = d.y; a.du[2] = d.z;
-            a.rho_i = s.rho[i];
-            a.p_i = s.p[i];
-        }
-        if (ti == P.fluid) {
-            a.pr_i = fdiv(a.p_i, a.rho_i * a.rho_i);
-            a.vi = s.vm[i];
-            a.hc.init(xi.w);
-        }
-    }
-    __device__ __forceinline__ void pair(int i, int j, int ti, int tj, float4 xi, float4 xj,
-                                         float dx, float dy, float dz, float dr2, Acc& a) const {
-        const bool ff = tj == P.fluid;
-        const bool fw = tj == P.wall;
-        if (!(ff || fw)) return;
-        const float r = sqrtf(dr2);
-        const float hinv = a.hc.pair_hinv(xj.w);
-        const float dw = wc2_gradient<D>(r, hinv);
-        const float4 vj = s.vm[j];
-        float rho_j, p_j;
-        if (FUSED) {
-            const float2 rp = s.rpn[j];
-            rho_j = rp.x;
-            p_j = rp.y;
-        } else {
-            rho_j = s.rho[j];
-            p_j = s.p[j];
-        }
-        float p_rho_2 = ff ? a.pr_i + fdiv(p_j, rho_j * rho_j) : fdiv(a.p_i + p_j, a.rho_i * rho_j);
-        p_rho_2 *= fdiv(-vj.w * dw, r);
-        a.du[0] += p_rho_2 * dx;
-        a.du[1] += p_rho_2 * dy;
-        if (D == 3) a.du[2] += p_rho_2 * dz;
-        float vdx = dx * (a.vi.x - vj.x);
-        vdx += dy * (a.vi.y - vj.y);
-        if (D == 3) vdx += dz * (a.vi.z - vj.z);
-        if (vdx < 0.0f) {
-            const float rhob = 0.5f * (a.rho_i + rho_j);
-            const float hh = xj.w == a.hc.h ? a.hc.hh : fdiv(1.0f, hinv);
-            const float az = r * r + 0.01f * hh * hh;
-            const float phi = fdiv(vdx, hinv * az);
-            float force = fdiv((-P.alpha * P.c0 + P.beta * phi) * phi, rhob);
-            if (P.visc == EPP_VISCOSITY_REFERENCE) force *= fdiv(-vj.w, a.rho_i * rho_j * r) * dw;
-            else force *= fdiv(-vj.w, r) * dw;
-            a.du[0] += force * dx;
-            a.du[1] += force * dy;
-            if (D == 3) a.du[2] += force * dz;
-        }
-    }
-    __device__ __forceinline__ void end(int i, int ti, Acc& a) const {
-        if (!FUSED) {
-            if (ti == P.fluid) s.dv[i] = make_float4(a.du[0], a.du[1], a.du[2], 0.0f);
-            return;
-        }
-        integrate_and_bin(i, ti, &a);
-    }
-    __device__ __forceinline__ int count(const Acc&) const { return 0; }
-    // Fused epilogue; also used (acc == nullptr) for particles outside the pair loop.
-    __device__ __forceinline__ void integrate_and_bin(int i, int ti, const Acc* a) const {
-        float4 x = s.xh[i];
-        float4 v = s.vm[i];
-        float4 cp = s.comp[i];
-        const int tm = s.tagm[i];
-        int c = s.cell[i];
-        const bool alive = c != dom.n_cells;
-        if (alive && ti == P.fluid && a) {
-            float du[3] = {a->du[0], a->du[1], a->du[2]};
-            float vv[3] = {v.x, v.y, v.z}, xx[3] = {x.x, x.y, x.z}, cc[3] = {cp.x, cp.y, cp.z};
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                du[k] = __fadd_rn(du[k], P.g[k]);                      // sGravity!
-                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], P.dt));      // sAccelerate!
-            }
-#pragma unroll
-            for (int k = 0; k < D; ++k) {                              // sMove!
-                if (P.kahan) {
-                    const float y = __fsub_rn(__fmul_rn(vv[k], P.dt), cc[k]);
-                    const float t = __fadd_rn(xx[k], y);
-                    cc[k] = __fsub_rn(__fsub_rn(t, xx[k]), y);
-                    xx[k] = t;
-                } else {
-                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], P.dt));
-                }
-            }
-            x.x = xx[0]; x.y = xx[1]; x.z = xx[2];
-            v.x = vv[0]; v.y = vv[1]; v.z = vv[2];
-            cp.x = cc[0]; cp.y = cc[1]; cp.z = cc[2];
-            if (F.accel) F.accel[i] = make_float4(du[0], du[1], du[2], 0.0f);
-            if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z)))
-                atomicOr(status, EPP_STATUS_NONFINITE);
-        }
-        F.xh[i] = x;
-        F.vm[i] = v;
-        F.comp[i] = cp;
-        // bin the new position (insertParticlesIntoCells!, NeighbourSearch.jl:26-45)
-        if (alive && (movable_of(tm) || c < 0)) {
-            c = cell_of<D>(dom, x);
-            if (c < 0) {
-                c = dom.n_cells;
-                atomicOr(status, EPP_STATUS_KILLED);
-            }
-        }
-        const int slot = atomicAdd(&F.count[c], 1);
-        F.cs[i] = make_int2(c, slot);
-    }
-};
-
-// Fused momentum pass: the pair kernel for alive particles, the epilogue alone for the dead
-// bin; block 0 clears the scan's look-back state.
-template <int D>
-__global__ void __launch_bounds__(128) k_momentum_fused(PairArgs A, ActMomentum<D, true> act) {
-    if (blockIdx.x == 0)
-        for (int t = threadIdx.x; t < act.F.n_scan_words; t += blockDim.x) act.F.scan_state[t] = 0ull;
-    const int n_alive = min(A.start[A.dom.n_cells], A.n_max);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= act.F.n) return;
-    if (i >= n_alive) {
-        act.integrate_and_bin(i, tag_of(A.s.tagm[i]), nullptr);
-        return;
-    }
-    const float4 xi = A.s.xh[i];
-    const int ti = tag_of(A.s.tagm[i]);
-    typename ActMomentum<D, true>::Acc acc;
-    act.begin(i, ti, xi, acc);
-    const bool bad_i = ti < 1 || ti > A.n_tags;
-    if (bad_i) atomicOr(A.status, EPP_STATUS_BAD_TAG);
-    if (!bad_i && act.wants(ti)) traverse<D>(A, i, xi, ti, act, acc);
-    act.integrate_and_bin(i, ti, (!bad_i && ti == act.P.fluid) ? &acc : nullptr);
-}
-
-// interaction! test action (ActionTest.jl:71-75): dVelocity += 1 per listed neighbour.
-template <int D>
-struct ActCount {
-    State s;
-    struct Acc {
-        float n;
-    };
-    __device__ __forceinline__ bool wants(int) const { return true; }
-    __device__ __forceinline__ void begin(int, int, float4, Acc& a) const { a.n = 0.0f; }
-    __device__ __forceinline__ void pair(int, int, int, int, float4, float4, float, float, float,
-                                         float, Acc& a) const {
-        a.n += 1.0f;
-    }
-    __device__ __forceinline__ void end(int i, int, Acc& a) const {
-        float4 d = s.dv[i];
-        // one += per neighbour and component, as the reference loop adds 1.0 each time
-        d.x += a.n;
-        d.y += a.n;
-        if (D == 3) d.z += a.n;
-        s.dv[i] = d;
-    }
-    __device__ __forceinline__ int count(const Acc&) const { return 0; }
 };
 
 }  // namespace epp

@@ -1,7 +1,7 @@
 // epp_self.cuh -- per-particle passes: selfaction! actions, the fused-step gather, FP64
 // integrals, and the pack/unpack kernels between the reference layout and the sorted state.
 #pragma once
-#include "epp_pair.cuh"
+#include "epp_pass.cuh"
 
 namespace epp {
 
@@ -10,7 +10,7 @@ namespace epp {
 // DAMBREAK_INTEGRATE: sMomentum! of main.jl:120-126 with sAccelerate! + sMove! (Motion.jl:17-51).
 template <int D>
 __global__ void k_self(int action, const int* start, int n_cells, int n_max, State s, DevPhys P,
-                       unsigned* status) {
+                       unsigned* status, float4* accel) {
     const int n_alive = min(start[n_cells], n_max);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_alive) return;
@@ -47,6 +47,7 @@ __global__ void k_self(int action, const int* start, int n_cells, int n_max, Sta
                     xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], P.dt));
                 }
             }
+            if (accel) accel[i] = make_float4(du[0], du[1], du[2], 0.0f);
             s.dv[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             s.vm[i] = make_float4(vv[0], vv[1], vv[2], v.w);
             s.xh[i] = make_float4(xx[0], xx[1], xx[2], x.w);
@@ -63,15 +64,12 @@ __global__ void k_density_preview(const int* start, int n_cells, int n_max, Stat
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_alive) return;
     const int ti = tag_of(s.tagm[i]);
-    float2 rp;
     if (ti == P.fluid || ti == P.wall) {
-        rp.x = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt));
-        rp.y = eos(P, rp.x);
+        const float rho = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt));
+        s.rp4[i] = make_rp4(rho, eos(P, rho));
     } else {
-        rp.x = s.rho[i];
-        rp.y = s.p[i];
+        s.rp4[i] = make_rp4(s.rho[i], s.p[i]);
     }
-    s.rpn[i] = rp;
 }
 
 // Gather of the fused step: positions / velocities / compensation from the momentum pass's
@@ -94,7 +92,7 @@ struct MoverFused {
         b.cell[dst] = c;
         const int t = tag_of(tm);
         if (src < start_old[n_cells] && (t == fluid || t == wall)) {
-            const float2 rp = a.rpn[src];
+            const float4 rp = a.rp4[src];
             b.rho[dst] = rp.x;
             b.p[dst] = rp.y;
             b.vol[dst] = __fdiv_rn(vm.w, rp.x);

@@ -17,7 +17,7 @@ EXPORTS = [
     "epp_upload", "epp_download", "epp_search", "epp_interaction", "epp_selfaction", "epp_step",
     "epp_get_integrals", "epp_cell_stats", "epp_synchronize", "epp_last_step_timing",
     "epp_pairs_total", "epp_set_accel_output", "epp_get_accel", "epp_set_stream",
-    "epp_profile_step",
+    "epp_profile_step", "epp_set_tuning",
 ]
 
 
@@ -64,6 +64,7 @@ def load(path=LIB_PATH):
     lib.epp_get_accel.argtypes = [ctx, f32p, C.c_int32]
     lib.epp_set_stream.argtypes = [ctx, C.c_void_p]
     lib.epp_profile_step.argtypes = [ctx, P(abi.epp_physics), f32p]
+    lib.epp_set_tuning.argtypes = [ctx, C.c_int32]
     for name in EXPORTS:
         if name not in ("epp_last_error", "epp_abi_version"):
             getattr(lib, name).restype = C.c_int32
@@ -172,6 +173,9 @@ class Context:
 
     def set_accel_output(self, enable):
         self._ck(self.lib.epp_set_accel_output(self.h, 1 if enable else 0), "epp_set_accel_output")
+
+    def set_tuning(self, lanes_per_particle):
+        self._ck(self.lib.epp_set_tuning(self.h, lanes_per_particle), "epp_set_tuning")
 
     def set_stream(self, stream_handle):
         """Queue work on a caller-owned cudaStream_t (integer handle); None restores the own stream."""

@@ -194,6 +194,12 @@ int32_t epp_pairs_total(epp_ctx* ctx, int64_t* out);
 int32_t epp_set_accel_output(epp_ctx* ctx, int32_t enable);
 int32_t epp_get_accel(epp_ctx* ctx, float* out, int32_t n);
 
+/* Pair-pass kernel family: 0 (default) = one thread per particle, neighbours filtered once per
+ * step into a mask that the momentum pass reuses; 1 = one warp per occupied cell with a compacted
+ * pair queue; 2, 4, 8, 16 or 32 = that many lanes of a warp per particle.  Chosen by the
+ * autotuner; results change only at the FP32 rounding level (neighbour sets are identical). */
+int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
+
 /* Queue the context's work on a caller-owned cudaStream_t (passed as void*; NULL restores the
  * context's own stream).  Lets a host application order it with its own work and events. */
 int32_t epp_set_stream(epp_ctx* ctx, void* stream);

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -221,7 +222,7 @@ struct System : SysBase {
     /* int_properties_ columns */
     std::vector<int32_t> tag, movable, ncount, nindex;
     /* float_properties_ columns */
-    std::vector<T> pos, vel, dvel, comp, accel;
+    std::vector<T> pos, vel, dvel, comp, accel, accel_abs, drho_abs;
     std::vector<T> mass, vol, rho, drho, p, gapc, h;
     std::vector<T> nw, ndw, nhinv, nr, nrvec;
     /* neighbour system */
@@ -265,7 +266,8 @@ struct System : SysBase {
         tag.assign(N, 0); movable.assign(N, 0); ncount.assign(N, 0);
         nindex.assign(N * max_nb, 0);
         pos.assign(N * D, 0); vel.assign(N * D, 0); dvel.assign(N * D, 0);
-        comp.assign(N * D, 0); accel.assign(N * D, 0);
+        comp.assign(N * D, 0); accel.assign(N * D, 0); accel_abs.assign(N * D, 0);
+        drho_abs.assign(N, 0);
         mass.assign(N, 0); vol.assign(N, 0); rho.assign(N, 0); drho.assign(N, 0);
         p.assign(N, 0); gapc.assign(N, 0); h.assign(N, 0);
         nw.assign(N * max_nb, 0); ndw.assign(N * max_nb, 0); nhinv.assign(N * max_nb, 0);
@@ -396,6 +398,7 @@ struct System : SysBase {
      * iClassicContinuity! / iBalancedContinuity! (Continuity.jl:23-47) */
     void search_action(int action, int I, const Phys<T>& P) {
         if (action != EPP_ACTION_DAMBREAK_CONTINUITY) return;
+        drho_abs[I] = T(0);
         for (int ni = 0; ni < ncount[I]; ++ni) {
             int J = NIDX(ni, I) - 1;
             bool ff = tag[I] == P.fluid && tag[J] == P.fluid;
@@ -407,8 +410,11 @@ struct System : SysBase {
             NW(ni, I) = wc2_value<T>(NR(ni, I), hinv, D);
             NDW(ni, I) = wc2_gradient<T>(NR(ni, I), hinv, D);
             T dw = NDW(ni, I);
-            if (ff) drho[I] += mass[J] * vdotx(I, ni, J) * dw / NR(ni, I);
-            else drho[I] += rho[I] * vol[J] * vdotx(I, ni, J) * dw / NR(ni, I);
+            T term;
+            if (ff) term = mass[J] * vdotx(I, ni, J) * dw / NR(ni, I);
+            else term = rho[I] * vol[J] * vdotx(I, ni, J) * dw / NR(ni, I);
+            drho[I] += term;
+            drho_abs[I] += std::fabs(term);
         }
     }
 
@@ -421,6 +427,7 @@ struct System : SysBase {
 #pragma omp parallel for schedule(dynamic, 256)
         for (int I = 0; I < n; ++I) {
             if (alive[I] != 1) continue;
+            for (int a = 0; a < D; ++a) accel_abs[(size_t)a * n_cap + I] = T(0);
             for (int ni = 0; ni < ncount[I]; ++ni) {
                 if (action == EPP_ACTION_COUNT_NEIGHBOURS) {
                     for (int a = 0; a < D; ++a) DU(a, I) += T(1.0);
@@ -447,7 +454,10 @@ struct System : SysBase {
         else p_rho_2 = (p[I] + p[J]) / (rho[I] * rho[J]);
         p_rho_2 += std::fabs(p_rho_2) * P.coef;
         p_rho_2 *= -mass[J] * dw / r;
-        for (int a = 0; a < D; ++a) DU(a, I) += p_rho_2 * RV(ni, a, I);
+        for (int a = 0; a < D; ++a) {
+            DU(a, I) += p_rho_2 * RV(ni, a, I);
+            accel_abs[(size_t)a * n_cap + I] += std::fabs(p_rho_2 * RV(ni, a, I));
+        }
         /* sArtificialViscosity! */
         T v_dot_x = vdotx(I, ni, J);
         if (v_dot_x > 0) return;
@@ -459,7 +469,10 @@ struct System : SysBase {
         T force = (-P.alpha * P.c0 + P.beta * phi) * phi / rhob;
         if (P.visc == EPP_VISCOSITY_REFERENCE) force *= -mass[J] / (rho[I] * rho[J] * r) * dw;
         else force *= -mass[J] / r * dw;
-        for (int a = 0; a < D; ++a) DU(a, I) += force * RV(ni, a, I);
+        for (int a = 0; a < D; ++a) {
+            DU(a, I) += force * RV(ni, a, I);
+            accel_abs[(size_t)a * n_cap + I] += std::fabs(force * RV(ni, a, I));
+        }
     }
 
     /* --- selfaction!, Action.jl:39-51 */
@@ -485,7 +498,10 @@ struct System : SysBase {
                 /* sMomentum!, main.jl:120-126 with sAccelerate! + sMove! (Motion.jl:17-51) in
                  * place of sAccelerateMove!; sGravity! State.jl:35-62 */
                 if (tag[I] == P.fluid) {
-                    for (int a = 0; a < D; ++a) DU(a, I) += P.g[a];
+                    for (int a = 0; a < D; ++a) {
+                        DU(a, I) += P.g[a];
+                        accel_abs[(size_t)a * n_cap + I] += std::fabs(P.g[a]);
+                    }
                     for (int a = 0; a < D; ++a) {
                         accel[(size_t)a * n_cap + I] = DU(a, I);
                         U(a, I) += DU(a, I) * P.dt;
@@ -539,6 +555,8 @@ T* field_ptr(System<T>* s, int field, int k, bool& vec) {
         case ORC_FIELD_VELOCITY: vec = true; return &s->vel[(size_t)k * s->n_cap];
         case ORC_FIELD_DVELOCITY: vec = true; return &s->dvel[(size_t)k * s->n_cap];
         case ORC_FIELD_ACCEL: vec = true; return &s->accel[(size_t)k * s->n_cap];
+        case ORC_FIELD_ACCEL_ABS: vec = true; return &s->accel_abs[(size_t)k * s->n_cap];
+        case ORC_FIELD_DDENSITY_ABS: return s->drho_abs.data();
         case ORC_FIELD_DENSITY: return s->rho.data();
         case ORC_FIELD_DDENSITY: return s->drho.data();
         case ORC_FIELD_PRESSURE: return s->p.data();
@@ -815,6 +833,24 @@ int32_t orc_get_field(orc_sys* s0, int32_t field, int32_t k, double* out) {
         if (!p) return EPP_ERR_INVALID_ARGUMENT;
         if (!vec && k != 0) return EPP_ERR_INVALID_ARGUMENT;
         for (int I = 0; I < S->n; ++I) out[I] = (double)p[I];
+        return EPP_OK;
+    };
+    if (s->precision == 64) return go(static_cast<System<double>*>(s));
+    return go(static_cast<System<float>*>(s));
+}
+
+int32_t orc_set_field(orc_sys* s0, int32_t field, int32_t k, const double* in) {
+    SysBase* s = reinterpret_cast<SysBase*>(s0);
+    if (!in) return EPP_ERR_INVALID_ARGUMENT;
+    auto go = [&](auto* S) -> int32_t {
+        using T = typename std::remove_reference<decltype(S->rho[0])>::type;
+        bool vec;
+        if (k < 0 || k >= S->D) return EPP_ERR_INVALID_ARGUMENT;
+        auto* p = field_ptr(S, field, k, vec);
+        if (!p || field == ORC_FIELD_ACCEL || field == ORC_FIELD_ACCEL_ABS ||
+            field == ORC_FIELD_DDENSITY_ABS || (!vec && k != 0))
+            return EPP_ERR_INVALID_ARGUMENT;
+        for (int I = 0; I < S->n; ++I) p[I] = (T)in[I];
         return EPP_OK;
     };
     if (s->precision == 64) return go(static_cast<System<double>*>(s));

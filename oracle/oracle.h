@@ -36,6 +36,10 @@ typedef struct orc_sys orc_sys;
 #define ORC_FIELD_MASS       7
 #define ORC_FIELD_ACCEL      8 /* dv/dt of the last DAMBREAK_INTEGRATE (momentum sum + gravity) */
 #define ORC_FIELD_NCOUNT     9
+/* Sum of |terms| of the last momentum interaction (vector, + |g| after integrate) and of the last
+ * continuity search: the scale against which an FP32 sum's rounding error is measured. */
+#define ORC_FIELD_ACCEL_ABS  10
+#define ORC_FIELD_DDENSITY_ABS 11
 
 int32_t orc_domain_info(const epp_domain* d, int32_t precision, int32_t n_out[3],
                         double gap_axis[3], double gap_inv[3]);
@@ -59,6 +63,8 @@ int32_t orc_download(orc_sys* s, int32_t* is_alive, int32_t* cell_index, int32_t
                      int64_t ld_int, float* float_props, int64_t ld_float,
                      const epp_column_map* map);
 int32_t orc_get_field(orc_sys* s, int32_t field, int32_t component, double* out);
+/* Overwrite a state field (position, velocity, dvelocity, density, ddensity, pressure, volume). */
+int32_t orc_set_field(orc_sys* s, int32_t field, int32_t component, const double* in);
 
 int32_t orc_search(orc_sys* s, int32_t criterion, int32_t action, const epp_physics* phys,
                    int32_t flags);

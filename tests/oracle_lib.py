@@ -25,6 +25,8 @@ ORC_FIELD_VOLUME = 6
 ORC_FIELD_MASS = 7
 ORC_FIELD_ACCEL = 8
 ORC_FIELD_NCOUNT = 9
+ORC_FIELD_ACCEL_ABS = 10
+ORC_FIELD_DDENSITY_ABS = 11
 
 _lib = None
 
@@ -51,6 +53,7 @@ def load():
     lib.orc_download.argtypes = [C.c_void_p, i32p, i32p, i32p, C.c_int64, f32p, C.c_int64,
                                  P(abi.epp_column_map)]
     lib.orc_get_field.argtypes = [C.c_void_p, C.c_int32, C.c_int32, f64p]
+    lib.orc_set_field.argtypes = [C.c_void_p, C.c_int32, C.c_int32, f64p]
     lib.orc_search.argtypes = [C.c_void_p, C.c_int32, C.c_int32, P(abi.epp_physics), C.c_int32]
     lib.orc_interaction.argtypes = [C.c_void_p, C.c_int32, P(abi.epp_physics)]
     lib.orc_selfaction.argtypes = [C.c_void_p, C.c_int32, P(abi.epp_physics)]
@@ -103,6 +106,11 @@ class Oracle:
         out = np.zeros(self.config.n_capacity, dtype=np.float64)
         self._ck(self.lib.orc_get_field(self.h, field, k, _p(out, C.c_double)), "orc_get_field")
         return out[:n]
+
+    def set_field(self, field, values, k=0):
+        v = np.zeros(self.config.n_capacity, dtype=np.float64)
+        v[: len(values)] = values
+        self._ck(self.lib.orc_set_field(self.h, field, k, _p(v, C.c_double)), "orc_set_field")
 
     def search(self, criterion, action, phys=None, flags=0):
         self._ck(self.lib.orc_search(self.h, criterion, action,
