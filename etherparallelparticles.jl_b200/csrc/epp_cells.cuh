@@ -64,7 +64,7 @@ __device__ __forceinline__ unsigned long long unpack_status(unsigned long long w
     return (((w >> 31) & 0x7fffffffull) << 32) | (w & 0x7fffffffull);
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count, int* start, int* occ,
+static __global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count, int* start, int* occ,
                                                        int* meta, unsigned long long* scan_state,
                                                        unsigned* status) {
     __shared__ int s_tile;
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count, int* s
 
 // Scatter in arrival order: perm[start[c] + slot] = (id, source index).  A destination outside
 // [0, n) can only come from a failed scan; it is reported, never written.
-__global__ void k_scatter(int n, const int2* cs, const int* start, const int* id, int2* perm,
+static __global__ void k_scatter(int n, const int2* cs, const int* start, const int* id, int2* perm,
                           unsigned* status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;

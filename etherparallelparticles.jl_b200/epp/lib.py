@@ -17,7 +17,7 @@ EXPORTS = [
     "epp_upload", "epp_download", "epp_search", "epp_interaction", "epp_selfaction", "epp_step",
     "epp_get_integrals", "epp_cell_stats", "epp_synchronize", "epp_last_step_timing",
     "epp_pairs_total", "epp_set_accel_output", "epp_get_accel", "epp_set_stream",
-    "epp_profile_step", "epp_set_tuning",
+    "epp_profile_step", "epp_set_tuning", "epp_cell_sort_noalloc", "epp_noalloc_limits",
 ]
 
 
@@ -65,6 +65,9 @@ def load(path=LIB_PATH):
     lib.epp_set_stream.argtypes = [ctx, C.c_void_p]
     lib.epp_profile_step.argtypes = [ctx, P(abi.epp_physics), f32p]
     lib.epp_set_tuning.argtypes = [ctx, C.c_int32]
+    lib.epp_cell_sort_noalloc.argtypes = [P(abi.epp_domain), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, i32p, C.c_void_p]
+    lib.epp_noalloc_limits.argtypes = [i32p, i32p, P(C.c_int64)]
     for name in EXPORTS:
         if name not in ("epp_last_error", "epp_abi_version"):
             getattr(lib, name).restype = C.c_int32

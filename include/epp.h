@@ -209,6 +209,28 @@ int32_t epp_set_stream(epp_ctx* ctx, void* stream);
  * search+continuity.  Same results as epp_step(ctx, 1, phys). */
 int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms);
 
+/* Cell-list build that allocates nothing, for callers that must not call cudaMalloc while they
+ * drive the library (a host application that owns a fixed device pool, or one that is in the
+ * middle of a step where a device allocation would synchronise or is not allowed).  No
+ * counterpart in the reference: it is the bin + count + scan + counting sort of search!
+ * (NeighbourSearch.jl:12-47) as one call on caller-owned device buffers.
+ *   pos         device, column-major positions: x at pos[i], y at pos[n + i], z at pos[2n + i]
+ *   counts      device [n_cells] or NULL;  offsets  device [n_cells + 1] or NULL
+ *   sorted_ids  device [n]: 1-based particle ids in cell order, by id inside a cell (the first
+ *               *n_alive entries are set; particles outside the domain are left out)
+ *   n_alive     host: number of particles inside the domain
+ *   stream      cudaStream_t (NULL = default stream); the call waits for it before returning
+ * All intermediate arrays live in one static device array of this library (see
+ * epp_noalloc_limits: up to 2^20 particles and 2^20 cells, about 29 MB, held by every GPU that
+ * loads the library until the process exits).  Larger inputs return EPP_ERR_CAPACITY.  Every call
+ * shares that array, so calls that overlap on the GPU (other streams, other host threads) race;
+ * serialise them.  The first call on a device looks up the array's device address for that
+ * device (cudaGetSymbolAddress), so make it before any stream capture.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine. */
+int32_t epp_cell_sort_noalloc(const epp_domain* domain, int32_t n, const float* pos, int32_t* counts,
+                              int32_t* offsets, int32_t* sorted_ids, int32_t* n_alive, void* stream);
+int32_t epp_noalloc_limits(int32_t* max_particles, int32_t* max_cells, int64_t* scratch_bytes);
+
 #ifdef __cplusplus
 }
 #endif
