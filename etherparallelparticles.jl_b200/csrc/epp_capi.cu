@@ -107,6 +107,7 @@ struct epp_ctx {
     int lanes = 0;             // pair-pass family: 0 mask passes, 1 cell-centric, 2..32 lane groups
     unsigned* mask = nullptr;  // neighbour masks of the last search ([NW * cap])
     bool mask_valid = false;   // the mask matches the current order, positions and criterion
+    bool uniform_h = false;    // every uploaded particle has the same smoothing length
     // fused step graphs, one per ping-pong parity
     cudaGraphExec_t graph[2]{};
     epp_physics graph_phys{};
@@ -158,7 +159,7 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
     b += (size_t)kIntegralBlocks * 8 * 7 + 8 * 8 + 4 * 256;
-    b += (size_t)cap * 4 * (D == 2 ? MaskConf<2>::NW : MaskConf<3>::NW) + 256;   // neighbour masks
+    b += (size_t)cap * 4 * (D == 2 ? TileConf<2>::NW : TileConf<3>::NW) + 256;   // neighbour masks
     return b + (1 << 20);
 }
 
@@ -195,13 +196,18 @@ PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
 
 int lanes_of(const epp_ctx* ctx) { return ctx->lanes; }
 
-// A mask pass (one thread per particle).  BUILD: filter (and store the mask if `store`).
+// A warp-tile pass.  BUILD: filter the candidates (and store the neighbour mask if `store`);
+// otherwise reuse the mask of the last search at these positions.
 template <int D, bool BUILD, class Act, bool EPI = false>
 int launch_pass(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs, bool store) {
     PairArgs A = pair_args(ctx, set, crit);
-    MaskArgs M{store || !BUILD ? ctx->mask : nullptr, ctx->cap};
-    k_pass<D, BUILD, Act, EPI><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
-                                                                          ctx->n_tiles + 1);
+    TileMask M{store || !BUILD ? ctx->mask : nullptr, ctx->cap};
+    if (ctx->uniform_h)
+        k_tile<D, BUILD, Act, EPI, true><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
+                                                                                      ctx->n_tiles + 1);
+    else
+        k_tile<D, BUILD, Act, EPI, false><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
+                                                                                       ctx->n_tiles + 1);
     CK_LAUNCH();
     return EPP_OK;
 }
@@ -665,7 +671,7 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->iticket = a.take<unsigned>(1);
     ctx->ihpart = a.take<double>(kIntegralBlocks);
     ctx->ihmin = a.take<double>(1);
-    ctx->mask = a.take<unsigned>((size_t)ctx->cap * (D == 2 ? MaskConf<2>::NW : MaskConf<3>::NW));
+    ctx->mask = a.take<unsigned>((size_t)ctx->cap * (D == 2 ? TileConf<2>::NW : TileConf<3>::NW));
     ctx->tmp.count = ctx->count;
     ctx->tmp.cs = ctx->cs;
     ctx->tmp.scan_state = ctx->scan_state;
@@ -768,6 +774,21 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     rc |= icol(SI_ALIVE, is_alive, 0);
     rc |= icol(SI_CELL, cell_index, 0);
     if (rc) return rc;
+    {
+        bool uni = m->h >= 0;
+        if (uni) {
+            const float* hc = fp + (size_t)m->h * ldf;
+            for (int k = 1; k < n && uni; ++k) uni = hc[k] == hc[0];
+        }
+        if (ctx->uniform_h != uni) {
+            ctx->uniform_h = uni;
+            for (int c = 0; c < 2; ++c)
+                if (ctx->graph[c]) {
+                    cudaGraphExecDestroy(ctx->graph[c]);
+                    ctx->graph[c] = nullptr;
+                }
+        }
+    }
     ctx->cur = 0;
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;

@@ -33,6 +33,35 @@ struct TargetConst {   // per target: h, invharmonic(h,h), dW/r factor, 1/hinv, 
     float h2sq;
 };
 
+// Kernel constants of the last neighbour h_j != h_i (a handful of distinct h values occur, so
+// the IEEE division of invharmonic runs once per change instead of once per pair).
+struct HPairCache {
+    float hj, hinv, kdw, hh;
+};
+
+template <int D>
+__device__ __noinline__ void hpair_fill(HPairCache& c, float hi, float hj) {
+    c.hj = hj;
+    c.hinv = invharmonic_exact(hi, hj);
+    c.kdw = wc2_kdw<D>(c.hinv);
+    c.hh = __fdividef(1.0f, c.hinv);
+}
+
+template <int D>
+__device__ __forceinline__ void pair_consts(const TargetConst& tc, HPairCache& pc, float hj, float& hinv,
+                                            float& kdw, float& hh) {
+    if (hj == tc.h) {
+        hinv = tc.hinv;
+        kdw = tc.kdw;
+        hh = tc.hh;
+        return;
+    }
+    if (hj != pc.hj) hpair_fill<D>(pc, tc.h, hj);
+    hinv = pc.hinv;
+    kdw = pc.kdw;
+    hh = pc.hh;
+}
+
 template <int D>
 struct CPShared {
     float4 cx[CPConf<D>::C];     // staged candidate (x, h)
@@ -70,34 +99,41 @@ struct CPCont {
     int* ncount;
     static constexpr int NC = 1;
     __device__ __forceinline__ bool wants(int) const { return true; }
-    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
-                                              const PairGeo& g, const TargetConst& tc) const {
+    struct Self {
+        float4 v;
+        float rho;
+    };
+    struct Nb {
+        float4 v;
+        float vol;
+    };
+    __device__ __forceinline__ Self self(int i) const { return Self{s.vm[i], s.rho[i]}; }
+    __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{s.vm[j], s.vol[j]}; }
+    __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
+                                           const PairGeo& g, const TargetConst& tc, HPairCache& pc) const {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const bool ff = ti == P.fluid && tj == P.fluid;
         const bool fw = ti == P.fluid && tj == P.wall;
         const bool wf = ti == P.wall && tj == P.fluid;
         if (!(ff || fw || wf)) return out;
         const float r = sqrtf(g.dr2);
-        float hinv, kdw;
-        if (xj.w == tc.h) {
-            hinv = tc.hinv;
-            kdw = tc.kdw;
-        } else {
-            hinv = invharmonic_exact(tc.h, xj.w);
-            kdw = wc2_kdw<D>(hinv);
-        }
+        float hinv, kdw, hh;
+        pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
         const float q = r * hinv;
         if (!(q < 2.0f)) return out;     // W = dW = 0 at q >= 2 (WendlandC2.jl:23,44)
         const float u = 2.0f - q;
         const float dwr = kdw * (u * u * u);
-        const float4 vi = s.vm[i];
-        const float4 vj = s.vm[j];
-        float vdx = g.dx * (vi.x - vj.x);
-        vdx += g.dy * (vi.y - vj.y);
-        if (D == 3) vdx += g.dz * (vi.z - vj.z);
-        if (ff) out.x = vj.w * vdx * dwr;                       // iClassicContinuity!
-        else out.x = s.rho[i] * s.vol[j] * vdx * dwr;           // iBalancedContinuity!
+        float vdx = g.dx * (me.v.x - nb.v.x);
+        vdx += g.dy * (me.v.y - nb.v.y);
+        if (D == 3) vdx += g.dz * (me.v.z - nb.v.z);
+        if (ff) out.x = nb.v.w * vdx * dwr;                     // iClassicContinuity!
+        else out.x = me.rho * nb.vol * vdx * dwr;               // iBalancedContinuity!
         return out;
+    }
+    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
+                                              const PairGeo& g, const TargetConst& tc) const {
+        HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
+        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc, pc);
     }
     __device__ __forceinline__ void end(int i, int ti, float4 sum, int cnt) const {
         ncount[i] = cnt;
@@ -119,6 +155,14 @@ template <int D>
 struct CPCount {
     int* ncount;
     static constexpr int NC = 0;
+    struct Self {};
+    struct Nb {};
+    __device__ __forceinline__ Self self(int) const { return Self{}; }
+    __device__ __forceinline__ Nb fetch(int, int, int) const { return Nb{}; }
+    __device__ __forceinline__ float4 term(const Self&, const Nb&, int, int, float4, const PairGeo&,
+                                           const TargetConst&, HPairCache&) const {
+        return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     __device__ __forceinline__ bool wants(int) const { return true; }
     __device__ __forceinline__ float4 contrib(int, int, int, int, float4, float4, const PairGeo&,
                                               const TargetConst&) const {
@@ -133,6 +177,14 @@ template <int D>
 struct CPCountDv {
     State s;
     static constexpr int NC = 0;
+    struct Self {};
+    struct Nb {};
+    __device__ __forceinline__ Self self(int) const { return Self{}; }
+    __device__ __forceinline__ Nb fetch(int, int, int) const { return Nb{}; }
+    __device__ __forceinline__ float4 term(const Self&, const Nb&, int, int, float4, const PairGeo&,
+                                           const TargetConst&, HPairCache&) const {
+        return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     __device__ __forceinline__ bool wants(int) const { return true; }
     __device__ __forceinline__ float4 contrib(int, int, int, int, float4, float4, const PairGeo&,
                                               const TargetConst&) const {
@@ -155,8 +207,16 @@ struct CPMom {
     ActMomG<D, FUSED> m;   // state, physics, fused outputs, integrate_and_bin
     static constexpr int NC = 3;
     __device__ __forceinline__ bool wants(int ti) const { return ti == m.P.fluid; }
-    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
-                                              const PairGeo& g, const TargetConst& tc) const {
+    struct Self {
+        float4 v, rp;
+    };
+    struct Nb {
+        float4 v, rp;
+    };
+    __device__ __forceinline__ Self self(int i) const { return Self{m.s.vm[i], m.s.rp4[i]}; }
+    __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{m.s.vm[j], m.s.rp4[j]}; }
+    __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
+                                           const PairGeo& g, const TargetConst& tc, HPairCache& pc) const {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const DevPhys& P = m.P;
         const bool ff = tj == P.fluid;
@@ -164,23 +224,12 @@ struct CPMom {
         if (!(ff || fw)) return out;
         const float r = sqrtf(g.dr2);
         float hinv, kdw, hh;
-        if (xj.w == tc.h) {
-            hinv = tc.hinv;
-            kdw = tc.kdw;
-            hh = tc.hh;
-        } else {
-            hinv = invharmonic_exact(tc.h, xj.w);
-            kdw = wc2_kdw<D>(hinv);
-            hh = __fdividef(1.0f, hinv);
-        }
+        pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
         const float q = r * hinv;
         if (!(q < 2.0f)) return out;
         const float u = 2.0f - q;
         const float dwr = kdw * (u * u * u);
-        const float4 rpi = m.s.rp4[i];
-        const float4 rpj = m.s.rp4[j];
-        const float4 vi = m.s.vm[i];
-        const float4 vj = m.s.vm[j];
+        const float4 rpi = me.rp, rpj = nb.rp, vi = me.v, vj = nb.v;
         const float p_rho_2 = ff ? rpi.z + rpj.z : (rpi.y + rpj.y) * rpi.w * rpj.w;
         const float fp = p_rho_2 * (-vj.w * dwr);
         out.x = fp * g.dx;
@@ -201,6 +250,11 @@ struct CPMom {
             if (D == 3) out.z += force * g.dz;
         }
         return out;
+    }
+    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
+                                              const PairGeo& g, const TargetConst& tc) const {
+        HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
+        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc, pc);
     }
     __device__ __forceinline__ void end(int i, int ti, float4 sum, int) const {
         typename ActMomG<D, FUSED>::Acc a;

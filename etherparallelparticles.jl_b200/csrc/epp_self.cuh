@@ -2,6 +2,7 @@
 // integrals, and the pack/unpack kernels between the reference layout and the sorted state.
 #pragma once
 #include "epp_pass.cuh"
+#include "epp_tile.cuh"
 
 namespace epp {
 
