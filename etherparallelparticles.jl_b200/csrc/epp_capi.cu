@@ -37,6 +37,7 @@ struct Arena {
 
 DevPhys to_dev(const epp_physics& p) {
     DevPhys d;
+    d.ip = nullptr;
     d.dt = p.dt;
     d.rho0 = p.rho0;
     d.c0 = p.c0;
@@ -106,8 +107,16 @@ struct epp_ctx {
     unsigned adj[kMaxTags]{};
     int lanes = 0;             // pair-pass family: 0 mask passes, 1 cell-centric, 2..32 lane groups
     unsigned* mask = nullptr;  // neighbour masks of the last search ([NW * cap])
+    int* nlist = nullptr;      // neighbour lists of the last search ([LCAP * cap])
     bool mask_valid = false;   // the mask matches the current order, positions and criterion
     bool uniform_h = false;    // every uploaded particle has the same smoothing length
+    int n_inst = 1;            // batch instances (independent layers of the cell grid)
+    InstPhys* inst_table = nullptr;     // device [n_inst]; null when no per-instance physics is set
+    std::vector<float> inst_dt, inst_c0;
+    bool inst_dirty = false;
+    float inst_rho0 = 0.0f;
+    int inst_gamma = 0;
+    double* inst_out = nullptr;         // device [n_inst * 9] integrals
     // fused step graphs, one per ping-pong parity
     cudaGraphExec_t graph[2]{};
     epp_physics graph_phys{};
@@ -160,6 +169,7 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
     b += (size_t)kIntegralBlocks * 8 * 7 + 8 * 8 + 4 * 256;
     b += (size_t)cap * 4 * (D == 2 ? TileConf<2>::NW : TileConf<3>::NW) + 256;   // neighbour masks
+    b += 2 * 256;                                                                  // instance tables (small)
     return b + (1 << 20);
 }
 
@@ -179,6 +189,30 @@ void fill_state(Arena& a, State& s, int cap) {
     s.id = a.take<int>(cap);
     s.cell = a.take<int>(cap);
     s.rp4 = a.take<float4>(cap);
+}
+
+// Device physics of a call: the per-instance table (uploaded when it changed) overrides dt, c0, B.
+DevPhys dev_phys(epp_ctx* ctx, const epp_physics& p) {
+    DevPhys d = to_dev(p);
+    if (!ctx->inst_dt.empty()) {
+        if (ctx->inst_dirty || ctx->inst_rho0 != p.rho0 || ctx->inst_gamma != p.gamma) {
+            std::vector<InstPhys> t(ctx->n_inst);
+            for (int k = 0; k < ctx->n_inst; ++k) {
+                t[k].dt = ctx->inst_dt[k];
+                t[k].c0 = ctx->inst_c0[k];
+                t[k].B = (float)((double)p.rho0 * (double)ctx->inst_c0[k] * (double)ctx->inst_c0[k] / (double)p.gamma);
+                t[k].pad = 0.0f;
+            }
+            cudaMemcpyAsync(ctx->inst_table, t.data(), sizeof(InstPhys) * ctx->n_inst, cudaMemcpyHostToDevice,
+                            ctx->stream);
+            cudaStreamSynchronize(ctx->stream);
+            ctx->inst_dirty = false;
+            ctx->inst_rho0 = p.rho0;
+            ctx->inst_gamma = p.gamma;
+        }
+        d.ip = ctx->inst_table;
+    }
+    return d;
 }
 
 PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
@@ -201,13 +235,18 @@ int lanes_of(const epp_ctx* ctx) { return ctx->lanes; }
 template <int D, bool BUILD, class Act, bool EPI = false>
 int launch_pass(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs, bool store) {
     PairArgs A = pair_args(ctx, set, crit);
-    TileMask M{store || !BUILD ? ctx->mask : nullptr, ctx->cap};
-    if (ctx->uniform_h)
+    // the search pass writes the mask and list when `store`; the reuse pass reads the list
+    TileMask M{store || !BUILD ? ctx->mask : nullptr, ctx->cap, store || !BUILD ? ctx->nlist : nullptr};
+    if constexpr (!BUILD) {   // reuse of the last search: walk its neighbour lists
+        k_list<D, Act, EPI><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, ctx->ncount, act, ctx->scan_state,
+                                                                         ctx->n_tiles + 1);
+    } else if (ctx->uniform_h) {
         k_tile<D, BUILD, Act, EPI, true><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
                                                                                       ctx->n_tiles + 1);
-    else
+    } else {
         k_tile<D, BUILD, Act, EPI, false><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
                                                                                        ctx->n_tiles + 1);
+    }
     CK_LAUNCH();
     return EPP_OK;
 }
@@ -328,7 +367,7 @@ template <int D>
 int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_physics* phys, bool emit,
                        bool fused) {
     PairArgs A = pair_args(ctx, set, crit);
-    DevPhys P = phys ? to_dev(*phys) : DevPhys{};
+    DevPhys P = phys ? dev_phys(ctx, *phys) : DevPhys{};
     const bool cont = action == EPP_ACTION_DAMBREAK_CONTINUITY;
     if (emit) {
         ctx->mask_valid = false;
@@ -404,7 +443,7 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     PairArgs A = pair_args(ctx, c, EPP_CRITERION_SYMMETRY);
     ActMomG<D, true> mom;
     mom.s = ctx->S[c];
-    mom.P = to_dev(phys);
+    mom.P = dev_phys(ctx, phys);
     mom.dom = ctx->dom;
     mom.F = ctx->tmp;
     mom.F.n = n;
@@ -476,7 +515,7 @@ int build_graphs(epp_ctx* ctx, const epp_physics& phys) {
 
 template <int D>
 int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
-    DevPhys P = phys ? to_dev(*phys) : DevPhys{};
+    DevPhys P = phys ? dev_phys(ctx, *phys) : DevPhys{};
     k_self<D><<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(action, ctx->start[ctx->cur], ctx->n_cells,
                                                                 ctx->n, ctx->S[ctx->cur], P, ctx->status,
                                                                 ctx->accel);
@@ -493,7 +532,7 @@ int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
         CK_LAUNCH();
         ActMomG<D, false> act;
         act.s = ctx->S[ctx->cur];
-        act.P = to_dev(*phys);
+        act.P = dev_phys(ctx, *phys);
         act.dom = ctx->dom;
         act.F = FusedOut{};
         act.status = ctx->status;
@@ -516,6 +555,7 @@ int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
 template <int D>
 int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     int rc;
+    if (ctx->inst_dirty) dev_phys(ctx, phys);   // upload the per-instance table the graphs read
     if (ctx->dv_dirty) {
         // the first step goes through the per-call kernels, which honour a non-zero dVelocity
         rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_DENSITY, &phys);
@@ -531,7 +571,7 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     }
     if (!ctx->rpn_valid || !same_phys(ctx->rpn_phys, phys)) {
         k_density_preview<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
-            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], to_dev(phys));
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], dev_phys(ctx, phys));
         CK_LAUNCH();
     }
     if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->mask_valid = false;
@@ -614,12 +654,16 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
         d.gap_inv[a] = 1.0f / ga;
         ncell *= na;
     }
-    if (ncell > (1ll << 30)) {
+    const int n_inst = cfg->n_instances > 1 ? cfg->n_instances : 1;
+    if ((D == 3 && n_inst > 1) || ncell * n_inst > (1ll << 30) || n_inst > (1 << 22)) {
         delete ctx;
         return EPP_ERR_INVALID_ARGUMENT;
     }
-    d.n_cells = (int)ncell;
-    ctx->n_cells = (int)ncell;
+    ctx->n_inst = n_inst;
+    d.cells_per_inst = (int)ncell;
+    d.n_inst = n_inst;
+    d.n_cells = (int)(ncell * n_inst);
+    ctx->n_cells = d.n_cells;
     ctx->n_tiles = (ctx->n_cells + 1 + kScanTile - 1) / kScanTile;
     for (int a = 0; a < cfg->n_tags; ++a) {
         unsigned m = 0;
@@ -681,7 +725,20 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
         epp_destroy(ctx);
         return EPP_ERR_OUT_OF_MEMORY;
     }
+    const size_t lcap = D == 2 ? ListConf<2>::LCAP : ListConf<3>::LCAP;
+    if (cfg->hbm_budget_bytes > 0 && (long long)(need + sizeof(int) * lcap * ctx->cap) > cfg->hbm_budget_bytes) {
+        epp_destroy(ctx);
+        return EPP_ERR_BUDGET;
+    }
+    if (cudaMalloc(&ctx->nlist, sizeof(int) * lcap * ctx->cap) != cudaSuccess ||
+        cudaMalloc(&ctx->inst_table, sizeof(InstPhys) * n_inst) != cudaSuccess ||
+        cudaMalloc(&ctx->inst_out, sizeof(double) * 9 * n_inst) != cudaSuccess) {
+        epp_destroy(ctx);
+        return EPP_ERR_OUT_OF_MEMORY;
+    }
+    // zeroed lists: a list slot read before any search wrote it holds index 0, in bounds
     if (cudaMemsetAsync(ctx->arena.base, 0, need, ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(ctx->nlist, 0, sizeof(int) * lcap * ctx->cap, ctx->stream) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         epp_destroy(ctx);
@@ -703,6 +760,9 @@ int32_t epp_destroy(epp_ctx* ctx) {
     for (int c = 0; c < 2; ++c)
         if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
     if (ctx->accel) cudaFree(ctx->accel);
+    if (ctx->inst_table) cudaFree(ctx->inst_table);
+    if (ctx->nlist) cudaFree(ctx->nlist);
+    if (ctx->inst_out) cudaFree(ctx->inst_out);
     if (ctx->list_mem) cudaFree(ctx->list_mem);
     if (ctx->list_stage) cudaFree(ctx->list_stage);
     if (ctx->arena.base) cudaFree(ctx->arena.base);
@@ -773,6 +833,21 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     rc |= icol(SI_NCOUNT, m->n_count >= 0 ? ip + (size_t)m->n_count * ldi : nullptr, 0);
     rc |= icol(SI_ALIVE, is_alive, 0);
     rc |= icol(SI_CELL, cell_index, 0);
+    if (m->instance >= 0) {
+        const int32_t* ic = ip + (size_t)m->instance * ldi;
+        for (int k = 0; k < n; ++k)
+            if (ic[k] < 0 || ic[k] >= ctx->n_inst)
+                return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "particle %d: instance %d outside 0..%d", k, ic[k],
+                            ctx->n_inst - 1);
+        rc |= icol(SI_INST, ic, 0);
+    } else {
+        rc |= icol(SI_INST, nullptr, 0);
+    }
+    {
+        const int32_t* tc = ip + (size_t)m->tag * ldi;
+        for (int k = 0; k < n; ++k)
+            if (tc[k] < 0 || tc[k] > 255) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "tag %d out of range", tc[k]);
+    }
     if (rc) return rc;
     {
         bool uni = m->h >= 0;
@@ -851,6 +926,7 @@ int32_t epp_download(epp_ctx* ctx, int32_t* is_alive, int32_t* cell_index, int32
         if (m->tag >= 0) rc |= iget(SI_TAG, ip + (size_t)m->tag * ldi);
         if (m->is_movable >= 0) rc |= iget(SI_MOV, ip + (size_t)m->is_movable * ldi);
         if (m->n_count >= 0) rc |= iget(SI_NCOUNT, ip + (size_t)m->n_count * ldi);
+        if (m->instance >= 0) rc |= iget(SI_INST, ip + (size_t)m->instance * ldi);
     }
     if (rc) return rc;
     const bool want_lists = ctx->lists_valid && ((ip && m->n_index >= 0) ||
@@ -968,7 +1044,7 @@ int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* 
     if (ctx->n == 0) return EPP_OK;
     if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
     IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket, ctx->ihpart, ctx->ihmin};
-    DevPhys P = to_dev(*phys);
+    DevPhys P = dev_phys(ctx, *phys);
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;
         k_integrals<DD><<<kIntegralBlocks, 256, 0, ctx->stream>>>(
@@ -1058,6 +1134,51 @@ int32_t epp_pairs_total(epp_ctx* ctx, int64_t* out) {
     return EPP_OK;
 }
 
+int32_t epp_set_instance_physics(epp_ctx* ctx, int32_t n, const float* dt, const float* c0) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (n != ctx->n_inst || !dt || !c0)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "need dt and c0 for all %d instances", ctx->n_inst);
+    ctx->inst_dt.assign(dt, dt + n);
+    ctx->inst_c0.assign(c0, c0 + n);
+    ctx->inst_dirty = true;
+    ctx->rpn_valid = false;   // the density preview used the previous time steps
+    return EPP_OK;
+}
+
+int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out, int32_t n) {
+    if (!ctx || !phys || !out) return EPP_ERR_INVALID_ARGUMENT;
+    if (n != ctx->n_inst) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "n = %d, context has %d instances", n, ctx->n_inst);
+    if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
+    cudaSetDevice(ctx->dev);
+    DevPhys P = dev_phys(ctx, *phys);
+    auto launch = [&](auto Dt) {
+        constexpr int DD = decltype(Dt)::value;
+        k_integrals_inst<DD><<<ctx->n_inst, 256, 0, ctx->stream>>>(
+            ctx->start[ctx->cur], ctx->dom, ctx->n, ctx->S[ctx->cur], ctx->ncount, P, phys->rho0, phys->gamma,
+            phys->p0, phys->gravity[0], phys->gravity[1], phys->gravity[2], ctx->inst_out);
+    };
+    if (ctx->D == 2) launch(std::integral_constant<int, 2>{});
+    else launch(std::integral_constant<int, 3>{});
+    CK_LAUNCH();
+    std::vector<double> r((size_t)9 * n);
+    CK(cudaMemcpyAsync(r.data(), ctx->inst_out, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < n; ++k) {
+        const double* v = &r[(size_t)9 * k];
+        const double c0 = ctx->inst_c0.empty() ? (double)phys->c0 : (double)ctx->inst_c0[k];
+        out[k].mass_total = v[0];
+        out[k].mass_fluid = v[1];
+        out[k].kinetic = v[2];
+        out[k].potential = v[3];
+        out[k].internal = v[4];
+        out[k].max_speed = v[5];
+        out[k].cfl_dt = v[6] < 1e300 ? 0.1 * v[6] / (c0 + v[5]) : 0.0;
+        out[k].n_alive = (int64_t)v[7];
+        out[k].n_pairs = (int64_t)v[8];
+    }
+    return EPP_OK;
+}
+
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     const int g = lanes_per_particle;
@@ -1074,6 +1195,12 @@ int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle) {
     }
     return EPP_OK;
 }
+
+#ifdef EPP_CHECKED
+extern "C" int32_t epp_checked_slot(int32_t* out4) {
+    return cudaMemcpyFromSymbol(out4, epp_check_slot, sizeof(int) * 4) == cudaSuccess ? EPP_OK : EPP_ERR_CUDA;
+}
+#endif
 
 int32_t epp_set_stream(epp_ctx* ctx, void* stream) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
@@ -1094,7 +1221,7 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
     }
     if (!ctx->rpn_valid || !same_phys(ctx->rpn_phys, *phys)) {
         k_density_preview<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
-            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], to_dev(*phys));
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], dev_phys(ctx, *phys));
         CK_LAUNCH();
     }
     if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->mask_valid = false;

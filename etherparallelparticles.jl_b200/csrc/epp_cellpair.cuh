@@ -141,8 +141,9 @@ struct CPCont {
         const float drho = FUSED ? sum.x : s.drho[i] + sum.x;
         s.drho[i] = drho;
         if (ti == P.fluid || ti == P.wall) {
-            const float rho = __fadd_rn(rho_i, __fmul_rn(drho, P.dt));
-            s.rp4[i] = make_rp4(rho, eos(P, rho));
+            const int inst = inst_of(s.tagm[i]);
+            const float rho = __fadd_rn(rho_i, __fmul_rn(drho, P.dt_of(inst)));
+            s.rp4[i] = make_rp4(rho, eos(P, inst, rho));
         } else {
             s.rp4[i] = make_rp4(rho_i, s.p[i]);
         }
@@ -209,11 +210,14 @@ struct CPMom {
     __device__ __forceinline__ bool wants(int ti) const { return ti == m.P.fluid; }
     struct Self {
         float4 v, rp;
+        float c0;
     };
     struct Nb {
         float4 v, rp;
     };
-    __device__ __forceinline__ Self self(int i) const { return Self{m.s.vm[i], m.s.rp4[i]}; }
+    __device__ __forceinline__ Self self(int i) const {
+        return Self{m.s.vm[i], m.s.rp4[i], m.P.c0_of(inst_of(m.s.tagm[i]))};
+    }
     __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{m.s.vm[j], m.s.rp4[j]}; }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
                                            const PairGeo& g, const TargetConst& tc, HPairCache& pc) const {
@@ -242,7 +246,7 @@ struct CPMom {
             const float rhob = 0.5f * (rpi.x + rpj.x);
             const float az = g.dr2 + 0.01f * hh * hh;
             const float phi = __fdividef(vdx, hinv * az);
-            float force = __fdividef((-P.alpha * P.c0 + P.beta * phi) * phi, rhob);
+            float force = __fdividef((-P.alpha * me.c0 + P.beta * phi) * phi, rhob);
             if (P.visc == EPP_VISCOSITY_REFERENCE) force *= (-vj.w * rpi.w * rpj.w) * dwr;
             else force *= -vj.w * dwr;
             out.x += force * g.dx;
@@ -346,10 +350,10 @@ __global__ void __launch_bounds__(kCPWarps * 32, 4) k_cellpair(CellArgs CA, Act 
         const int c = CA.occ[oc];
         const int cs0 = max(A.start[c], 0);
         const int cs1 = min(A.start[c + 1], n_alive);
-        const int cx = c % n0, cy = (c / n0) % n1, cz = D == 3 ? c / (n0 * n1) : 0;
+        const int cx = c % n0, cy = (c / n0) % n1, cz = c / (n0 * n1);   // 2D: cz = instance layer
         const int x0 = max(cx - 1, 0), x1 = min(cx + 1, n0 - 1);
         const int y0 = max(cy - 1, 0), y1 = min(cy + 1, n1 - 1);
-        const int z0 = D == 3 ? max(cz - 1, 0) : 0, z1 = D == 3 ? min(cz + 1, A.dom.n[2] - 1) : 0;
+        const int z0 = D == 3 ? max(cz - 1, 0) : cz, z1 = D == 3 ? min(cz + 1, A.dom.n[2] - 1) : cz;
         for (int tb = cs0; tb < cs1; tb += CPConf<D>::T) {
             const int TB = min(CPConf<D>::T, cs1 - tb);
             for (int t = lane; t < TB; t += 32) {

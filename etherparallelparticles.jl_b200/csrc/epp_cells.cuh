@@ -34,7 +34,7 @@ __global__ void k_bin_count(int n, DevDomain dom, State s, int* count, int2* cs,
     if (c != dom.n_cells) {
         int tm = s.tagm[i];
         if (movable_of(tm) || c < 0) {
-            c = cell_of<D>(dom, s.xh[i]);
+            c = cell_of<D>(dom, s.xh[i], inst_of(tm));
             if (c < 0) {
                 c = dom.n_cells;
                 st |= EPP_STATUS_KILLED;

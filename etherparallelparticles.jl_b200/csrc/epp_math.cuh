@@ -21,17 +21,30 @@ constexpr int kMaxTags = EPP_MAX_TAGS;
 struct DevDomain {
     int dim;
     int n[3];
-    int n_cells;
+    int n_cells;          // all instances
+    int cells_per_inst;   // n[0] * n[1] * n[2]
+    int n_inst;           // instances stacked as independent layers (2D only)
     float gap_square;
     float first[3], last[3], gap_inv[3];
 };
 
+// Per-instance constants of a batch (each instance has its own column height, so its own c0
+// and time step).
+struct InstPhys {
+    float dt, c0, B, pad;
+};
+
 // Physics constants rounded to FP32 the way `parallel(x)` converts them (Parallel.jl:62-74).
+// `ip` (batches only) overrides dt, c0 and B per instance.
 struct DevPhys {
     float dt, rho0, c0, p0, B;
     float g[3];
     float alpha, beta;
     int gamma, visc, fluid, wall, kahan;
+    const InstPhys* ip;
+    __device__ __forceinline__ float dt_of(int inst) const { return ip ? ip[inst].dt : dt; }
+    __device__ __forceinline__ float c0_of(int inst) const { return ip ? ip[inst].c0 : c0; }
+    __device__ __forceinline__ float B_of(int inst) const { return ip ? ip[inst].B : B; }
 };
 
 // Cell-sorted particle state.  Positions and velocities carry h and m in their w lanes so that
@@ -45,7 +58,7 @@ struct State {
     float* drho;
     float* vol;
     float* p;
-    int* tagm;       // tag | movable << 16
+    int* tagm;       // tag | movable << 8 | instance << 9
     int* id;         // 0-based row of the particle in the caller's matrices
     int* cell;       // 0-based cell (n_cells = dead bin)
     float4* rp4;     // (rho, p, p/rho^2, 1/rho) that the next momentum pass reads
@@ -62,8 +75,32 @@ struct NeighbourList {   // EPP_SEARCH_EMIT_LIST output, column-major [k * cap +
     int cap;
 };
 
-__host__ __device__ inline int tag_of(int tm) { return tm & 0xffff; }
-__host__ __device__ inline int movable_of(int tm) { return (tm >> 16) & 1; }
+// tagm = tag | movable << 8 | instance << 9
+// EPP_CHECKED builds: every index read from the cell offsets, lists and masks is checked before
+// the access; a bad one is recorded (site, index) in epp_check_slot and the access is skipped.
+#ifdef EPP_CHECKED
+__device__ int epp_check_slot[4];
+#define EPP_CHECK(cond, site, idx)                                    \
+    do {                                                              \
+        if (!(cond)) {                                                \
+            if (atomicCAS(&epp_check_slot[0], 0, (site)) == 0) {      \
+                epp_check_slot[1] = (int)(idx);                       \
+                epp_check_slot[2] = (int)(blockIdx.x);                \
+                epp_check_slot[3] = (int)(threadIdx.x);               \
+            }                                                         \
+            return;                                                   \
+        }                                                             \
+    } while (0)
+#else
+#define EPP_CHECK(cond, site, idx) do {} while (0)
+#endif
+
+__host__ __device__ inline int tag_of(int tm) { return tm & 0xff; }
+__host__ __device__ inline int movable_of(int tm) { return (tm >> 8) & 1; }
+__host__ __device__ inline int inst_of(int tm) { return (int)((unsigned)tm >> 9); }
+__host__ __device__ inline int make_tagm(int tag, int movable, int inst) {
+    return (tag & 0xff) | ((movable != 0) << 8) | (inst << 9);
+}
 
 // power(x, Val(N)) of OptimizedFunction.jl:10-42, same association.
 __device__ __forceinline__ float powi(float x, int n) {
@@ -128,8 +165,8 @@ __device__ __forceinline__ float wc2_gradient(float r, float hinv) {
 }
 
 // Tait EOS: p = B ((rho / rho0)^gamma - 1) + p0 (replaces the linear eos of main.jl:64).
-__device__ __forceinline__ float eos(const DevPhys& P, float rho) {
-    return P.B * (powi(__fdiv_rn(rho, P.rho0), P.gamma) - 1.0f) + P.p0;
+__device__ __forceinline__ float eos(const DevPhys& P, int inst, float rho) {
+    return P.B_of(inst) * (powi(__fdiv_rn(rho, P.rho0), P.gamma) - 1.0f) + P.p0;
 }
 
 // (rho, p, p / rho^2, 1 / rho): what a momentum pass needs of a neighbour (Pressure.jl:24-60).
@@ -141,7 +178,7 @@ __device__ __forceinline__ float4 make_rp4(float rho, float p) {
 // 0-based.  Returns -1 when the position is outside the domain (the particle is then killed,
 // NeighbourSearch.jl:41-43).
 template <int D>
-__device__ __forceinline__ int cell_of(const DevDomain& dom, float4 x) {
+__device__ __forceinline__ int cell_of(const DevDomain& dom, float4 x, int inst) {
     float xs[3] = {x.x, x.y, x.z};
 #pragma unroll
     for (int a = 0; a < D; ++a)
@@ -156,7 +193,7 @@ __device__ __forceinline__ int cell_of(const DevDomain& dom, float4 x) {
         lin += i * stride;
         stride *= dom.n[a];
     }
-    return lin;
+    return lin + inst * dom.cells_per_inst;
 }
 
 }  // namespace epp

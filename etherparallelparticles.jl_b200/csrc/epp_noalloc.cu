@@ -51,7 +51,7 @@ __global__ void k_na_bin(int n, DevDomain dom, const float* pos, int* count, int
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 x = make_float4(pos[i], pos[(size_t)n + i], D == 3 ? pos[(size_t)2 * n + i] : 0.0f, 0.0f);
-    int c = cell_of<D>(dom, x);
+    int c = cell_of<D>(dom, x, 0);
     if (c < 0) c = dom.n_cells;
     const int slot = atomicAdd(&count[c], 1);
     cs[i] = make_int2(c, slot);
@@ -118,6 +118,8 @@ int device_domain(const epp_domain& d, DevDomain& o) {
     }
     if (nc > kNaMaxCells) return EPP_ERR_CAPACITY;
     o.n_cells = (int)nc;
+    o.cells_per_inst = (int)nc;
+    o.n_inst = 1;
     return EPP_OK;
 }
 

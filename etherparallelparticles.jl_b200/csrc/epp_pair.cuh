@@ -32,7 +32,7 @@ __device__ __forceinline__ void traverse(const PairArgs& A, int i, float4 xi, in
     int cc[3];
     cc[0] = c % A.dom.n[0];
     cc[1] = (c / A.dom.n[0]) % A.dom.n[1];
-    cc[2] = D == 3 ? c / (A.dom.n[0] * A.dom.n[1]) : 0;
+    cc[2] = c / (A.dom.n[0] * A.dom.n[1]);   // 2D: the instance layer (no coupling across it)
     const float h2ii = harmonic2_exact(xi.w, xi.w);
     unsigned st = 0;
     for (int di = -1; di <= 1; ++di) {
@@ -191,8 +191,9 @@ struct ActSearch {
             s.drho[i] = a.drho;
             // density preview of sContinuity! (Continuity.jl:10-21) + eos, exact FP32 order
             if (ti == P.fluid || ti == P.wall) {
-                const float rho = __fadd_rn(a.rho_i, __fmul_rn(a.drho, P.dt));
-                s.rp4[i] = make_rp4(rho, eos(P, rho));
+                const int inst = inst_of(s.tagm[i]);
+                const float rho = __fadd_rn(a.rho_i, __fmul_rn(a.drho, P.dt_of(inst)));
+                s.rp4[i] = make_rp4(rho, eos(P, inst, rho));
             } else {
                 s.rp4[i] = make_rp4(a.rho_i, s.p[i]);
             }

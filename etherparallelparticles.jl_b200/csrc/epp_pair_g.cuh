@@ -42,10 +42,10 @@ __device__ __forceinline__ void traverse_rows(const PairArgs& A, int i, float4 x
     const int n0 = A.dom.n[0], n1 = A.dom.n[1];
     const int cx = c % n0;
     const int cy = (c / n0) % n1;
-    const int cz = D == 3 ? c / (n0 * n1) : 0;
+    const int cz = c / (n0 * n1);   // 2D: the instance layer (no coupling across it)
     const int x0 = max(cx - 1, 0), x1 = min(cx + 1, n0 - 1);
     const int y0 = max(cy - 1, 0), y1 = min(cy + 1, n1 - 1);
-    const int z0 = D == 3 ? max(cz - 1, 0) : 0, z1 = D == 3 ? min(cz + 1, A.dom.n[2] - 1) : 0;
+    const int z0 = D == 3 ? max(cz - 1, 0) : cz, z1 = D == 3 ? min(cz + 1, A.dom.n[2] - 1) : cz;
     const unsigned amask = A.adj[ti - 1];
     const float h2ii = acc.hc.h2;
     unsigned st = 0;
@@ -159,8 +159,9 @@ struct ActContG {
         s.drho[i] = drho;
         // density preview (sContinuity! of the next step, Continuity.jl:10-21, + eos)
         if (ti == P.fluid || ti == P.wall) {
-            const float rho = __fadd_rn(a.rho_i, __fmul_rn(drho, P.dt));
-            s.rp4[i] = make_rp4(rho, eos(P, rho));
+            const int inst = inst_of(s.tagm[i]);
+            const float rho = __fadd_rn(a.rho_i, __fmul_rn(drho, P.dt_of(inst)));
+            s.rp4[i] = make_rp4(rho, eos(P, inst, rho));
         } else {
             s.rp4[i] = make_rp4(a.rho_i, s.p[i]);
         }
@@ -189,6 +190,7 @@ struct ActMomG {
         float4 rpi;
         float4 vi;
         HConst hc;
+        float c0;
     };
     __device__ __forceinline__ bool wants(int ti) const { return ti == P.fluid; }
     __device__ __forceinline__ void begin(int i, int ti, float4 xi, Acc& a) const {
@@ -197,6 +199,7 @@ struct ActMomG {
             a.rpi = s.rp4[i];
             a.vi = s.vm[i];
             a.hc.init(xi.w, D);
+            a.c0 = P.c0_of(inst_of(s.tagm[i]));
         }
     }
     __device__ __forceinline__ void pair(int i, int j, int ti, int tj, float4 xi, float4 xj,
@@ -234,7 +237,7 @@ struct ActMomG {
             const float rhob = 0.5f * (a.rpi.x + rpj.x);
             const float az = dr2 + 0.01f * hh * hh;
             const float phi = __fdividef(vdx, hinv * az);
-            float force = __fdividef((-P.alpha * P.c0 + P.beta * phi) * phi, rhob);
+            float force = __fdividef((-P.alpha * a.c0 + P.beta * phi) * phi, rhob);
             if (P.visc == EPP_VISCOSITY_REFERENCE) force *= (-vj.w * a.rpi.w * rpj.w) * dwr;
             else force *= -vj.w * dwr;
             a.du[0] += force * dx;
@@ -274,23 +277,24 @@ struct ActMomG {
         const int tm = s.tagm[i];
         int c = s.cell[i];
         const bool alive = c != dom.n_cells;
+        const float dt = P.dt_of(inst_of(tm));
         if (alive && ti == P.fluid && a) {
             float du[3] = {a->du[0], a->du[1], a->du[2]};
             float vv[3] = {v.x, v.y, v.z}, xx[3] = {x.x, x.y, x.z}, cc[3] = {cp.x, cp.y, cp.z};
 #pragma unroll
             for (int k = 0; k < D; ++k) {
                 du[k] = __fadd_rn(du[k], P.g[k]);
-                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], P.dt));
+                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], dt));
             }
 #pragma unroll
             for (int k = 0; k < D; ++k) {
                 if (P.kahan) {
-                    const float y = __fsub_rn(__fmul_rn(vv[k], P.dt), cc[k]);
+                    const float y = __fsub_rn(__fmul_rn(vv[k], dt), cc[k]);
                     const float t = __fadd_rn(xx[k], y);
                     cc[k] = __fsub_rn(__fsub_rn(t, xx[k]), y);
                     xx[k] = t;
                 } else {
-                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], P.dt));
+                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], dt));
                 }
             }
             x.x = xx[0]; x.y = xx[1]; x.z = xx[2];
@@ -304,7 +308,7 @@ struct ActMomG {
         F.vm[i] = v;
         F.comp[i] = cp;
         if (alive && (movable_of(tm) || c < 0)) {
-            c = cell_of<D>(dom, x);
+            c = cell_of<D>(dom, x, inst_of(tm));
             if (c < 0) {
                 c = dom.n_cells;
                 atomicOr(status, EPP_STATUS_KILLED);

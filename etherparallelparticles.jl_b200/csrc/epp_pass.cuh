@@ -35,13 +35,13 @@ struct RowIter {
     __device__ __forceinline__ void init(const PairArgs& A, int c) {
         n0 = A.dom.n[0];
         n1 = A.dom.n[1];
-        const int cx = c % n0, cy = (c / n0) % n1, cz = D == 3 ? c / (n0 * n1) : 0;
+        const int cx = c % n0, cy = (c / n0) % n1, cz = c / (n0 * n1);   // 2D: instance layer
         x0 = max(cx - 1, 0);
         x1 = min(cx + 1, n0 - 1);
         y0 = max(cy - 1, 0);
         y1 = min(cy + 1, n1 - 1);
-        z0 = D == 3 ? max(cz - 1, 0) : 0;
-        z1 = D == 3 ? min(cz + 1, A.dom.n[2] - 1) : 0;
+        z0 = D == 3 ? max(cz - 1, 0) : cz;
+        z1 = D == 3 ? min(cz + 1, A.dom.n[2] - 1) : cz;
         yy = y0;
         zz = z0;
     }

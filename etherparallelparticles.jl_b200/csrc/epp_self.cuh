@@ -15,16 +15,19 @@ __global__ void k_self(int action, const int* start, int n_cells, int n_max, Sta
     const int n_alive = min(start[n_cells], n_max);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_alive) return;
-    const int ti = tag_of(s.tagm[i]);
+    const int tm = s.tagm[i];
+    const int ti = tag_of(tm);
+    const int inst = inst_of(tm);
+    const float dt = P.dt_of(inst);
     if (action == EPP_ACTION_ZERO_DVELOCITY) {
         s.dv[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     } else if (action == EPP_ACTION_DAMBREAK_DENSITY) {
         if (ti == P.fluid || ti == P.wall) {
-            const float rho = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt));
+            const float rho = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], dt));
             s.rho[i] = rho;
             s.drho[i] = 0.0f;
             s.vol[i] = __fdiv_rn(s.vm[i].w, rho);
-            s.p[i] = eos(P, rho);
+            s.p[i] = eos(P, inst, rho);
             if (!isfinite(rho)) atomicOr(status, EPP_STATUS_NONFINITE);
         }
     } else if (action == EPP_ACTION_DAMBREAK_INTEGRATE) {
@@ -35,17 +38,17 @@ __global__ void k_self(int action, const int* start, int n_cells, int n_max, Sta
 #pragma unroll
             for (int k = 0; k < D; ++k) {
                 du[k] = __fadd_rn(du[k], P.g[k]);
-                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], P.dt));
+                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], dt));
             }
 #pragma unroll
             for (int k = 0; k < D; ++k) {
                 if (P.kahan) {
-                    const float y = __fsub_rn(__fmul_rn(vv[k], P.dt), cc[k]);
+                    const float y = __fsub_rn(__fmul_rn(vv[k], dt), cc[k]);
                     const float t = __fadd_rn(xx[k], y);
                     cc[k] = __fsub_rn(__fsub_rn(t, xx[k]), y);
                     xx[k] = t;
                 } else {
-                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], P.dt));
+                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], dt));
                 }
             }
             if (accel) accel[i] = make_float4(du[0], du[1], du[2], 0.0f);
@@ -66,8 +69,9 @@ __global__ void k_density_preview(const int* start, int n_cells, int n_max, Stat
     if (i >= n_alive) return;
     const int ti = tag_of(s.tagm[i]);
     if (ti == P.fluid || ti == P.wall) {
-        const float rho = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt));
-        s.rp4[i] = make_rp4(rho, eos(P, rho));
+        const int inst = inst_of(s.tagm[i]);
+        const float rho = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt_of(inst)));
+        s.rp4[i] = make_rp4(rho, eos(P, inst, rho));
     } else {
         s.rp4[i] = make_rp4(s.rho[i], s.p[i]);
     }
@@ -186,6 +190,58 @@ __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells
     }
 }
 
+// FP64 integrals of every instance of a batch: block k reduces instance k's particles, which are
+// contiguous in cell order (cells of instance k are [k * cells_per_inst, (k + 1) * cells_per_inst)).
+// out[k * 9 + ...] = mass_total, mass_fluid, kinetic, potential, internal, max|v|, h_min,
+// n_alive, n_pairs (the last two as doubles).
+template <int D>
+__global__ void __launch_bounds__(256) k_integrals_inst(const int* start, DevDomain dom, int n_max, State s,
+                                                        const int* ncount, DevPhys P, double rho0, double gam,
+                                                        double p0, double g0, double g1, double g2, double* out) {
+    __shared__ double sh[8][256 / 32];
+    const int k = blockIdx.x;
+    const int lo = max(start[k * dom.cells_per_inst], 0);
+    const int hi = min(start[(k + 1) * dom.cells_per_inst], n_max);
+    const double c0 = (double)P.c0_of(k);
+    const double B = rho0 * c0 * c0 / gam;
+    double v[8] = {0, 0, 0, 0, 0, 0, 1e300, 0};
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const float4 vm = s.vm[i];
+        const double m = (double)vm.w;
+        v[0] += m;
+        v[7] += (double)ncount[i];
+        if (tag_of(s.tagm[i]) != P.fluid) continue;
+        const float4 xh = s.xh[i];
+        v[1] += m;
+        const double u2 = (double)vm.x * vm.x + (double)vm.y * vm.y + (D == 3 ? (double)vm.z * vm.z : 0.0);
+        v[2] += 0.5 * m * u2;
+        v[3] += -m * (g0 * xh.x + g1 * xh.y + (D == 3 ? g2 * xh.z : 0.0));
+        const double r = (double)s.rho[i];
+        v[4] += m * ((B / rho0) * (pow(r / rho0, gam - 1.0) / (gam - 1.0) + rho0 / r - gam / (gam - 1.0)) +
+                     p0 * (1.0 / rho0 - 1.0 / r));
+        v[5] = fmax(v[5], sqrt(u2));
+        v[6] = fmin(v[6], (double)xh.w);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_down_sync(0xffffffffu, v[q], o);
+            v[q] = q == 5 ? fmax(v[q], t) : (q == 6 ? fmin(v[q], t) : v[q] + t);
+        }
+        if (lane == 0) sh[q][warp] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        const int q = threadIdx.x;
+        double a = sh[q][0];
+        for (int w = 1; w < 256 / 32; ++w) a = q == 5 ? fmax(a, sh[q][w]) : (q == 6 ? fmin(a, sh[q][w]) : a + sh[q][w]);
+        out[k * 9 + (q < 7 ? q : 8)] = a;
+        if (q == 0) out[k * 9 + 7] = (double)(hi - lo);
+    }
+}
+
 // Staging columns (by particle row), used by upload and download:
 //   float: position[D], velocity[D], dvelocity[D], mass, volume, density, ddensity, pressure, h
 //   int:   tag, movable, ncount, alive, cell
@@ -199,7 +255,7 @@ __host__ __device__ inline int sf_drho(int D) { return 3 * D + 3; }
 __host__ __device__ inline int sf_p(int D) { return 3 * D + 4; }
 __host__ __device__ inline int sf_h(int D) { return 3 * D + 5; }
 __host__ __device__ inline int sf_count(int D) { return 3 * D + 6; }
-enum { SI_TAG = 0, SI_MOV = 1, SI_NCOUNT = 2, SI_ALIVE = 3, SI_CELL = 4, SI_COUNT = 5 };
+enum { SI_TAG = 0, SI_MOV = 1, SI_NCOUNT = 2, SI_ALIVE = 3, SI_CELL = 4, SI_INST = 5, SI_COUNT = 6 };
 
 // Rows of the caller's matrices -> state in row order (a search sorts it afterwards).
 template <int D>
@@ -216,7 +272,7 @@ __global__ void k_unpack(int n, int n_cells, const float* sf, const int* si, Sta
     s.drho[i] = F(sf_drho(D));
     s.vol[i] = F(sf_vol(D));
     s.p[i] = F(sf_p(D));
-    s.tagm[i] = (I(SI_TAG) & 0xffff) | ((I(SI_MOV) != 0) << 16);
+    s.tagm[i] = make_tagm(I(SI_TAG), I(SI_MOV), I(SI_INST));
     s.id[i] = i;
     const int cell1 = I(SI_CELL);
     s.cell[i] = I(SI_ALIVE) == 1 ? (cell1 >= 1 && cell1 <= n_cells ? cell1 - 1 : -1) : n_cells;
@@ -249,6 +305,7 @@ __global__ void k_pack(int n, int n_cells, float* sf, int* si, State s, const in
     const bool alive = c != n_cells;
     I(SI_ALIVE, alive ? 1 : 0);
     I(SI_CELL, alive && c >= 0 ? c + 1 : 0);
+    I(SI_INST, inst_of(tm));
 }
 
 // Emitted neighbour lists -> reference columns by particle row: nIndex (1-based ids), nRVec,

@@ -97,13 +97,14 @@ class epp_config(C.Structure):
         ("adjacency", C.c_int32 * (EPP_MAX_TAGS * EPP_MAX_TAGS)),
         ("device", C.c_int32),
         ("hbm_budget_bytes", C.c_int64),
+        ("n_instances", C.c_int32),
     ]
 
 
 _COLUMN_FIELDS = [
     "tag", "is_movable", "n_count", "n_index",
     "position", "velocity", "dvelocity", "mass", "volume", "density", "ddensity", "pressure",
-    "gap", "h", "n_rvec", "n_r", "n_w", "n_dw", "n_hinv",
+    "gap", "h", "n_rvec", "n_r", "n_w", "n_dw", "n_hinv", "instance",
 ]
 
 
@@ -166,7 +167,7 @@ def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81
 
 
 def make_config(domain, n_capacity, adjacency, max_neighbour_number=50, max_cell_particles=0,
-                device=0, hbm_budget_bytes=0):
+                device=0, hbm_budget_bytes=0, n_instances=1):
     c = epp_config()
     c.domain = domain
     c.n_capacity = n_capacity
@@ -183,4 +184,5 @@ def make_config(domain, n_capacity, adjacency, max_neighbour_number=50, max_cell
             c.adjacency[i * EPP_MAX_TAGS + j] = int(adjacency[i][j])
     c.device = device
     c.hbm_budget_bytes = hbm_budget_bytes
+    c.n_instances = n_instances
     return c

@@ -10,7 +10,7 @@ import os
 from . import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libepp.so")
+LIB_PATH = os.environ.get("EPP_LIB") or os.path.join(HERE, "libepp.so")
 
 EXPORTS = [
     "epp_abi_version", "epp_device_count", "epp_create", "epp_destroy", "epp_last_error",
@@ -18,6 +18,7 @@ EXPORTS = [
     "epp_get_integrals", "epp_cell_stats", "epp_synchronize", "epp_last_step_timing",
     "epp_pairs_total", "epp_set_accel_output", "epp_get_accel", "epp_set_stream",
     "epp_profile_step", "epp_set_tuning", "epp_cell_sort_noalloc", "epp_noalloc_limits",
+    "epp_set_instance_physics", "epp_get_instance_integrals",
 ]
 
 
@@ -68,6 +69,8 @@ def load(path=LIB_PATH):
     lib.epp_cell_sort_noalloc.argtypes = [P(abi.epp_domain), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, i32p, C.c_void_p]
     lib.epp_noalloc_limits.argtypes = [i32p, i32p, P(C.c_int64)]
+    lib.epp_set_instance_physics.argtypes = [ctx, C.c_int32, f32p, f32p]
+    lib.epp_get_instance_integrals.argtypes = [ctx, P(abi.epp_physics), P(abi.epp_integrals), C.c_int32]
     for name in EXPORTS:
         if name not in ("epp_last_error", "epp_abi_version"):
             getattr(lib, name).restype = C.c_int32
@@ -176,6 +179,18 @@ class Context:
 
     def set_accel_output(self, enable):
         self._ck(self.lib.epp_set_accel_output(self.h, 1 if enable else 0), "epp_set_accel_output")
+
+    def set_instance_physics(self, dt, c0):
+        import numpy as np
+        dt = np.ascontiguousarray(dt, dtype=np.float32)
+        c0 = np.ascontiguousarray(c0, dtype=np.float32)
+        self._ck(self.lib.epp_set_instance_physics(self.h, len(dt), _ptr(dt, C.c_float), _ptr(c0, C.c_float)),
+                 "epp_set_instance_physics")
+
+    def instance_integrals(self, phys, n):
+        out = (abi.epp_integrals * n)()
+        self._ck(self.lib.epp_get_instance_integrals(self.h, C.byref(phys), out, n), "epp_get_instance_integrals")
+        return [o.as_dict() for o in out]
 
     def set_tuning(self, lanes_per_particle):
         self._ck(self.lib.epp_set_tuning(self.h, lanes_per_particle), "epp_set_tuning")

@@ -108,6 +108,9 @@ typedef struct epp_config {
     int32_t adjacency[EPP_MAX_TAGS * EPP_MAX_TAGS]; /* row-major [tag_i-1][tag_j-1] */
     int32_t device;                /* CUDA ordinal */
     int64_t hbm_budget_bytes;      /* 0 = unlimited; creation fails with EPP_ERR_BUDGET above it */
+    int32_t n_instances;           /* batch: independent 2D systems on the same domain (0 or 1 = one);
+                                    * particles carry their instance in the `instance` column and
+                                    * never interact across instances */
 } epp_config;
 
 /* 0-based column indices into the caller's property matrices; -1 = absent.
@@ -118,6 +121,7 @@ typedef struct epp_column_map {
     /* float_properties_ */
     int32_t position, velocity, dvelocity, mass, volume, density, ddensity, pressure, gap, h;
     int32_t n_rvec, n_r, n_w, n_dw, n_hinv;
+    int32_t instance;   /* int column: 0-based instance of a batch (-1: all in instance 0) */
 } epp_column_map;
 
 typedef struct epp_integrals {
@@ -194,8 +198,15 @@ int32_t epp_pairs_total(epp_ctx* ctx, int64_t* out);
 int32_t epp_set_accel_output(epp_ctx* ctx, int32_t enable);
 int32_t epp_get_accel(epp_ctx* ctx, float* out, int32_t n);
 
-/* Pair-pass kernel family: 0 (default) = one thread per particle, neighbours filtered once per
- * step into a mask that the momentum pass reuses; 1 = one warp per occupied cell with a compacted
+/* Batch: per-instance time step and speed of sound (Tait B = rho0 c0^2 / gamma per instance);
+ * they override phys.dt / phys.c0 of epp_step for instance k = 0..n-1. */
+int32_t epp_set_instance_physics(epp_ctx* ctx, int32_t n, const float* dt, const float* c0);
+/* Batch: FP64 integrals of every instance, out[0..n_instances). */
+int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out, int32_t n);
+
+/* Pair-pass kernel family (batches of more than one instance use family 0): 0 (default) = one
+ * warp tile of 32 particles per warp, neighbours filtered once per step into a per-particle
+ * neighbour list that the momentum pass reuses; 1 = one warp per occupied cell with a compacted
  * pair queue; 2, 4, 8, 16 or 32 = that many lanes of a warp per particle.  Chosen by the
  * autotuner; results change only at the FP32 rounding level (neighbour sets are identical). */
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
