@@ -6,7 +6,7 @@ artificial viscosity, symplectic Euler with Kahan positions.  A step is one full
 example/collapse_dry/same/main.jl:166-182 (density update, momentum, integrate, search +
 continuity).  The metric counts the directed active neighbour pairs of each step's search once.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl epp|reference] [--case 2d|3d|2d-small]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl epp|reference] [--case 2d|3d|2d-small|3d-small]
 
 N > 1 (torchrun): the plain path does not shard, so every rank runs an independent replica
 ("replicas only"), no collective on the data path; value = pairs of all ranks / max time.
@@ -18,7 +18,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -29,11 +28,20 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import numpy as np  # noqa: E402
 
-# Algorithmic bytes per particle per step (FP32 state, Int32 ids, compulsory traffic of a fused
-# design with neighbours served on chip, counted once).
+# Algorithmic bytes per particle (FP32 components actually used, Int32 ids; neighbour data served
+# on chip, so each particle's record is read once and written once):
+#   whole step             2D 189 B, 3D 245 B
+#   momentum+integrate+bin reads x, v, rho, p, Kahan c, tag; writes x, v, c, cell   2D 64, 3D 88
+#   search                 reads x, h, tag; writes nCount                          2D 20, 3D 24
+#   continuity             reads x, h, v, m, rho, vol, tag; writes drho, (rho, p)', nCount
+#                                                                                    2D 52, 3D 60
 B_ALG_STEP = {2: 189.0, 3: 245.0}
-B_ALG_MOMENTUM = {2: 64.0, 3: 88.0}   # dominant kernel: momentum + integrate + bin
-STAGES = ["momentum_integrate_bin", "scan", "scatter", "rank_gather", "search_continuity"]
+STAGES = ["momentum_integrate_bin", "scan", "scatter", "rank_gather", "search", "continuity"]
+B_ALG_STAGE = {"momentum_integrate_bin": {2: 64.0, 3: 88.0}, "search": {2: 20.0, 3: 24.0},
+               "continuity": {2: 52.0, 3: 60.0}}
+KERNEL_OF_STAGE = {"momentum_integrate_bin": "k_list<CPMom> (momentum + integrate + bin, fused)",
+                   "search": "k_build (neighbour lists + nCount)",
+                   "continuity": "k_list<CPCont> (continuity + density preview, fused)"}
 
 
 def parse():
@@ -42,7 +50,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="epp", choices=["epp", "reference"])
-    ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small"])
+    ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small", "3d-small"])
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per particle (0 = tuned default)")
     return ap.parse_args()
@@ -54,59 +62,72 @@ def make_case(name):
         return casegen.dam_break_2d(dx=0.002, max_neighbour_number=1), "2D dam break dx=0.002 (500k fluid)"
     if name == "2d-small":
         return casegen.dam_break_2d(dx=0.02, max_neighbour_number=1), "2D dam break dx=0.02 (5k fluid)"
+    if name == "3d-small":
+        return casegen.dam_break_3d(dx=0.01, max_neighbour_number=1), "3D dam break dx=0.01 (600k fluid)"
     return casegen.dam_break_3d(dx=0.005, max_neighbour_number=1), "3D dam break dx=0.005 (4.8M fluid)"
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clock and clock-event reasons, polled through NVML (read-only queries) every ~2 ms
+    from a host thread while the timed region runs; falls back to `nvidia-smi -lms 100`."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown")]
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, torch_device):
+        self.dev = torch_device
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self.stop_flag = threading.Event()
+        self.t = None
+        self.nv = None
+        self.h = None
+
+    def _handle(self):
+        import pynvml as nv
+        import torch
+        nv.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.dev)
+        bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        self.nv = nv
+        self.h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+        self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            self._handle()
         except Exception:
-            self.proc = None
+            self.h = None
+            return
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                bits = get_reasons(self.h)
+                for name, const in self.REASONS:
+                    if bits & getattr(nv, const, 0):
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for k, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(k)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.t is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"], "samples": 0}
+        self.stop_flag.set()
+        self.t.join(timeout=5)
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml, 2 ms poll"}
 
 
 def cpu_reference(case, steps_budget_s=20.0, max_steps=3):
@@ -228,17 +249,18 @@ def main():
 
     # ---- per-kernel device times (instrumented step on the same state, same stream) ----
     with torch.cuda.stream(stream):
-        stage = np.zeros(5)
+        stage = np.zeros(len(STAGES))
         nprof = 5
         for _ in range(nprof):
             if not args.no_flush:
                 flush.fill_(1.0)
             stage += np.array(ctx.profile_step(phys))
         stage /= nprof
-    dom_k = int(np.argmax(stage))
+    # roofline of the dominant pair kernel (the larger of the two pair stages)
+    dom_stage = max(B_ALG_STAGE, key=lambda k: stage[STAGES.index(k)])
+    dom_ms = float(stage[STAGES.index(dom_stage)])
     n = case.n
-    b_mom = B_ALG_MOMENTUM[dim] * n
-    achieved = b_mom / (stage[0] * 1e-3) / 1e9
+    achieved = B_ALG_STAGE[dom_stage][dim] * n / (dom_ms * 1e-3) / 1e9
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -247,9 +269,9 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
-    try:
+    try:   # DRAM bytes of one launch of that kernel from an ncu capture of the same workload
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            tr = json.load(f).get(args.case, {}).get("k_momentum_fused")
+            tr = json.load(f).get(args.case, {}).get(dom_stage)
             if tr:
                 traffic = tr["bytes_per_launch"]
     except Exception:
@@ -281,12 +303,14 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "step_hbm_gbs_algorithmic": step_bytes / (ms_max / args.steps * 1e-3) / 1e9},
             "gpu_launches": 5 * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_momentum_fused", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": KERNEL_OF_STAGE[dom_stage], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback",
-                         "algorithmic_bytes_per_particle": B_ALG_MOMENTUM[dim],
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                         else "fallback 6650 GB/s (of fallback)",
+                         "algorithmic_bytes_per_particle": B_ALG_STAGE[dom_stage][dim],
+                         "kernel_ms": round(dom_ms, 5),
                          "stage_ms": dict(zip(STAGES, [round(x, 5) for x in stage])),
-                         "dominant_stage": STAGES[dom_k]},
+                         "note": "pair kernels are issue/latency bound, not HBM bound (ncu summaries in profiles/)"},
             "clocks": clk,
             "e2e": e2e,
             "device_status": st,
@@ -298,7 +322,7 @@ def main():
                 if dim == 3:   # the 3D oracle keeps 100 neighbour columns: sample a smaller block
                     sample = casegen.dam_break_3d(dx=0.01, max_neighbour_number=1)
                     sample.meta["label"] = "3D dam break dx=0.01 (600k fluid), same physics"
-                cb = cpu_reference(sample, steps_budget_s=20.0, max_steps=2)
+                cb = cpu_reference(sample, steps_budget_s=10.0, max_steps=1000)
                 out["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
             except Exception as exc:  # reported, not fatal
                 out["cpu_baseline"] = {"value": None, "error": str(exc)}

@@ -18,6 +18,7 @@ using namespace epp;
 namespace {
 
 constexpr int kThreads = 128;
+constexpr int kProfileStages = EPP_PROFILE_STAGES;
 constexpr int kIntegralBlocks = 592;   // 4 x 148 SMs
 
 inline int blocks_for(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
@@ -105,11 +106,9 @@ struct epp_ctx {
     epp_physics rpn_phys{};
     int last_crit = EPP_CRITERION_SYMMETRY;
     unsigned adj[kMaxTags]{};
-    int lanes = 0;             // pair-pass family: 0 mask passes, 1 cell-centric, 2..32 lane groups
-    unsigned* mask = nullptr;  // neighbour masks of the last search ([NW * cap])
+    int lanes = 0;             // pair-pass family: 0 warp tiles + lists, 1 cell-centric, 2..32 lane groups
     int* nlist = nullptr;      // neighbour lists of the last search ([LCAP * cap])
-    bool mask_valid = false;   // the mask matches the current order, positions and criterion
-    bool uniform_h = false;    // every uploaded particle has the same smoothing length
+    bool nlist_valid = false;   // the lists match the current order, positions and criterion
     int n_inst = 1;            // batch instances (independent layers of the cell grid)
     InstPhys* inst_table = nullptr;     // device [n_inst]; null when no per-instance physics is set
     std::vector<float> inst_dt, inst_c0;
@@ -168,7 +167,6 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
     b += (size_t)kIntegralBlocks * 8 * 7 + 8 * 8 + 4 * 256;
-    b += (size_t)cap * 4 * (D == 2 ? TileConf<2>::NW : TileConf<3>::NW) + 256;   // neighbour masks
     b += 2 * 256;                                                                  // instance tables (small)
     return b + (1 << 20);
 }
@@ -230,25 +228,37 @@ PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
 
 int lanes_of(const epp_ctx* ctx) { return ctx->lanes; }
 
-// A warp-tile pass.  BUILD: filter the candidates (and store the neighbour mask if `store`);
-// otherwise reuse the mask of the last search at these positions.
-template <int D, bool BUILD, class Act, bool EPI = false>
-int launch_pass(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs, bool store) {
+// Family 0, the search pass: neighbour lists and nCount of set `set` under `crit`.
+template <int D>
+int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
     PairArgs A = pair_args(ctx, set, crit);
-    // the search pass writes the mask and list when `store`; the reuse pass reads the list
-    TileMask M{store || !BUILD ? ctx->mask : nullptr, ctx->cap, store || !BUILD ? ctx->nlist : nullptr};
-    if constexpr (!BUILD) {   // reuse of the last search: walk its neighbour lists
-        k_list<D, Act, EPI><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, ctx->ncount, act, ctx->scan_state,
-                                                                         ctx->n_tiles + 1);
-    } else if (ctx->uniform_h) {
-        k_tile<D, BUILD, Act, EPI, true><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
-                                                                                      ctx->n_tiles + 1);
-    } else {
-        k_tile<D, BUILD, Act, EPI, false><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, act, pairs, ctx->scan_state,
-                                                                                       ctx->n_tiles + 1);
-    }
+    TileMask M{ctx->cap, ctx->nlist};
+    k_build<D><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, ctx->ncount, pairs);
     CK_LAUNCH();
     return EPP_OK;
+}
+
+// Family 0, a pair action over the lists of the last search pass (same order and positions).
+template <int D, class Act, bool EPI = false>
+int launch_list(epp_ctx* ctx, int set, int crit, const Act& act) {
+    PairArgs A = pair_args(ctx, set, crit);
+    TileMask M{ctx->cap, ctx->nlist};
+    k_list<D, Act, EPI><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, ctx->ncount, act, ctx->scan_state,
+                                                                     ctx->n_tiles + 1);
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+// A pair pass of family 0.  BUILD: the search pass first (new lists at the current positions);
+// then the action over the lists (none for the count-only action: the search wrote nCount).
+template <int D, bool BUILD, class Act, bool EPI = false>
+int launch_pass(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs) {
+    if (BUILD) {
+        int rc = launch_build<D>(ctx, set, crit, pairs);
+        if (rc) return rc;
+    }
+    if constexpr (std::is_same<Act, CPCount<D>>::value) return EPP_OK;
+    else return launch_list<D, Act, EPI>(ctx, set, crit, act);
 }
 
 // Launch a G-lane pair pass over `groups` particles (G from the context's tuning).
@@ -335,7 +345,7 @@ int sort_cells(epp_ctx* ctx) {
     k_scatter<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->cs, ctx->start[to], ctx->S[from].id,
                                                            ctx->perm, ctx->status);
     CK_LAUNCH();
-    ctx->mask_valid = false;
+    ctx->nlist_valid = false;
     MoverAll mv{ctx->S[from], ctx->S[to]};
     k_rank_gather<<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->perm, ctx->cs,
                                                                ctx->start[to], mv, ctx->status);
@@ -370,7 +380,7 @@ int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_ph
     DevPhys P = phys ? dev_phys(ctx, *phys) : DevPhys{};
     const bool cont = action == EPP_ACTION_DAMBREAK_CONTINUITY;
     if (emit) {
-        ctx->mask_valid = false;
+        ctx->nlist_valid = false;
         // the emitted list keeps the reference's neighbour order: one thread per particle
         const int grid = blocks_for(ctx->n);
         if (cont) {
@@ -385,13 +395,13 @@ int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_ph
     }
     if (ctx->lanes == 0) {
         int rc;
-        if (fused) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs, true);
-        else if (cont) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncount}, ctx->pairs, true);
-        else rc = launch_pass<D, true>(ctx, set, crit, CPCount<D>{ctx->ncount}, ctx->pairs, true);
-        ctx->mask_valid = rc == EPP_OK;
+        if (fused) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+        else if (cont) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+        else rc = launch_pass<D, true>(ctx, set, crit, CPCount<D>{ctx->ncount}, ctx->pairs);
+        ctx->nlist_valid = rc == EPP_OK;
         return rc;
     }
-    ctx->mask_valid = false;
+    ctx->nlist_valid = false;
     if (ctx->lanes >= 2) {   // lane-group kernels (tuning alternative)
         if (fused) {
             ActContG<D, true, true> act{ctx->S[set], P, ctx->ncount};
@@ -453,8 +463,8 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
         int rc0 = ctx->lanes >= 2 ? launch_pair_g<D, ActMomG<D, true>, true>(ctx, A, mom, nullptr, n)
                   : ctx->lanes == 1 ? launch_cellpair<D, CPMom<D, true>, true>(ctx, c, EPP_CRITERION_SYMMETRY,
                                                                                CPMom<D, true>{mom}, nullptr)
-                                    : launch_pass<D, false, CPMom<D, true>, true>(ctx, c, EPP_CRITERION_SYMMETRY,
-                                                                                  CPMom<D, true>{mom}, nullptr, false);
+                                    : launch_list<D, CPMom<D, true>, true>(ctx, c, EPP_CRITERION_SYMMETRY,
+                                                                           CPMom<D, true>{mom});
         if (rc0) return rc0;
     }
     EPP_MARK(1);
@@ -472,32 +482,46 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
                                                                ctx->start[to], mv, ctx->status);
     CK_LAUNCH();
     EPP_MARK(4);
-    int rc = launch_search_pass<D>(ctx, to, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys,
-                                   false, true);
-    if (rc) return rc;
-    EPP_MARK(5);
+    int rc;
+    if (ctx->lanes == 0) {   // search pass, then continuity over the new lists
+        rc = launch_build<D>(ctx, to, EPP_CRITERION_SYMMETRY, ctx->pairs);
+        if (rc) return rc;
+        EPP_MARK(5);
+        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], mom.P, ctx->ncount});
+        if (rc) return rc;
+    } else {
+        rc = launch_search_pass<D>(ctx, to, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false,
+                                   true);
+        if (rc) return rc;
+        EPP_MARK(5);
+    }
+    EPP_MARK(6);
 #undef EPP_MARK
     return EPP_OK;
 }
 
-// The fused momentum pass reads the neighbour mask of the last search: rebuild it (count-only
+// The fused momentum pass reads the neighbour lists of the last search: rebuild them (count-only
 // search pass at the current positions) when the last search did not leave one.
 template <int D>
-int ensure_mask(epp_ctx* ctx) {
-    if (ctx->lanes != 0 || ctx->mask_valid) return EPP_OK;
-    int rc = launch_pass<D, true>(ctx, ctx->cur, EPP_CRITERION_SYMMETRY, CPCount<D>{ctx->ncount}, nullptr, true);
-    if (rc == EPP_OK) ctx->mask_valid = true;
+int ensure_nlist(epp_ctx* ctx) {
+    if (ctx->lanes != 0 || ctx->nlist_valid) return EPP_OK;
+    int rc = launch_build<D>(ctx, ctx->cur, EPP_CRITERION_SYMMETRY, nullptr);
+    if (rc == EPP_OK) ctx->nlist_valid = true;
     return rc;
 }
 
-template <int D>
-int build_graphs(epp_ctx* ctx, const epp_physics& phys) {
+void drop_graphs(epp_ctx* ctx) {
     for (int c = 0; c < 2; ++c) {
         if (ctx->graph[c]) {
             cudaGraphExecDestroy(ctx->graph[c]);
             ctx->graph[c] = nullptr;
         }
     }
+}
+
+template <int D>
+int build_graphs(epp_ctx* ctx, const epp_physics& phys) {
+    drop_graphs(ctx);
     for (int c = 0; c < 2; ++c) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -523,6 +547,18 @@ int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
     return EPP_OK;
 }
 
+// interaction! with family 0: over the lists of the last search, rebuilt first when this order,
+// these positions or the criterion no longer match them.
+template <int D, class Act>
+int launch_interaction_pass(epp_ctx* ctx, const Act& act) {
+    if (!ctx->nlist_valid) {
+        int rc = launch_build<D>(ctx, ctx->cur, ctx->last_crit, nullptr);
+        if (rc) return rc;
+        ctx->nlist_valid = true;
+    }
+    return launch_list<D>(ctx, ctx->cur, ctx->last_crit, act);
+}
+
 template <int D>
 int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
     PairArgs A = pair_args(ctx, ctx->cur, ctx->last_crit);
@@ -538,18 +574,14 @@ int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
         act.status = ctx->status;
         if (ctx->lanes >= 2) return launch_pair_g<D, decltype(act), false>(ctx, A, act, nullptr, ctx->n);
         if (ctx->lanes == 1) return launch_cellpair<D>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false>{act}, nullptr);
-        if (ctx->mask_valid)
-            return launch_pass<D, false>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false>{act}, nullptr, false);
-        return launch_pass<D, true>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false>{act}, nullptr, false);
+        return launch_interaction_pass<D>(ctx, CPMom<D, false>{act});
     }
     if (ctx->lanes >= 2) {
         ActCountG<D> act{ctx->S[ctx->cur]};
         return launch_pair_g<D, decltype(act), false>(ctx, A, act, nullptr, ctx->n);
     }
     if (ctx->lanes == 1) return launch_cellpair<D>(ctx, ctx->cur, ctx->last_crit, CPCountDv<D>{ctx->S[ctx->cur]}, nullptr);
-    if (ctx->mask_valid)
-        return launch_pass<D, false>(ctx, ctx->cur, ctx->last_crit, CPCountDv<D>{ctx->S[ctx->cur]}, nullptr, false);
-    return launch_pass<D, true>(ctx, ctx->cur, ctx->last_crit, CPCountDv<D>{ctx->S[ctx->cur]}, nullptr, false);
+    return launch_interaction_pass<D>(ctx, CPCountDv<D>{ctx->S[ctx->cur]});
 }
 
 template <int D>
@@ -574,8 +606,8 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
             ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], dev_phys(ctx, phys));
         CK_LAUNCH();
     }
-    if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->mask_valid = false;
-    rc = ensure_mask<D>(ctx);
+    if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->nlist_valid = false;
+    rc = ensure_nlist<D>(ctx);
     if (rc) return rc;
     if (!ctx->graph[0] || !same_phys(ctx->graph_phys, phys) || ctx->graph_accel != accel) {
         ctx->graph_accel = accel;
@@ -591,7 +623,7 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     ctx->searched = true;
     ctx->lists_valid = false;
     ctx->last_crit = EPP_CRITERION_SYMMETRY;
-    ctx->mask_valid = ctx->lanes == 0;
+    ctx->nlist_valid = ctx->lanes == 0;
     return EPP_OK;
 }
 
@@ -715,7 +747,6 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->iticket = a.take<unsigned>(1);
     ctx->ihpart = a.take<double>(kIntegralBlocks);
     ctx->ihmin = a.take<double>(1);
-    ctx->mask = a.take<unsigned>((size_t)ctx->cap * (D == 2 ? TileConf<2>::NW : TileConf<3>::NW));
     ctx->tmp.count = ctx->count;
     ctx->tmp.cs = ctx->cs;
     ctx->tmp.scan_state = ctx->scan_state;
@@ -786,6 +817,7 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     const int D = ctx->D;
     ctx->n = n;
     if (n == 0) {
+        drop_graphs(ctx);
         ctx->searched = false;
         return EPP_OK;
     }
@@ -849,21 +881,6 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
             if (tc[k] < 0 || tc[k] > 255) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "tag %d out of range", tc[k]);
     }
     if (rc) return rc;
-    {
-        bool uni = m->h >= 0;
-        if (uni) {
-            const float* hc = fp + (size_t)m->h * ldf;
-            for (int k = 1; k < n && uni; ++k) uni = hc[k] == hc[0];
-        }
-        if (ctx->uniform_h != uni) {
-            ctx->uniform_h = uni;
-            for (int c = 0; c < 2; ++c)
-                if (ctx->graph[c]) {
-                    cudaGraphExecDestroy(ctx->graph[c]);
-                    ctx->graph[c] = nullptr;
-                }
-        }
-    }
     ctx->cur = 0;
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;
@@ -873,9 +890,10 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     if (D == 2) launch(std::integral_constant<int, 2>{});
     else launch(std::integral_constant<int, 3>{});
     CK_LAUNCH();
+    drop_graphs(ctx);   // the captured launches hold the old particle count
     ctx->searched = false;
     ctx->sorted_once = false;
-    ctx->mask_valid = false;
+    ctx->nlist_valid = false;
     ctx->lists_valid = false;
     ctx->rpn_valid = false;
     ctx->dv_dirty = true;
@@ -1011,7 +1029,7 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (ctx->n == 0) return EPP_OK;
     int rc = ctx->D == 2 ? run_selfaction<2>(ctx, action, phys) : run_selfaction<3>(ctx, action, phys);
     if (action == EPP_ACTION_DAMBREAK_INTEGRATE) {
-        ctx->mask_valid = false;
+        ctx->nlist_valid = false;
         ctx->searched = false;   // positions moved: the next pass needs a search!
         ctx->rpn_valid = false;
     }
@@ -1186,12 +1204,8 @@ int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle) {
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pair-pass family %d not in {0,1,2,4,8,16,32}", g);
     if (g != ctx->lanes) {
         ctx->lanes = g;
-        ctx->mask_valid = false;
-        for (int c = 0; c < 2; ++c)
-            if (ctx->graph[c]) {
-                cudaGraphExecDestroy(ctx->graph[c]);
-                ctx->graph[c] = nullptr;
-            }
+        ctx->nlist_valid = false;
+        drop_graphs(ctx);
     }
     return EPP_OK;
 }
@@ -1224,13 +1238,13 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
             ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], dev_phys(ctx, *phys));
         CK_LAUNCH();
     }
-    if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->mask_valid = false;
+    if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->nlist_valid = false;
     {
-        int rc0 = ctx->D == 2 ? ensure_mask<2>(ctx) : ensure_mask<3>(ctx);
+        int rc0 = ctx->D == 2 ? ensure_nlist<2>(ctx) : ensure_nlist<3>(ctx);
         if (rc0) return rc0;
     }
-    cudaEvent_t ev[6];
-    for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
+    cudaEvent_t ev[kProfileStages + 1];
+    for (int k = 0; k <= kProfileStages; ++k) CK(cudaEventCreate(&ev[k]));
     int rc = ctx->D == 2 ? enqueue_fused_step<2>(ctx, ctx->cur, *phys, ev)
                          : enqueue_fused_step<3>(ctx, ctx->cur, *phys, ev);
     if (!rc) {
@@ -1238,12 +1252,13 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
         ctx->rpn_valid = true;
         ctx->rpn_phys = *phys;
         ctx->lists_valid = false;
-        ctx->mask_valid = ctx->lanes == 0;
-        cudaError_t e = cudaEventSynchronize(ev[5]);
-        for (int k = 0; k < 5 && e == cudaSuccess; ++k) e = cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
+        ctx->nlist_valid = ctx->lanes == 0;
+        cudaError_t e = cudaEventSynchronize(ev[kProfileStages]);
+        for (int k = 0; k < kProfileStages && e == cudaSuccess; ++k)
+            e = cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
         if (e != cudaSuccess) rc = fail(ctx, EPP_ERR_CUDA, "profile events: %s", cudaGetErrorString(e));
     }
-    for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
+    for (int k = 0; k <= kProfileStages; ++k) cudaEventDestroy(ev[k]);
     return rc;
 }
 

@@ -1,7 +1,6 @@
 // epp_self.cuh -- per-particle passes: selfaction! actions, the fused-step gather, FP64
 // integrals, and the pack/unpack kernels between the reference layout and the sorted state.
 #pragma once
-#include "epp_pass.cuh"
 #include "epp_tile.cuh"
 
 namespace epp {

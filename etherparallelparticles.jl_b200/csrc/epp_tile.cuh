@@ -6,16 +6,13 @@
 // 9 (3D) contiguous particle ranges shared by the whole warp.  A warp that crosses a row end
 // (about 2% of them) uses each lane's own stencil instead; both passes make the same choice.
 //
-// Phase A (search pass): the candidates are staged 32 at a time in shared memory with one
-// coalesced 16-byte load per lane; every lane then tests all 32 staged candidates against its own
-// particle with broadcast shared-memory reads -- all lanes in lockstep, no divergence -- using
-// the reference's IEEE criterion, and packs the results into one 32-bit word per chunk: the
-// particle's neighbour mask over the first CAP candidates of the warp's enumeration.  Phase B:
-// each lane walks the set bits of its own mask in one flattened loop (candidate order), checks
-// the active-pair matrix and adds the pair term; candidates past CAP (very dense cells) follow
-// in a per-lane tail loop, in order.  The search pass stores each particle's accepted
-// neighbours (sorted indices, in summation order) as a list; the next momentum pass sees the
-// same positions and cells, so it walks that list (k_list) instead of searching again.
+// The search pass (k_build) stages each chunk of 32 candidates in shared memory with one
+// coalesced load per lane; every lane then tests all 32 staged candidates against its own
+// particle with broadcast shared-memory reads -- all lanes in lockstep -- using the reference's
+// IEEE criterion and the active-pair matrix, and appends its accepted neighbours (sorted
+// indices, candidate order) to its list.  The pair passes (k_list: continuity, momentum, the
+// count actions) then walk each particle's list, one thread per particle, so every lane runs
+// its own neighbour count without waiting for the others' candidates.
 //
 // Summation order per particle = stencil rows (z, y offset), then cell order, then id order
 // inside a cell: deterministic, a rounding-level reordering of the reference's list order.
@@ -30,23 +27,130 @@ __device__ __noinline__ float pair_r2(float hi, float hj) {
     return __fmul_rn(h2, h2);
 }
 
+// Candidate filter: the reference's criterion (IEEE, exact) and the active-pair matrix.
+template <int D>
+__device__ __forceinline__ bool accept(const PairArgs& A, int i, float4 xi, unsigned amask, float h2sq,
+                                       int j, float4 xj, unsigned& st) {
+    if (j == i) return false;
+    const float dx = __fsub_rn(xi.x, xj.x);
+    const float dy = __fsub_rn(xi.y, xj.y);
+    float dr2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+    if (D == 3) {
+        const float dz = __fsub_rn(xi.z, xj.z);
+        dr2 = __fadd_rn(dr2, __fmul_rn(dz, dz));
+    }
+    bool ok;
+    if (A.crit == EPP_CRITERION_DEFAULT) {
+        ok = dr2 <= A.dom.gap_square;
+    } else if (xj.w == xi.w) {
+        ok = dr2 <= h2sq;
+    } else {
+        const float h2 = harmonic2_exact(xi.w, xj.w);
+        ok = dr2 <= __fmul_rn(h2, h2);
+    }
+    if (!ok) return false;
+    const int tj = tag_of(A.s.tagm[j]);
+    if (tj < 1 || tj > A.n_tags) {
+        st |= EPP_STATUS_BAD_TAG;
+        return false;
+    }
+    return (amask >> (tj - 1)) & 1u;
+}
+
+template <int D>
+__device__ __forceinline__ PairGeo geometry(float4 xi, float4 xj) {
+    PairGeo g;
+    g.dx = __fsub_rn(xi.x, xj.x);
+    g.dy = __fsub_rn(xi.y, xj.y);
+    g.dz = D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f;
+    g.dr2 = __fadd_rn(__fmul_rn(g.dx, g.dx), __fmul_rn(g.dy, g.dy));
+    if (D == 3) g.dr2 = __fadd_rn(g.dr2, __fmul_rn(g.dz, g.dz));
+    return g;
+}
+
 template <int D>
 struct TileConf {
-    static constexpr int NR = D == 2 ? 3 : 9;    // stencil rows of one cell row
-    static constexpr int NRMAX = NR;             // ranges of a tile (one cell row) or one particle
-    static constexpr int NW = D == 2 ? 8 : 32;   // mask words per particle (32 candidates each)
-    static constexpr int CAP = 32 * NW;          // candidates covered by the mask
+    static constexpr int NRMAX = D == 2 ? 3 : 9;   // stencil rows: ranges of a tile or of one particle
 };
 
 struct TileMask {
-    unsigned* words;   // [NW * cap]: word w of particle i at w * cap + i
     int cap;
-    int* list;         // [LCAP * cap]: k-th neighbour (sorted index) of particle i at k * cap + i
+    int* list;   // [cap * LCAP]: row i holds the neighbours (sorted indices) of particle i in order
 };
 
 template <int D>
 struct ListConf {
-    static constexpr int LCAP = D == 2 ? 64 : 160;   // neighbours kept per particle
+    static constexpr int LCAP = D == 2 ? 64 : 160;   // neighbours kept per particle (multiple of 4)
+    // 3D: row-major, a particle's entries contiguous (written and read 16 bytes at a time);
+    // 2D: column-major, entry k of particle i at k * cap + i (a warp's reads coalesce).
+    static constexpr bool ROW = D == 3;
+};
+
+// Appends a lane's neighbours to its list; entries past LCAP are counted but not stored.
+// Row-major lists take one int4 store per four neighbours.
+template <int D>
+struct ListWriter {
+    int* base;   // row of the particle (row-major) or its column origin (column-major)
+    int cap;
+    int b0, b1, b2;
+    __device__ __forceinline__ void put(int cnt, int j) {
+        if (cnt >= ListConf<D>::LCAP) return;
+        if (!ListConf<D>::ROW) {
+            base[(size_t)cnt * cap] = j;
+            return;
+        }
+        const int s = cnt & 3;
+        if (s == 0) b0 = j;
+        else if (s == 1) b1 = j;
+        else if (s == 2) b2 = j;
+        else *reinterpret_cast<int4*>(base + (cnt - 3)) = make_int4(b0, b1, b2, j);
+    }
+    // the last partial group of a row (its unused slots are never read)
+    __device__ __forceinline__ void flush(int cnt) {
+        if (ListConf<D>::ROW && cnt < ListConf<D>::LCAP && (cnt & 3))
+            *reinterpret_cast<int4*>(base + (cnt & ~3)) = make_int4(b0, b1, b2, 0);
+    }
+};
+
+template <int D>
+__device__ __forceinline__ ListWriter<D> list_writer(const TileMask& M, int i) {
+    return ListWriter<D>{ListConf<D>::ROW ? M.list + (size_t)i * ListConf<D>::LCAP : M.list + i, M.cap, 0, 0, 0};
+}
+
+// Reads a particle's list in order, the next entries already in flight.
+template <int D>
+struct ListReader {
+    const int* base;
+    int cap, cnt;
+    int4 q, qn;
+    __device__ __forceinline__ void start(const TileMask& M, int i, int n) {
+        cap = M.cap;
+        cnt = n;
+        if (ListConf<D>::ROW) {
+            base = M.list + (size_t)i * ListConf<D>::LCAP;
+            const int4* row = reinterpret_cast<const int4*>(base);
+            q = n > 0 ? row[0] : make_int4(0, 0, 0, 0);
+            qn = n > 4 ? row[1] : make_int4(0, 0, 0, 0);
+        } else {
+            base = M.list + i;
+            q.x = n > 0 ? base[0] : 0;
+        }
+    }
+    // entry k (called with k = 0, 1, 2, ... < cnt)
+    __device__ __forceinline__ int next(int k) {
+        if (!ListConf<D>::ROW) {
+            const int j = q.x;
+            if (k + 1 < cnt) q.x = base[(size_t)(k + 1) * cap];
+            return j;
+        }
+        const int s = k & 3;
+        const int j = s == 0 ? q.x : s == 1 ? q.y : s == 2 ? q.z : q.w;
+        if (s == 3) {   // next group of four, the one after it in flight
+            q = qn;
+            if (k + 5 < cnt) qn = reinterpret_cast<const int4*>(base)[(k + 5) >> 2];
+        }
+        return j;
+    }
 };
 
 // Candidate ranges (contiguous particle index ranges) of a warp tile or of one particle.
@@ -97,17 +201,37 @@ struct TileRanges {
     }
 };
 
-// UH: every particle has the same h (checked at upload), so both criteria reduce to
-// dr^2 <= R^2 with one constant (gap^2, or (2 harmonic(h, h))^2 -- the same IEEE value).
-template <int D, bool BUILD, class Act, bool EPI, bool UH>
-__global__ void __launch_bounds__(128, D == 2 ? 8 : 6) k_tile(PairArgs A, TileMask M, Act act, unsigned long long* pairs,
-                                                 unsigned long long* scan_state, int n_scan_words) {
-    static_assert(BUILD, "the reuse pass is k_list");
-    constexpr int NW = TileConf<D>::NW;
-    constexpr int CAP = TileConf<D>::CAP;
+// Neighbour list of one lane from its own stencil (warps that cross a cell-row end): candidates
+// in order, each filtered with the reference's criterion and the active-pair matrix.
+template <int D>
+__device__ __forceinline__ int lane_stencil_list(const PairArgs& A, ListWriter<D>& L, const TileRanges<D>& R,
+                                                 int i, float4 xi, int ti, float h2sq, unsigned& st) {
+    const unsigned amask = A.adj[ti - 1];
+    int cnt = 0;
+    for (int r = 0; r < R.n; ++r) {
+        for (int j = R.lo[r]; j < R.lo[r] + R.len[r]; ++j) {
+            EPP_CHECK(j >= 0 && j < A.n_max, 14, j);
+            if (!accept<D>(A, i, xi, amask, h2sq, j, A.s.xh[j], st)) continue;
+            L.put(cnt++, j);
+        }
+    }
+    return cnt;
+}
+
+// The search pass: neighbour lists and nCount.  Each chunk of 32 candidates of the warp's union
+// is staged in shared memory (position and index, one coalesced load per lane; the next chunk's
+// loads are issued before the current chunk is tested); every lane tests all 32 against its own
+// particle in lockstep with the reference's IEEE criterion.  A chunk whose candidates share one
+// h (all of them away from material interfaces) is tested against one exact bound per lane;
+// other chunks look the bound up per candidate.  One ballot per tag gives the chunk's candidates
+// of each tag, so a lane keeps only the pairs its row of the active-pair matrix allows, then
+// appends them to its list in candidate order.
+template <int D>
+__global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
+    k_build(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M, int* ncount,
+            unsigned long long* pairs) {
     __shared__ float4 s_x[4][32];
-    if (EPI && blockIdx.x == 0)
-        for (int t = threadIdx.x; t < n_scan_words; t += blockDim.x) scan_state[t] = 0ull;
+    __shared__ int s_j[4][32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int n_alive = min(A.start[A.dom.n_cells], A.n_max);
@@ -122,84 +246,70 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6) k_tile(PairArgs A, TileMa
         const int n0 = A.dom.n[0];
         const int r0 = c_first / n0, r1 = c_last / n0;
         // tile mode: the warp's cells lie in one cell row (all but the ~2% of warps that cross
-        // a row end); otherwise every lane uses its own stencil (same choice in every pass)
+        // a row end); otherwise every lane uses its own stencil
         const bool tiled = r1 == r0;
         TileRanges<D> R;
+        R.n = 0;
+        R.total = 0;
         if (tiled) {
-            R.n = 0;
-            R.total = 0;
             R.stencil(A, r0 % A.dom.n[1], r0 / A.dom.n[1], c_first - r0 * n0, c_last - r0 * n0);
         } else {
             const int c = A.s.cell[min(i, n_alive - 1)];
-            const int ry = (c / n0) % A.dom.n[1], rz = (c / n0) / A.dom.n[1];
-            R.n = 0;
-            R.total = 0;
-            R.stencil(A, ry, rz, c % n0, c % n0);
+            R.stencil(A, (c / n0) % A.dom.n[1], (c / n0) / A.dom.n[1], c % n0, c % n0);
         }
         const float4 xi = on ? A.s.xh[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const int ti = on ? tag_of(A.s.tagm[i]) : 0;
         const bool valid = on && ti >= 1 && ti <= A.n_tags;
-        if (on && !valid) atomicOr(A.status, EPP_STATUS_BAD_TAG);
-        const bool want = valid && act.wants(ti);
-        const TargetConst tc = target_const<D>(on ? xi.w : 1.0f);
         unsigned st = 0;
-        float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        unsigned local_words[NW];   // this pass's mask (dynamic index: local memory, L1)
-        float hc_h = xi.w;                      // criterion cache: last h_j and its exact R^2
-        float hc_r2 = A.crit == EPP_CRITERION_DEFAULT ? A.dom.gap_square : tc.h2sq;
-        // ---- phase A: lockstep filter over staged chunks (search pass only) ----
-        if (BUILD && !tiled) {
-            // per-lane stencil (warps that cross a cell-row end): mask bits of the first CAP candidates
-            unsigned cur = 0u;
-            int k = 0;
-            for (int r = 0; r < R.n && k < CAP; ++r) {
-                for (int j = R.lo[r]; j < R.lo[r] + R.len[r] && k < CAP; ++j, ++k) {
-                    EPP_CHECK(j >= 0 && j < A.n_max, 14, j);
-                    bool ok = false;
-                    if (want) {
-                        const float4 xj = A.s.xh[j];
-                        const float dx = __fsub_rn(xi.x, xj.x);
-                        const float dy = __fsub_rn(xi.y, xj.y);
-                        float dr2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-                        if (D == 3) {
-                            const float dz = __fsub_rn(xi.z, xj.z);
-                            dr2 = __fadd_rn(dr2, __fmul_rn(dz, dz));
-                        }
-                        if (A.crit == EPP_CRITERION_DEFAULT) {
-                            ok = dr2 <= A.dom.gap_square;
-                        } else if (xj.w == xi.w) {
-                            ok = dr2 <= tc.h2sq;
-                        } else {
-                            const float h2 = harmonic2_exact(xi.w, xj.w);
-                            ok = dr2 <= __fmul_rn(h2, h2);
-                        }
-                    }
-                    cur |= (unsigned)ok << (k & 31);
-                    if ((k & 31) == 31) {
-                        local_words[k >> 5] = cur;
-                        if (M.words && on) M.words[(size_t)(k >> 5) * M.cap + i] = cur;
-                        cur = 0u;
-                    }
-                }
-            }
-            if (k & 31) {
-                local_words[k >> 5] = cur;
-                if (M.words && on) M.words[(size_t)(k >> 5) * M.cap + i] = cur;
-            }
-        }
-        if (BUILD && tiled) {
-            // mask words of the first CAP candidates (the rest: tail loop below)
-            const int nchunk = min((R.total + 31) >> 5, NW);
+        if (on && !valid) st |= EPP_STATUS_BAD_TAG;
+        const TargetConst tc = target_const<D>(on ? xi.w : 1.0f);
+        const unsigned amask = valid ? A.adj[ti - 1] : 0u;
+        ListWriter<D> L = list_writer<D>(M, min(i, n_alive - 1));
+        if (!tiled) {
+            if (valid) cnt = lane_stencil_list<D>(A, L, R, i, xi, ti, tc.h2sq, st);
+        } else {
+            const bool dflt = A.crit == EPP_CRITERION_DEFAULT;
+            float hc_h = xi.w;   // exact bound of the last h_j seen
+            float hc_r2 = dflt ? A.dom.gap_square : tc.h2sq;
+            const int nchunk = (R.total + 31) >> 5;
+            // chunk 0 in flight
+            bool real = lane < R.total;
+            int jn = real ? R.at(lane) : 0;
+            float4 xn = real ? A.s.xh[jn] : make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+            int tn = real ? tag_of(A.s.tagm[jn]) : 0;
             for (int ch = 0; ch < nchunk; ++ch) {
-                const int k = (ch << 5) + lane;
-                const int jj = k < R.total ? R.at(k) : 0;
-                EPP_CHECK(jj >= 0 && jj < A.n_max, 12, jj);
-                // padding past the last candidate is far away with h = 0: it fails every test
-                s_x[wib][lane] = k < R.total ? A.s.xh[jj] : make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+                EPP_CHECK(jn >= 0 && jn < A.n_max, 12, jn);
+                // padding past the last candidate is far away: it fails every test
+                s_x[wib][lane] = xn;
+                s_j[wib][lane] = jn;
+                const int tj = tn;
+                const bool real_c = real;
+                if (__ballot_sync(0xffffffffu, real_c && (tj < 1 || tj > A.n_tags))) st |= EPP_STATUS_BAD_TAG;
+                // candidates whose tag this lane's row of the active-pair matrix accepts
+                unsigned allowed = 0u;
+                for (int t = 1; t <= A.n_tags; ++t) {
+                    const unsigned of_t = __ballot_sync(0xffffffffu, real_c && tj == t);
+                    if ((amask >> (t - 1)) & 1u) allowed |= of_t;
+                }
+                // one h for every real candidate of the chunk?
+                const float h0 = __shfl_sync(0xffffffffu, xn.w, 0);
+                const bool one_h = __all_sync(0xffffffffu, !real_c || xn.w == h0);
                 __syncwarp();
+                // next chunk's loads, in flight while this one is tested
+                if (ch + 1 < nchunk) {
+                    const int k = ((ch + 1) << 5) + lane;
+                    real = k < R.total;
+                    jn = real ? R.at(k) : 0;
+                    xn = real ? A.s.xh[jn] : make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+                    tn = real ? tag_of(A.s.tagm[jn]) : 0;
+                }
                 unsigned word = 0u;
-                if (UH) {
-                    const float R2 = A.crit == EPP_CRITERION_DEFAULT ? A.dom.gap_square : tc.h2sq;
+                if (one_h) {
+                    if (h0 != hc_h) {
+                        hc_h = h0;
+                        hc_r2 = dflt ? A.dom.gap_square : h0 == xi.w ? tc.h2sq : pair_r2(xi.w, h0);
+                    }
+                    const float R2 = hc_r2;
 #pragma unroll 16
                     for (int b = 0; b < 32; ++b) {
                         const float4 xj = s_x[wib][b];
@@ -213,7 +323,6 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6) k_tile(PairArgs A, TileMa
                         word |= (unsigned)(dr2 <= R2) << b;
                     }
                 } else {
-                    // a handful of distinct h values: cache the exact bound of the last h_j seen
 #pragma unroll 8
                     for (int b = 0; b < 32; ++b) {
                         const float4 xj = s_x[wib][b];
@@ -226,102 +335,35 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6) k_tile(PairArgs A, TileMa
                         }
                         if (xj.w != hc_h) {
                             hc_h = xj.w;
-                            hc_r2 = A.crit == EPP_CRITERION_DEFAULT ? A.dom.gap_square : pair_r2(xi.w, xj.w);
+                            hc_r2 = dflt ? A.dom.gap_square : xj.w == xi.w ? tc.h2sq : pair_r2(xi.w, xj.w);
                         }
                         word |= (unsigned)(dr2 <= hc_r2) << b;
                     }
                 }
-                if (!want) word = 0u;
-                EPP_CHECK(!(M.words && on) || i < M.cap, 15, i);
-                local_words[ch] = word;
-                if (M.words && on) M.words[(size_t)ch * M.cap + i] = word;
+                word &= allowed;
+                // this lane's neighbours among the chunk, in candidate order
+                while (word) {
+                    const int b = __ffs(word) - 1;
+                    word &= word - 1u;
+                    const int j = s_j[wib][b];
+                    if (j == i) continue;
+                    L.put(cnt++, j);
+                }
                 __syncwarp();
             }
         }
-        // ---- phase B: the lane's own neighbours, in candidate order.  All loads of a neighbour
-        //      are issued together (tag, position, state) and the next mask word is fetched one
-        //      word ahead, so each pair costs one memory round trip. ----
-        if (want) {
-            const int nwords = min((R.total + 31) >> 5, NW);
-            const unsigned amask = A.adj[ti - 1];
-            const typename Act::Self me = act.self(i);
-            HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
-            float4 part = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            int w = 0;
-            unsigned bits = 0u, ahead = 0u;
-            if (nwords > 0) bits = local_words[0];
-            if (nwords > 1) ahead = local_words[1];
-            int r = 0, roff = 0;   // range cursor: k increases monotonically
-            for (;;) {
-                while (!bits && ++w < nwords) {
-                    bits = ahead;
-                    if (w + 1 < nwords) ahead = local_words[w + 1];
-                }
-                if (!bits) break;
-                const int b = __ffs(bits) - 1;
-                bits &= bits - 1u;
-                const int k = (w << 5) + b;
-                while (r < R.n - 1 && k >= roff + R.len[r]) {
-                    roff += R.len[r];
-                    ++r;
-                }
-                const int j = R.lo[r] + (k - roff);
-                EPP_CHECK(j >= 0 && j < A.n_max, 13, j);
-                const int tj = tag_of(A.s.tagm[j]);
-                const float4 xj = A.s.xh[j];
-                const typename Act::Nb nb = act.fetch(j, ti, tj);
-                if (j == i) continue;
-                if (tj < 1 || tj > A.n_tags) {
-                    st |= EPP_STATUS_BAD_TAG;
-                    continue;
-                }
-                if (!((amask >> (tj - 1)) & 1u)) continue;
-                if (M.list && cnt < ListConf<D>::LCAP) M.list[(size_t)cnt * M.cap + i] = j;
-                const float4 c = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc, pc);
-                part.x += c.x;
-                part.y += c.y;
-                part.z += c.z;
-                ++cnt;
-            }
-            sum = part;
-            // candidates past the mask's capacity (very dense cells): filtered inline, in
-            // candidate order, after the mask's pairs -- the order of the stored list too
-            if (R.total > CAP) {
-                int k0 = 0;
-                for (int r = 0; r < R.n; ++r) {
-                    for (int j = R.lo[r] + max(CAP - k0, 0); j < R.lo[r] + R.len[r]; ++j) {
-                        EPP_CHECK(j >= 0 && j < A.n_max, 17, j);
-                        const float4 xj = A.s.xh[j];
-                        if (!accept<D>(A, i, xi, amask, tc.h2sq, j, xj, st)) continue;
-                        const int tj = tag_of(A.s.tagm[j]);
-                        if (M.list && cnt < ListConf<D>::LCAP) M.list[(size_t)cnt * M.cap + i] = j;
-                        const float4 c = act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc, pc);
-                        sum.x += c.x;
-                        sum.y += c.y;
-                        sum.z += c.z;
-                        ++cnt;
-                    }
-                    k0 += R.len[r];
-                }
-            }
-        }
+        L.flush(cnt);
         if (st) atomicOr(A.status, st);
-        if (on) {
-            if (want) act.end(i, ti, sum, cnt);
-            else act.end_idle(i, ti);
-        }
-    } else if (EPI && i < A.n_max) {
-        act.end_idle(i, tag_of(A.s.tagm[i]));
+        if (on) ncount[i] = cnt;
     }
-    if (EPI && w0 < n_alive && i >= n_alive && i < A.n_max) act.end_idle(i, tag_of(A.s.tagm[i]));
     count_pairs(pairs, cnt);
 }
 
 // Neighbours of particle i from its own stencil, filtered inline (used when the list of the last
-// search overflowed); same order as the search pass.
+// search overflowed); same order as the search pass.  Returns the sum with the count in w.
 template <int D, class Act>
 __device__ __noinline__ float4 neighbours_by_stencil(const PairArgs& A, int i, float4 xi, int ti,
-                                                     const TargetConst& tc, const Act& act, int* count) {
+                                                     const TargetConst& tc, const Act& act) {
     const int c = A.s.cell[i];
     const int n0 = A.dom.n[0];
     TileRanges<D> R;
@@ -346,17 +388,18 @@ __device__ __noinline__ float4 neighbours_by_stencil(const PairArgs& A, int i, f
             ++cnt;
         }
     if (st) atomicOr(A.status, st);
-    *count = cnt;
+    sum.w = (float)cnt;
     return sum;
 }
 
-// Momentum over the neighbour list written by the last search pass (same positions, cells and
-// criterion): one thread per particle, a coalesced list read per neighbour, the next index
-// fetched one ahead.  EPI: fused step (integrate + bin for every particle, dead bin included;
-// block 0 clears the scan state).
+// A pair action over the neighbour lists written by the last search pass (same positions,
+// cells and criterion): one thread per particle walking its own list, the next entries already
+// in flight.  EPI: fused momentum step (integrate + bin for every
+// particle, dead bin included; block 0 clears the scan state).
 template <int D, class Act, bool EPI>
-__global__ void __launch_bounds__(128, D == 2 ? 8 : 4) k_list(PairArgs A, TileMask M, const int* ncount, Act act,
-                                                             unsigned long long* scan_state, int n_scan_words) {
+__global__ void __launch_bounds__(128, D == 2 ? 8 : 4)
+    k_list(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M, const int* ncount,
+           const __grid_constant__ Act act, unsigned long long* scan_state, int n_scan_words) {
     if (EPI && blockIdx.x == 0)
         for (int t = threadIdx.x; t < n_scan_words; t += blockDim.x) scan_state[t] = 0ull;
     const int n_alive = min(A.start[A.dom.n_cells], A.n_max);
@@ -374,20 +417,22 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 4) k_list(PairArgs A, TileMa
             if (cnt <= ListConf<D>::LCAP) {
                 const typename Act::Self me = act.self(i);
                 HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
-                int j = cnt > 0 ? M.list[i] : 0;
+                ListReader<D> lr;
+                lr.start(M, i, cnt);
                 for (int k = 0; k < cnt; ++k) {
+                    const int j = lr.next(k);
                     EPP_CHECK(j >= 0 && j < A.n_max, 16, j);
-                    const int jn = k + 1 < cnt ? M.list[(size_t)(k + 1) * M.cap + i] : 0;
                     const int tj = tag_of(A.s.tagm[j]);
                     const float4 xj = A.s.xh[j];
                     const float4 t = act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc, pc);
                     sum.x += t.x;
                     sum.y += t.y;
                     sum.z += t.z;
-                    j = jn;
                 }
             } else {
-                sum = neighbours_by_stencil<D>(A, i, xi, ti, tc, act, &got);
+                sum = neighbours_by_stencil<D>(A, i, xi, ti, tc, act);
+                got = (int)sum.w;
+                sum.w = 0.0f;
             }
             act.end(i, ti, sum, got);
         }

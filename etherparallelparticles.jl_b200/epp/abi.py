@@ -57,6 +57,8 @@ EPP_ACTION_COUNT_NEIGHBOURS = 6
 
 EPP_SEARCH_EMIT_LIST = 1
 
+EPP_PROFILE_STAGES = 6   # momentum+integrate+bin, scan, scatter, rank+gather, search, continuity
+
 EPP_VISCOSITY_REFERENCE = 0
 EPP_VISCOSITY_MONAGHAN = 1
 

@@ -201,8 +201,8 @@ class Context:
                  "epp_set_stream")
 
     def profile_step(self, phys):
-        """One step kernel by kernel; returns the 5 stage times in ms."""
-        out = (C.c_float * 5)()
+        """One step kernel by kernel; returns the EPP_PROFILE_STAGES stage times in ms."""
+        out = (C.c_float * abi.EPP_PROFILE_STAGES)()
         self._ck(self.lib.epp_profile_step(self.h, C.byref(phys), out), "epp_profile_step")
         return list(out)
 

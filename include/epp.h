@@ -216,8 +216,10 @@ int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
 int32_t epp_set_stream(epp_ctx* ctx, void* stream);
 
 /* One dam-break step launched kernel by kernel (no graph) with CUDA events between the
- * kernels; stage_ms[0..4] = momentum+integrate+bin, scan, scatter, rank+gather,
- * search+continuity.  Same results as epp_step(ctx, 1, phys). */
+ * kernels; stage_ms[0 .. EPP_PROFILE_STAGES-1] = momentum+integrate+bin, scan, scatter,
+ * rank+gather, search (neighbour lists), continuity (0 for pair-pass families that fuse the
+ * search and continuity into one kernel).  Same results as epp_step(ctx, 1, phys). */
+#define EPP_PROFILE_STAGES 6
 int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms);
 
 /* Cell-list build that allocates nothing, for callers that must not call cudaMalloc while they
