@@ -302,7 +302,9 @@ def main():
                        "l2": "flushed (256 MB write) before every timed step" if not args.no_flush else "not flushed",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "step_hbm_gbs_algorithmic": step_bytes / (ms_max / args.steps * 1e-3) / 1e9},
-            "gpu_launches": 5 * args.steps,
+            # per fused step: momentum+integrate+bin, scan, scatter, rank+gather, search, continuity
+            # (families other than 0 fuse search and continuity into one kernel)
+            "gpu_launches": (6 if args.lanes == 0 else 5) * args.steps,
             "roofline": {"bound": "hbm", "kernel": KERNEL_OF_STAGE[dom_stage], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks

@@ -90,7 +90,6 @@ struct epp_ctx {
     double* ipartial = nullptr;
     double* iresult = nullptr;
     unsigned* iticket = nullptr;
-    double* ihpart = nullptr;
     double* ihmin = nullptr;
     float4* accel = nullptr;   // optional dv/dt output of the fused momentum pass
     // lazily allocated neighbour lists (EPP_SEARCH_EMIT_LIST)
@@ -745,7 +744,6 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->ipartial = a.take<double>(kIntegralBlocks * 7);
     ctx->iresult = a.take<double>(8);
     ctx->iticket = a.take<unsigned>(1);
-    ctx->ihpart = a.take<double>(kIntegralBlocks);
     ctx->ihmin = a.take<double>(1);
     ctx->tmp.count = ctx->count;
     ctx->tmp.cs = ctx->cs;
@@ -1061,7 +1059,7 @@ int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* 
     std::memset(out, 0, sizeof *out);
     if (ctx->n == 0) return EPP_OK;
     if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
-    IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket, ctx->ihpart, ctx->ihmin};
+    IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket, ctx->ihmin};
     DevPhys P = dev_phys(ctx, *phys);
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;

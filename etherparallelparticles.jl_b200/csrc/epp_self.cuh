@@ -110,25 +110,41 @@ struct MoverFused {
 
 // FP64 integrals: per-block partials, the last block folds them in block order (deterministic).
 struct IntegralsOut {
-    double* partial;       // [n_blocks * 6]
+    double* partial;       // [n_blocks * 7]: the 6 results and min h of each block
     double* result;        // [6]: mass_total, mass_fluid, kinetic, potential, internal, max|v|
     unsigned* ticket;
-    double* hmin_partial;  // [n_blocks]
     double* hmin;          // [1]
 };
+
+// x^n for an integer n >= 0 in FP64 (binary exponentiation; the Tait exponent is an integer).
+__device__ __forceinline__ double powi_d(double x, int n) {
+    double r = 1.0;
+    while (n > 0) {
+        if (n & 1) r *= x;
+        x *= x;
+        n >>= 1;
+    }
+    return r;
+}
+
+// Weakly compressible internal energy per unit mass of the Tait EOS (as the oracle):
+// (B / rho0) ((rho/rho0)^(gamma-1) / (gamma-1) + rho0/rho - gamma/(gamma-1)) + p0 (1/rho0 - 1/rho).
+__device__ __forceinline__ double tait_energy(double r, double rho0, double B, int gam, double p0) {
+    const double g1 = (double)(gam - 1);
+    return (B / rho0) * (powi_d(r / rho0, gam - 1) / g1 + rho0 / r - (double)gam / g1) + p0 * (1.0 / rho0 - 1.0 / r);
+}
 
 template <int D>
 __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells, int n_max, State s,
                                                    DevPhys P, double rho0, double c0,
-                                                   double gam, double p0, double g0, double g1,
+                                                   int gam, double p0, double g0, double g1,
                                                    double g2, IntegralsOut O) {
-    __shared__ double sh[6][256 / 32];
-    __shared__ double shh[256 / 32];
+    __shared__ double sh[7][256 / 32];
     __shared__ bool last;
     const int n_alive = min(start[n_cells], n_max);
-    const double B = rho0 * c0 * c0 / gam;
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    double hmin = 1e300;
+    const double B = rho0 * c0 * c0 / (double)gam;
+    // v: mass, fluid mass, kinetic, potential, internal, max |v| (max), min h (min)
+    double v[7] = {0, 0, 0, 0, 0, 0, 1e300};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_alive; i += gridDim.x * blockDim.x) {
         const float4 vm = s.vm[i];
         const double m = (double)vm.w;
@@ -139,54 +155,44 @@ __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells
         const double u2 = (double)vm.x * vm.x + (double)vm.y * vm.y + (D == 3 ? (double)vm.z * vm.z : 0.0);
         v[2] += 0.5 * m * u2;
         v[3] += -m * (g0 * xh.x + g1 * xh.y + (D == 3 ? g2 * xh.z : 0.0));
-        const double r = (double)s.rho[i];
-        v[4] += m * ((B / rho0) * (pow(r / rho0, gam - 1.0) / (gam - 1.0) + rho0 / r - gam / (gam - 1.0)) +
-                     p0 * (1.0 / rho0 - 1.0 / r));
+        v[4] += m * tait_energy((double)s.rho[i], rho0, B, gam, p0);
         v[5] = fmax(v[5], sqrt(u2));
-        hmin = fmin(hmin, (double)xh.w);
+        v[6] = fmin(v[6], (double)xh.w);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto combine = [](int k, double a, double b) { return k == 5 ? fmax(a, b) : k == 6 ? fmin(a, b) : a + b; };
+    auto block_reduce = [&](double (&x)[7]) {   // fixed tree: deterministic
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+        for (int k = 0; k < 7; ++k) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double t = __shfl_down_sync(0xffffffffu, v[k], o);
-            v[k] = k == 5 ? fmax(v[k], t) : v[k] + t;
+            for (int o = 16; o > 0; o >>= 1) x[k] = combine(k, x[k], __shfl_down_sync(0xffffffffu, x[k], o));
+            if (lane == 0) sh[k][warp] = x[k];
         }
-        if (lane == 0) sh[k][warp] = v[k];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) hmin = fmin(hmin, __shfl_down_sync(0xffffffffu, hmin, o));
-    if (lane == 0) shh[warp] = hmin;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < 6; ++k) {
+        __syncthreads();
+        if (threadIdx.x < 7) {
+            const int k = threadIdx.x;
             double a = sh[k][0];
-            for (int w = 1; w < 256 / 32; ++w) a = k == 5 ? fmax(a, sh[k][w]) : a + sh[k][w];
-            O.partial[blockIdx.x * 6 + k] = a;
+            for (int w = 1; w < 256 / 32; ++w) a = combine(k, a, sh[k][w]);
+            x[k] = a;
         }
-        double hm = shh[0];
-        for (int w = 1; w < 256 / 32; ++w) hm = fmin(hm, shh[w]);
-        O.hmin_partial[blockIdx.x] = hm;
-        __threadfence();
-        last = atomicAdd(O.ticket, 1u) == gridDim.x - 1;
-    }
+    };
+    block_reduce(v);
+    if (threadIdx.x < 7) O.partial[blockIdx.x * 7 + threadIdx.x] = v[threadIdx.x];
+    __threadfence();
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        for (int k = 0; k < 6; ++k) {
-            double a = k == 5 ? 0.0 : 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b) {
-                const double t = ((volatile double*)O.partial)[b * 6 + k];
-                a = k == 5 ? fmax(a, t) : a + t;
-            }
-            O.result[k] = a;
-        }
-        double hm = 1e300;
-        for (unsigned b = 0; b < gridDim.x; ++b) hm = fmin(hm, ((volatile double*)O.hmin_partial)[b]);
-        O.hmin[0] = hm;
-        *O.ticket = 0;
-    }
+    if (threadIdx.x == 0) last = atomicAdd(O.ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last block combines the partials: thread t takes blocks t, t + 256, ... in order
+    double w[7] = {0, 0, 0, 0, 0, 0, 1e300};
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < 7; ++k) w[k] = combine(k, w[k], __ldcg(&O.partial[b * 7 + k]));
+    block_reduce(w);
+    if (threadIdx.x < 6) O.result[threadIdx.x] = w[threadIdx.x];
+    if (threadIdx.x == 6) O.hmin[0] = w[6];
+    if (threadIdx.x == 0) *O.ticket = 0;
 }
 
 // FP64 integrals of every instance of a batch: block k reduces instance k's particles, which are
@@ -195,14 +201,14 @@ __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells
 // n_alive, n_pairs (the last two as doubles).
 template <int D>
 __global__ void __launch_bounds__(256) k_integrals_inst(const int* start, DevDomain dom, int n_max, State s,
-                                                        const int* ncount, DevPhys P, double rho0, double gam,
+                                                        const int* ncount, DevPhys P, double rho0, int gam,
                                                         double p0, double g0, double g1, double g2, double* out) {
     __shared__ double sh[8][256 / 32];
     const int k = blockIdx.x;
     const int lo = max(start[k * dom.cells_per_inst], 0);
     const int hi = min(start[(k + 1) * dom.cells_per_inst], n_max);
     const double c0 = (double)P.c0_of(k);
-    const double B = rho0 * c0 * c0 / gam;
+    const double B = rho0 * c0 * c0 / (double)gam;
     double v[8] = {0, 0, 0, 0, 0, 0, 1e300, 0};
     for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const float4 vm = s.vm[i];
@@ -215,9 +221,7 @@ __global__ void __launch_bounds__(256) k_integrals_inst(const int* start, DevDom
         const double u2 = (double)vm.x * vm.x + (double)vm.y * vm.y + (D == 3 ? (double)vm.z * vm.z : 0.0);
         v[2] += 0.5 * m * u2;
         v[3] += -m * (g0 * xh.x + g1 * xh.y + (D == 3 ? g2 * xh.z : 0.0));
-        const double r = (double)s.rho[i];
-        v[4] += m * ((B / rho0) * (pow(r / rho0, gam - 1.0) / (gam - 1.0) + rho0 / r - gam / (gam - 1.0)) +
-                     p0 * (1.0 / rho0 - 1.0 / r));
+        v[4] += m * tait_energy((double)s.rho[i], rho0, B, gam, p0);
         v[5] = fmax(v[5], sqrt(u2));
         v[6] = fmin(v[6], (double)xh.w);
     }

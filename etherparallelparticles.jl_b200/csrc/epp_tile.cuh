@@ -456,12 +456,39 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 4)
                 HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
                 ListReader<D> lr;
                 lr.start(M, i, cnt);
+                if (D == 2) {   // 64 registers: no room for a second neighbour record
+                    for (int k = 0; k < cnt; ++k) {
+                        const int j = lr.next(k);
+                        EPP_CHECK(j >= 0 && j < A.n_max, 16, j);
+                        const int tj = tag_of(A.s.tagm[j]);
+                        const float4 xj = A.s.xh[j];
+                        const float4 t =
+                            act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc, pc);
+                        sum.x += t.x;
+                        sum.y += t.y;
+                        sum.z += t.z;
+                    }
+                    act.end(i, ti, sum, got);
+                    return;
+                }
+                // 3D: software pipeline, neighbour k + 1's loads in flight while k's term runs
+                int jn = cnt > 0 ? lr.next(0) : 0;
+                EPP_CHECK(jn >= 0 && jn < A.n_max, 16, jn);
+                int tn = cnt > 0 ? A.s.tagm[jn] : 0;
+                float4 xn = cnt > 0 ? A.s.xh[jn] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                typename Act::Nb nn = act.fetch(jn, ti, 0);
                 for (int k = 0; k < cnt; ++k) {
-                    const int j = lr.next(k);
-                    EPP_CHECK(j >= 0 && j < A.n_max, 16, j);
-                    const int tj = tag_of(A.s.tagm[j]);
-                    const float4 xj = A.s.xh[j];
-                    const float4 t = act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc, pc);
+                    const int tj = tag_of(tn);
+                    const float4 xj = xn;
+                    const typename Act::Nb nb = nn;
+                    if (k + 1 < cnt) {
+                        jn = lr.next(k + 1);
+                        EPP_CHECK(jn >= 0 && jn < A.n_max, 16, jn);
+                        tn = A.s.tagm[jn];
+                        xn = A.s.xh[jn];
+                        nn = act.fetch(jn, ti, 0);
+                    }
+                    const float4 t = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc, pc);
                     sum.x += t.x;
                     sum.y += t.y;
                     sum.z += t.z;
