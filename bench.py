@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="epp", choices=["epp", "reference"])
-    ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small", "3d-small"])
+    ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small", "3d-small", "batch"])
+    ap.add_argument("--instances", type=int, default=256, help="batch: number of instances")
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per particle (0 = tuned default)")
     return ap.parse_args()
@@ -69,7 +70,7 @@ def make_case(name):
 
 class Clocks:
     """SM clock and clock-event reasons, polled through NVML (read-only queries) every ~2 ms
-    from a host thread while the timed region runs; falls back to `nvidia-smi -lms 100`."""
+    from a host thread while the timed region runs."""
 
     REASONS = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
@@ -164,6 +165,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.case == "batch":
+        return run_reference_batch(args)
     case, label = make_case(args.case)
     case.meta["label"] = label
     probe = cpu_reference(case, steps_budget_s=0.0, max_steps=1)      # cost of one step
@@ -182,10 +185,222 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def run_reference_batch(args):
+    """--impl reference --case batch: the oracle runs simulations one at a time (the reference has
+    no batched form); sims/s from the mean step time of every 16th instance of the mix."""
+    from epp import casegen
+    cols = casegen.batch_columns(args.instances, seed=0)
+    sample = list(range(0, len(cols), 16))
+    per_step, cores, n_p = [], 1, 0
+    for k in sample:
+        case = casegen.dam_break_2d(dx=0.01, column=cols[k], max_neighbour_number=1)
+        case.meta["label"] = "instance %d" % k
+        res = cpu_reference(case, steps_budget_s=1.0, max_steps=max(1, min(args.steps, 10)))
+        per_step.append(res["seconds_per_step"])
+        cores = res["cores"]
+        n_p += case.n
+    val = 1.0 / (2000 * float(np.mean(per_step)))
+    sample_txt = "instances %s of the %d-instance mix (%d particles), mean %.2f ms/step" % (
+        sample, len(cols), n_p, 1e3 * float(np.mean(per_step)))
+    out = {"metric": "batched sims/s (256-instance 2D dam-break mix, 2000 steps per simulation)",
+           "value": val, "unit": "sims/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": max(1, min(args.steps, 10)), "warmup": 0, "ms_per_step": 1e3 * float(np.mean(per_step)),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded column sizes, numpy default_rng(0))",
+           "config": {"workload": "%d uneven 2D dam breaks, dx=0.01 m" % len(cols), "instances": len(cols)},
+           "cpu_baseline": {"value": val, "unit": "sims/s", "cores": cores, "kind": "port", "sample": sample_txt},
+           "e2e": {"value": val, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def energy(ig):
+    return ig["kinetic"] + ig["potential"] + ig["internal"]
+
+
+def run_batch(args):
+    """--case batch: the 256-instance mix of uneven 2D dam breaks (column width U[0.5, 1.5] m,
+    height U[1.0, 2.5] m, seed 0, dx = 0.01 m, each instance with its own c0 and dt), every pass
+    one launch over all instances.  value = sims/s at 2000 steps per simulation, against the
+    plain path running the same instances one at a time (each timed alone on the device)."""
+    import torch
+    import torch.distributed as dist
+    from epp import abi, casegen
+    from epp.algorithm import DeviceParticleSystem
+    from epp.classes import NeighbourSystem
+    import oracle_lib
+    from helpers import config_for
+
+    SIM_STEPS = 2000
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    SYM, CONT = abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY
+    b = casegen.dam_break_batch(args.instances, seed=0, dx=0.01)
+    phys = b.physics
+    ns = NeighbourSystem(b.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    dps = DeviceParticleSystem(b.ps, ns, device=local, n_instances=b.n_instances)
+    ctx = dps.ctx
+    ctx.set_instance_physics(b.inst_dt, b.inst_c0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    dps.syncto()
+    ctx.search(SYM, CONT, phys, 0)
+    e0 = [energy(x) for x in ctx.instance_integrals(phys, b.n_instances)]
+    W = max(args.warmup, 3)
+    with torch.cuda.stream(stream):
+        ctx.step(W, phys)
+    ctx.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = Clocks(local)
+    p0 = ctx.pairs_total()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            ctx.step(1, phys)
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    st = ctx.synchronize(raise_on_status=False)
+    ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
+    pairs = ctx.pairs_total() - p0
+    e1 = [energy(x) for x in ctx.instance_integrals(phys, b.n_instances)]
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+    step_ms = ms / args.steps
+    sims_s = world * b.n_instances / (SIM_STEPS * step_ms * 1e-3)
+    with torch.cuda.stream(stream):
+        stage = np.mean([ctx.profile_step(phys) for _ in range(3)], axis=0)
+    # end to end through the C ABI with pinned host buffers (upload, search, K x (step +
+    # per-instance integrals read back), download)
+    h = dps.host
+    ip = np.asfortranarray(torch.from_numpy(np.asfortranarray(h.int_properties)).pin_memory().numpy())
+    fp = np.asfortranarray(torch.from_numpy(np.asfortranarray(h.float_properties)).pin_memory().numpy())
+    alive = torch.from_numpy(h.is_alive.copy()).pin_memory().numpy()
+    cell = torch.from_numpy(h.cell_index.copy()).pin_memory().numpy()
+    ctx.download(alive, cell, ip, fp, dps.cmap)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.upload(h.n_particles, alive, cell, ip, fp, dps.cmap)
+    ctx.search(SYM, CONT, phys, 0)
+    for _ in range(args.steps):
+        ctx.step(1, phys)
+        ctx.instance_integrals(phys, b.n_instances)
+    ctx.download(alive, cell, ip, fp, dps.cmap)
+    t_e2e = time.perf_counter() - t0
+    n_cols = 2 * 3 + 6 + 5   # float columns moved (x, v, dv, m, V, rho, drho, p, h) + int (tag, mov, ncount, alive, cell, instance)
+    bytes_io = h.n_particles * 4 * (n_cols + 1)
+    dps.close()
+    out = None
+    if rank == 0:
+        # plain path: every instance alone, one after the other, on one context sized for the
+        # largest (the state of one instance stays resident in L2 between its own steps)
+        K2 = 20
+        cases = [casegen.dam_break_2d(dx=0.01, column=col, max_neighbour_number=1) for col in b.meta["columns"]]
+        big = max(cases, key=lambda c: c.n)
+        ns1 = NeighbourSystem(big.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+        plain = DeviceParticleSystem(big.ps, ns1, device=local)
+        pctx = plain.ctx
+        pctx.set_stream(stream.cuda_stream)
+        per_step = []
+        for c in cases:
+            q = c.ps
+            pctx.upload(q.n_particles, q.is_alive, q.cell_index, q.int_properties, q.float_properties, plain.cmap)
+            pctx.search(SYM, CONT, c.physics, 0)
+            with torch.cuda.stream(stream):
+                pctx.step(3, c.physics)
+            torch.cuda.synchronize()
+            a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                a_.record(stream)
+                pctx.step(K2, c.physics)
+                b_.record(stream)
+            torch.cuda.synchronize()
+            per_step.append(a_.elapsed_time(b_) / K2)
+        plain.close()
+        plain_sims_s = len(cases) / (SIM_STEPS * sum(per_step) * 1e-3)
+        # energy drift against the FP64 oracle for sampled instances (the smallest three and the
+        # largest), same number of steps from the same initial state
+        S = W + args.steps
+        order = sorted(range(len(cases)), key=lambda k: cases[k].n)
+        sample = order[:3] + order[-1:]
+        drift = {}
+        oracle_lib.set_threads(os.cpu_count() or 1)
+        for k in sample:
+            c = casegen.dam_break_2d(dx=0.01, column=b.meta["columns"][k], max_neighbour_number=60)
+            nso = NeighbourSystem(c.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=60)
+            o = oracle_lib.Oracle(config_for(c.ps, nso, max_cell_particles=64), 64)
+            q = c.ps
+            o.upload(q.n_particles, q.is_alive, q.cell_index, q.int_properties, q.float_properties, q.column_map())
+            o.search(SYM, CONT, c.physics)
+            o0 = energy(o.integrals(c.physics))
+            o.step(S, c.physics)
+            o1 = energy(o.integrals(c.physics))
+            dg, do = (e1[k] - e0[k]) / abs(e0[k]), (o1 - o0) / abs(o0)
+            drift[str(k)] = {"particles": c.n, "gpu_fp32": dg, "oracle_fp64": do, "abs_diff": abs(dg - do)}
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except Exception:
+            pass
+        out = {
+            "metric": "batched sims/s (256-instance 2D dam-break mix, 2000 steps per simulation)",
+            "value": sims_s, "unit": "sims/s", "n_gpus": world, "steps": args.steps, "warmup": W,
+            "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded column sizes, numpy default_rng(0))",
+            "config": {"workload": "%d uneven 2D dam breaks, width U[0.5,1.5] m, height U[1.0,2.5] m, dx=0.01 m"
+                       % b.n_instances, "instances": b.n_instances, "particles": b.n,
+                       "fluid": b.meta["n_fluid"], "walls": b.meta["n_wall"],
+                       "fluid_per_instance": [min(b.meta["inst_n_fluid"]), max(b.meta["inst_n_fluid"])],
+                       "cells": b.meta["n_cells"], "resort": "every step",
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": "instances per GPU, replicas across GPUs" if world > 1 else "single GPU"},
+            "plain_path": {"sims_per_s": plain_sims_s, "ms_per_instance_step_mean": float(np.mean(per_step)),
+                           "ms_per_instance_step_range": [float(min(per_step)), float(max(per_step))],
+                           "method": "each instance alone on the plain path (epp_step graph), %d steps "
+                                     "timed per instance by CUDA events, summed over the %d instances"
+                                     % (K2, len(cases))},
+            "speedup_vs_plain": sims_s / world / plain_sims_s,
+            "pairs_per_s": pairs / (ms * 1e-3) if world == 1 else None,
+            "energy_drift": {"steps": S, "bar": 1e-4, "instances": drift,
+                             "max_abs_diff": max(v["abs_diff"] for v in drift.values())},
+            "gpu_launches": 6 * args.steps,
+            "roofline": {"bound": "hbm", "stage_ms": dict(zip(STAGES, [round(float(x), 4) for x in stage])),
+                         "achieved": B_ALG_STEP[2] * b.n / (step_ms * 1e-3) / 1e9,
+                         "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
+                         "frac": B_ALG_STEP[2] * b.n / (step_ms * 1e-3) / 1e9 / peaks.get("hbm_gbs", 6650.0),
+                         "traffic": None, "note": "whole step, algorithmic bytes; pair kernels are issue/latency bound"},
+            "clocks": clk,
+            "e2e": {"value": b.n_instances * args.steps / SIM_STEPS / t_e2e, "unit": "sims/s",
+                    "h2d_bytes_per_step": int(bytes_io / args.steps), "d2h_bytes_per_step": int(bytes_io / args.steps + 72 * b.n_instances),
+                    "seconds": t_e2e,
+                    "note": "upload + search + K x (step + per-instance integrals read back) + download, host clock"},
+            "device_status": st,
+        }
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.case == "batch":
+        return run_batch(args)
     import torch
     import torch.distributed as dist
     from epp import abi, casegen

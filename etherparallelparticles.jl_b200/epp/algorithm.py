@@ -19,14 +19,16 @@ defaultSelfaction = abi.EPP_ACTION_NONE
 class DeviceParticleSystem:
     """The device side of a particle system: an epp context sized for the host system."""
 
-    def __init__(self, host_ps, neighbour_system, device=0, hbm_budget_bytes=0, column_names=None):
+    def __init__(self, host_ps, neighbour_system, device=0, hbm_budget_bytes=0, column_names=None,
+                 n_instances=1):
         self.host = host_ps
         self.ns = neighbour_system
         adj = neighbour_system.active_pair.adjacency_matrix.tolist()
         self.config = abi.make_config(host_ps.domain.to_abi(), host_ps.n_capacity, adj,
                                       max_neighbour_number=neighbour_system.max_neighbour_number,
                                       max_cell_particles=neighbour_system.max_cell_particles,
-                                      device=device, hbm_budget_bytes=hbm_budget_bytes)
+                                      device=device, hbm_budget_bytes=hbm_budget_bytes,
+                                      n_instances=n_instances)
         self.ctx = Context(self.config)
         self.cmap = host_ps.column_map(column_names)
         self.physics = None

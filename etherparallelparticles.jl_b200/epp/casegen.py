@@ -77,8 +77,10 @@ class DamBreakCase:
         return self.ps.n_particles
 
 
-def _layout(dim, max_nb):
+def _layout(dim, max_nb, instance=False):
     ints = OrderedDict([("Tag", 1), ("IsMovable", 1), ("nCount", 1), ("nIndex", max_nb)])
+    if instance:
+        ints["Instance"] = 1   # batch: 0-based instance of the particle (no reference counterpart)
     floats = OrderedDict([
         ("PositionVec", dim), ("VelocityVec", dim), ("dVelocityVec", dim), ("AccelerationVec", dim),
         ("Mass", 1), ("Volume", 1), ("Density", 1), ("dDensity", 1), ("Pressure", 1), ("Gap", 1),
@@ -92,13 +94,24 @@ def dam_break_2d(dx=0.02, tank=(4.0, 3.0), column=(1.0, 2.0), wall_layers=3, h_f
                  max_neighbour_number=40, reference_quirk=False, kahan=1,
                  viscosity=abi.EPP_VISCOSITY_REFERENCE, alpha=0.1, beta=0.1):
     """2D dry dam break (casegen.jl:17-146 geometry; benchmark physics)."""
-    x0, y0 = 0.0, 0.0
-    ww = wall_layers * dx
-    h = h_factor * dx
-    gap = 2.0 * h
     height = column[1]
     c0 = 10.0 * math.sqrt(2.0 * GRAVITY * height)
-    domain = Domain2D(gap, x0 - ww, y0 - ww, x0 + tank[0] + ww, y0 + tank[1] + ww)
+    domain = _tank_domain_2d(dx, tank, wall_layers, h_factor)
+    parts = _dam_parts_2d(dx, tank, column, wall_layers, reference_quirk)
+    return _assemble(2, domain, parts, h_factor, height, c0, max_neighbour_number, kahan,
+                     viscosity, alpha, beta, {"dx": dx, "tank": tank, "column": column,
+                                              "reference_quirk": reference_quirk})
+
+
+def _tank_domain_2d(dx, tank, wall_layers, h_factor):
+    ww = wall_layers * dx
+    return Domain2D(2.0 * h_factor * dx, -ww, -ww, tank[0] + ww, tank[1] + ww)
+
+
+def _dam_parts_2d(dx, tank, column, wall_layers, reference_quirk=False):
+    """Fluid column at the tank's lower-left corner and 3-layer floor and side walls."""
+    x0, y0 = 0.0, 0.0
+    ww = wall_layers * dx
     parts = []
     fp, fv, fg = lattice([x0, y0], [x0 + column[0], y0 + column[1]], dx, reference_quirk)
     parts.append((fp, fv, fg, FLUID_TAG, 1))
@@ -109,9 +122,7 @@ def dam_break_2d(dx=0.02, tank=(4.0, 3.0), column=(1.0, 2.0), wall_layers=3, h_f
     ]:
         wp, wv, wg = lattice(lo, hi, dx, reference_quirk)
         parts.append((wp, wv, wg, WALL_TAG, 0))
-    return _assemble(2, domain, parts, h_factor, height, c0, max_neighbour_number, kahan,
-                     viscosity, alpha, beta, {"dx": dx, "tank": tank, "column": column,
-                                              "reference_quirk": reference_quirk})
+    return parts
 
 
 def dam_break_3d(dx=0.005, tank=(3.2, 1.0, 1.0), column=(1.0, 1.0, 0.6), wall_layers=3,
@@ -143,13 +154,10 @@ def dam_break_3d(dx=0.005, tank=(3.2, 1.0, 1.0), column=(1.0, 1.0, 0.6), wall_la
                      viscosity, alpha, beta, {"dx": dx, "tank": tank, "column": column})
 
 
-def _assemble(dim, domain, parts, h_factor, height, c0, max_nb, kahan, viscosity, alpha, beta, meta):
+def _state(dim, parts, h_factor, height, c0):
+    """Per-particle initial state of one case: hydrostatic density on the Tait EOS with this
+    case's c0 and column height, Mass = Density .* Volume, H = Gap * h_factor."""
     n = sum(p[0].shape[0] for p in parts)
-    ints, floats = _layout(dim, max_nb)
-    params = OrderedDict([("rho0", RHO0), ("p0", 0.0), ("FLUID_TAG", FLUID_TAG),
-                          ("WALL_TAG", WALL_TAG), ("gap0", meta["dx"]),
-                          ("h0", h_factor * meta["dx"])])
-    ps = ParticleSystem(domain, n, ints, floats, params)
     pos = np.concatenate([p[0] for p in parts])
     vol = np.concatenate([np.full(p[0].shape[0], p[1], np.float32) for p in parts])
     pg = np.concatenate([np.full(p[0].shape[0], p[2], np.float32) for p in parts])
@@ -162,27 +170,104 @@ def _assemble(dim, domain, parts, h_factor, height, c0, max_nb, kahan, viscosity
     rho = rho.astype(np.float32)
     B = tait_b(RHO0, c0, GAMMA)
     p = (B * ((rho.astype(np.float64) / RHO0) ** GAMMA - 1.0)).astype(np.float32)
-    ps["PositionVec"] = pos
-    ps["Volume"] = vol
-    ps["Gap"] = pg
-    ps["Tag"] = tag
-    ps["IsMovable"] = mov
-    ps["Density"] = rho
-    ps["Mass"] = (rho * vol).astype(np.float32)          # Mass = Density .* Volume (casegen.jl:85)
-    ps["H"] = (pg * np.float32(h_factor)).astype(np.float32)   # H = Gap * 1.5 (casegen.jl:86)
-    ps["Pressure"] = p
-    h0 = np.float32(h_factor * meta["dx"])
+    return {"PositionVec": pos, "Volume": vol, "Gap": pg, "Tag": tag, "IsMovable": mov, "Density": rho,
+            "Mass": (rho * vol).astype(np.float32),            # Mass = Density .* Volume (casegen.jl:85)
+            "H": (pg * np.float32(h_factor)).astype(np.float32),  # H = Gap * 1.5 (casegen.jl:86)
+            "Pressure": p}
+
+
+def _time_step(h_factor, dx, c0):
+    """(float32 c0, dt = 0.1 h0 / c0 (main.jl:68) rounded to float32)."""
+    h0 = np.float32(h_factor * dx)
     c0f = np.float32(c0)
-    dt = float(np.float32(0.1 * float(h0) / float(c0f)))   # dt = 0.1 h0 / c0 (main.jl:68)
+    return float(c0f), float(np.float32(0.1 * float(h0) / float(c0f)))
+
+
+def _physics(dim, dt, c0, kahan, viscosity, alpha, beta):
     grav = (0.0, -GRAVITY, 0.0) if dim == 2 else (0.0, 0.0, -GRAVITY)
-    physics = abi.make_physics(dt, rho0=RHO0, c0=float(c0f), p0=0.0, gamma=GAMMA, gravity=grav,
-                               alpha=alpha, beta=beta, viscosity=viscosity, fluid_tag=FLUID_TAG,
-                               wall_tag=WALL_TAG, kahan=kahan)
+    return abi.make_physics(dt, rho0=RHO0, c0=c0, p0=0.0, gamma=GAMMA, gravity=grav,
+                            alpha=alpha, beta=beta, viscosity=viscosity, fluid_tag=FLUID_TAG,
+                            wall_tag=WALL_TAG, kahan=kahan)
+
+
+def _assemble(dim, domain, parts, h_factor, height, c0, max_nb, kahan, viscosity, alpha, beta, meta):
+    st = _state(dim, parts, h_factor, height, c0)
+    n = st["Tag"].shape[0]
+    ints, floats = _layout(dim, max_nb)
+    params = OrderedDict([("rho0", RHO0), ("p0", 0.0), ("FLUID_TAG", FLUID_TAG),
+                          ("WALL_TAG", WALL_TAG), ("gap0", meta["dx"]),
+                          ("h0", h_factor * meta["dx"])])
+    ps = ParticleSystem(domain, n, ints, floats, params)
+    for k, v in st.items():
+        ps[k] = v
+    c0f, dt = _time_step(h_factor, meta["dx"], c0)
+    physics = _physics(dim, dt, c0f, kahan, viscosity, alpha, beta)
+    fl = st["Tag"] == FLUID_TAG
     meta = dict(meta)
-    meta.update({"n": n, "n_fluid": int(fl.sum()), "n_wall": int((~fl).sum()), "c0": float(c0f),
-                 "dt": dt, "h": float(h0), "dim": dim, "height": height,
+    meta.update({"n": n, "n_fluid": int(fl.sum()), "n_wall": int((~fl).sum()), "c0": c0f,
+                 "dt": dt, "h": float(np.float32(h_factor * meta["dx"])), "dim": dim, "height": height,
                  "n_cells": domain.get_n()})
     return DamBreakCase(ps, domain, physics, meta)
+
+
+class BatchCase(DamBreakCase):
+    """Independent instances in one particle system (an Instance column), with per-instance
+    time step and speed of sound (`inst_dt`, `inst_c0`) and each instance's particle rows."""
+
+    def __init__(self, ps, domain, physics, meta, inst_dt, inst_c0, rows):
+        super().__init__(ps, domain, physics, meta)
+        self.inst_dt = inst_dt
+        self.inst_c0 = inst_c0
+        self.rows = rows   # rows[k] = (first, last + 1) of instance k in the particle matrices
+
+    @property
+    def n_instances(self):
+        return len(self.rows)
+
+
+def batch_columns(n_instances, seed=0, width=(0.5, 1.5), height=(1.0, 2.5)):
+    """The seeded column sizes of a batch: width ~ U[width], height ~ U[height] per instance."""
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(width[0], width[1], n_instances)
+    h = rng.uniform(height[0], height[1], n_instances)
+    return [(float(a), float(b)) for a, b in zip(w, h)]
+
+
+def dam_break_batch(n_instances=256, seed=0, dx=0.01, tank=(4.0, 3.0), width=(0.5, 1.5),
+                    height=(1.0, 2.5), wall_layers=3, h_factor=1.5, max_neighbour_number=1, kahan=1,
+                    viscosity=abi.EPP_VISCOSITY_REFERENCE, alpha=0.1, beta=0.1, columns=None):
+    """Uneven 2D dam breaks in one batch: instance k is dam_break_2d(dx, tank, columns[k]) --
+    the same particles, state and physics as that case built alone -- with c0_k = 10 sqrt(2 g H_k)
+    and dt_k = 0.1 h / c0_k of its own column height."""
+    columns = columns or batch_columns(n_instances, seed, width, height)
+    domain = _tank_domain_2d(dx, tank, wall_layers, h_factor)
+    states, inst_dt, inst_c0, rows, n_fluid = [], [], [], [], []
+    first = 0
+    for (w, hgt) in columns:
+        c0 = 10.0 * math.sqrt(2.0 * GRAVITY * hgt)
+        st = _state(2, _dam_parts_2d(dx, tank, (w, hgt), wall_layers), h_factor, hgt, c0)
+        c0f, dt = _time_step(h_factor, dx, c0)
+        states.append(st)
+        inst_dt.append(dt)
+        inst_c0.append(c0f)
+        n = st["Tag"].shape[0]
+        rows.append((first, first + n))
+        n_fluid.append(int((st["Tag"] == FLUID_TAG).sum()))
+        first += n
+    ints, floats = _layout(2, max_neighbour_number, instance=True)
+    params = OrderedDict([("rho0", RHO0), ("p0", 0.0), ("FLUID_TAG", FLUID_TAG),
+                          ("WALL_TAG", WALL_TAG), ("gap0", dx), ("h0", h_factor * dx)])
+    ps = ParticleSystem(domain, first, ints, floats, params)
+    for k in states[0]:
+        ps[k] = np.concatenate([st[k] for st in states])
+    ps["Instance"] = np.concatenate([np.full(r[1] - r[0], k, np.int32) for k, r in enumerate(rows)])
+    physics = _physics(2, inst_dt[0], inst_c0[0], kahan, viscosity, alpha, beta)
+    meta = {"dim": 2, "dx": dx, "tank": tank, "n": first, "n_fluid": int(sum(n_fluid)),
+            "n_wall": first - int(sum(n_fluid)), "columns": columns, "seed": seed,
+            "inst_n_fluid": n_fluid, "h": float(np.float32(h_factor * dx)),
+            "n_cells": domain.get_n() * len(columns)}
+    return BatchCase(ps, domain, physics, meta, np.array(inst_dt, np.float32), np.array(inst_c0, np.float32),
+                     rows)
 
 
 # active pairs of casegen.jl:137: fluid-fluid, fluid-wall, wall-fluid

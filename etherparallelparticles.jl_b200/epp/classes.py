@@ -285,7 +285,7 @@ class ParticleSystem:
             "position": "PositionVec", "velocity": "VelocityVec", "dvelocity": "dVelocityVec",
             "mass": "Mass", "volume": "Volume", "density": "Density", "ddensity": "dDensity",
             "pressure": "Pressure", "gap": "Gap", "h": "H", "n_rvec": "nRVec", "n_r": "nR",
-            "n_w": "nW", "n_dw": "nDW", "n_hinv": "nHInv",
+            "n_w": "nW", "n_dw": "nDW", "n_hinv": "nHInv", "instance": "Instance",
         }
         m = abi.epp_column_map.empty()
         for field, ref in lookup.items():
