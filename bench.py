@@ -50,8 +50,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="epp", choices=["epp", "reference"])
-    ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small", "3d-small", "batch"])
+    ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small", "3d-small", "batch", "serve"])
     ap.add_argument("--instances", type=int, default=256, help="batch: number of instances")
+    ap.add_argument("--requests", type=int, default=32, help="serve: number of requests in the stream")
+    ap.add_argument("--sim-steps", type=int, default=2000, help="serve: steps per request")
+    ap.add_argument("--mix", default="stream", choices=["stream", "batch"],
+                    help="serve: the Poisson request stream, or the batched form's 256-instance mix as a burst")
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per particle (0 = tuned default)")
     return ap.parse_args()
@@ -167,6 +171,8 @@ def run_reference(args):
         return
     if args.case == "batch":
         return run_reference_batch(args)
+    if args.case == "serve":
+        return run_reference_serve(args)
     case, label = make_case(args.case)
     case.meta["label"] = label
     probe = cpu_reference(case, steps_budget_s=0.0, max_steps=1)      # cost of one step
@@ -209,6 +215,31 @@ def run_reference_batch(args):
            "data": "synthetic (seeded column sizes, numpy default_rng(0))",
            "config": {"workload": "%d uneven 2D dam breaks, dx=0.01 m" % len(cols), "instances": len(cols)},
            "cpu_baseline": {"value": val, "unit": "sims/s", "cores": cores, "kind": "port", "sample": sample_txt},
+           "e2e": {"value": val, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_reference_serve(args):
+    """--impl reference --case serve: the oracle serves requests one at a time (the reference has
+    no serving form); sims/s from a sample of the stream's requests timed for a few steps each."""
+    from epp import serve
+    specs = serve.request_stream(args.requests, seed=0, steps=args.sim_steps)
+    sample = specs[:: max(1, len(specs) // 6)]
+    total, cores = 0.0, 1
+    for s in sample:
+        case = s.case()
+        case.meta["label"] = "request %d" % s.rid
+        res = cpu_reference(case, steps_budget_s=2.0, max_steps=5)
+        total += res["seconds_per_step"] * s.steps
+        cores = res["cores"]
+    val = len(sample) / total
+    out = {"metric": "served sims/s (Poisson request stream, %d steps per simulation)" % args.sim_steps,
+           "value": val, "unit": "sims/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.sim_steps,
+           "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic request stream (numpy default_rng(0))",
+           "config": {"workload": "%d requests" % args.requests},
+           "cpu_baseline": {"value": val, "unit": "sims/s", "cores": cores, "kind": "port",
+                            "sample": "requests %s, up to 5 steps each, one at a time" % [s.rid for s in sample]},
            "e2e": {"value": val, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -395,12 +426,81 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+def run_serve(args):
+    """--case serve: the seeded request stream (Poisson arrivals, mean 50 / s; 70% 2D, 30% 3D; fluid
+    counts log-uniform in 1e3 - 1e6; 2000 steps each) served under a 120 GB HBM budget with
+    continuous batching, against the same trace served one request at a time on the plain path.
+    value = completed simulations / makespan (arrival of the first request to completion of the
+    last), latency = completion - arrival, both on the host clock; every request is uploaded,
+    searched, stepped and read back (FP64 integrals) inside the measured time."""
+    # more hardware queues than the default 8, so up to 32 resident runs get their own (set
+    # before the first CUDA call of the process)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+    import torch
+    from epp import serve
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if args.mix == "batch":
+        specs = serve.batch_mix_requests(args.instances, steps=args.sim_steps)
+    else:
+        specs = serve.request_stream(args.requests, seed=0, steps=args.sim_steps)
+    be = serve.DeviceBackend(device=local)
+    # warm-up: one small request of each dimension (module load, first graph build)
+    warm = [s for s in serve.request_stream(16, seed=99, n_range=(1e3, 3e3), steps=10)]
+    warm = [next(s for s in warm if s.dim == 2), next(s for s in warm if s.dim == 3)]
+    for s in warm:
+        s.arrival = 0.0
+    serve.Server(be).run(serve.make_runs(warm, be))
+    runs = serve.make_runs(specs, be)
+    clocks = Clocks(local)
+    clocks.start()
+    st = serve.Server(be, budget_bytes=120 * 10**9).run(runs)
+    clk = clocks.stop()
+    plain_runs = serve.make_runs(specs, be)
+    plain = serve.Server(be, budget_bytes=120 * 10**9, max_active=1).run(plain_runs)
+    n_p = [r.case.n for r in runs]
+    h2d = sum(n * 4 * 18 for n in n_p)
+    if rank == 0:
+        if args.mix == "batch":
+            workload = ("the batched form's %d-instance 2D mix as requests arriving at once (width U[0.5,1.5] m, "
+                        "height U[1.0,2.5] m, dx=0.01 m)" % len(specs))
+        else:
+            workload = ("%d requests, Poisson mean 50/s, 70%% 2D / 30%% 3D, fluid log-uniform 1e3-1e6, "
+                        "aspect U[0.5,2.5]" % len(specs))
+        out = {"metric": "served sims/s (%s, %d steps per simulation)"
+                         % ("256-instance mix" if args.mix == "batch" else "Poisson request stream", args.sim_steps),
+               "value": st["sims_per_s"], "unit": "sims/s", "n_gpus": 1, "steps": args.sim_steps,
+               "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic request stream (numpy default_rng(0)): arrivals, sizes and aspects seeded",
+               "config": {"workload": workload, "requests": len(specs), "stream_priorities": "by size",
+                          "requests_2d": sum(1 for s in specs if s.dim == 2),
+                          "requests_3d": sum(1 for s in specs if s.dim == 3),
+                          "particles_total": int(sum(n_p)), "particles_range": [min(n_p), max(n_p)],
+                          "hbm_budget_bytes": 120 * 10**9, "chunk_steps": 100, "parallelism": "single GPU"},
+               "latency_p50_s": st["latency_p50_s"], "latency_p99_s": st["latency_p99_s"],
+               "served": st,
+               "plain_path": dict(plain, method="same trace, one request at a time (max_active = 1), same kernels"),
+               "speedup_vs_plain": st["sims_per_s"] / plain["sims_per_s"],
+               "p99_vs_plain": st["latency_p99_s"] / plain["latency_p99_s"],
+               "gpu_launches": 6 * args.sim_steps * len(specs),
+               "clocks": clk,
+               "e2e": {"value": st["sims_per_s"], "unit": "sims/s", "h2d_bytes_per_step": int(h2d / args.sim_steps / len(specs)),
+                       "d2h_bytes_per_step": 0,
+                       "note": "serving is end to end: each request's upload, search, steps and integrals read-back "
+                               "are inside the makespan"}}
+        print(json.dumps(out))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.case == "batch":
         return run_batch(args)
+    if args.case == "serve":
+        return run_serve(args)
     import torch
     import torch.distributed as dist
     from epp import abi, casegen

@@ -170,6 +170,55 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     return b + (1 << 20);
 }
 
+// Device memory of a context comes from the stream-ordered allocator on the context's stream:
+// creating or destroying one context never synchronises the device, so a server can admit and
+// retire simulations while others keep running.
+template <class T>
+cudaError_t dev_alloc(epp_ctx* ctx, T** p, size_t bytes) {
+    return cudaMallocAsync(reinterpret_cast<void**>(p), bytes, ctx->stream);
+}
+template <class T>
+void dev_free(epp_ctx* ctx, T*& p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
+    p = nullptr;
+}
+
+// Cells of the grid (all instances) and scan tiles of a configuration; false if it is invalid.
+bool plan_cells(const epp_config* cfg, DevDomain& d, long long& ncell) {
+    const int D = cfg->domain.dim;
+    d.dim = D;
+    const float gap = cfg->domain.gap;
+    d.gap_square = gap * gap;
+    ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        d.n[a] = 1;
+        d.first[a] = d.last[a] = 0.0f;
+        d.gap_inv[a] = 1.0f;
+    }
+    for (int a = 0; a < D; ++a) {
+        d.first[a] = cfg->domain.first[a];
+        d.last[a] = cfg->domain.last[a];
+        const float span = d.last[a] - d.first[a];
+        volatile float q = span / gap;
+        const int na = (int)floorf(q);
+        if (na < 1) return false;
+        d.n[a] = na;
+        volatile float ga = span / (float)na;
+        d.gap_inv[a] = 1.0f / ga;
+        ncell *= na;
+    }
+    const int n_inst = cfg->n_instances > 1 ? cfg->n_instances : 1;
+    if ((D == 3 && n_inst > 1) || ncell * n_inst > (1ll << 30) || n_inst > (1 << 22)) return false;
+    d.cells_per_inst = (int)ncell;
+    d.n_inst = n_inst;
+    d.n_cells = (int)(ncell * n_inst);
+    return true;
+}
+
+size_t nlist_bytes(int D, int cap) {
+    return sizeof(int) * (size_t)(D == 2 ? ListConf<2>::LCAP : ListConf<3>::LCAP) * cap;
+}
+
 template <int D>
 int run_search(epp_ctx* ctx, int crit, int action, const epp_physics* phys, bool emit);
 
@@ -357,9 +406,9 @@ int ensure_lists(epp_ctx* ctx) {
     if (ctx->list_mem) return EPP_OK;
     const size_t cap = ctx->cap, nb = ctx->cfg.max_neighbour_number, D = ctx->D;
     const size_t words = cap * nb * (1 + D + 4);
-    CK(cudaMalloc(&ctx->list_mem, words * 4));
+    CK(dev_alloc(ctx, &ctx->list_mem, words * 4));
     CK(cudaMemsetAsync(ctx->list_mem, 0, words * 4, ctx->stream));
-    CK(cudaMalloc(&ctx->list_stage, words * 4));
+    CK(dev_alloc(ctx, &ctx->list_stage, words * 4));
     char* p = (char*)ctx->list_mem;
     ctx->L.idx = (int*)p; p += cap * nb * 4;
     ctx->L.rvec = (float*)p; p += cap * nb * D * 4;
@@ -661,39 +710,13 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->cap = cfg->n_capacity;
     // domain in FP32 exactly as Domain2D (Domain2D.jl:34-66)
     DevDomain& d = ctx->dom;
-    d.dim = D;
-    const float gap = cfg->domain.gap;
-    d.gap_square = gap * gap;
     long long ncell = 1;
-    for (int a = 0; a < 3; ++a) {
-        d.n[a] = 1;
-        d.first[a] = d.last[a] = 0.0f;
-        d.gap_inv[a] = 1.0f;
-    }
-    for (int a = 0; a < D; ++a) {
-        d.first[a] = cfg->domain.first[a];
-        d.last[a] = cfg->domain.last[a];
-        const float span = d.last[a] - d.first[a];
-        volatile float q = span / gap;
-        const int na = (int)floorf(q);
-        if (na < 1) {
-            delete ctx;
-            return EPP_ERR_INVALID_ARGUMENT;
-        }
-        d.n[a] = na;
-        volatile float ga = span / (float)na;
-        d.gap_inv[a] = 1.0f / ga;
-        ncell *= na;
-    }
-    const int n_inst = cfg->n_instances > 1 ? cfg->n_instances : 1;
-    if ((D == 3 && n_inst > 1) || ncell * n_inst > (1ll << 30) || n_inst > (1 << 22)) {
+    if (!plan_cells(cfg, d, ncell)) {
         delete ctx;
         return EPP_ERR_INVALID_ARGUMENT;
     }
+    const int n_inst = d.n_inst;
     ctx->n_inst = n_inst;
-    d.cells_per_inst = (int)ncell;
-    d.n_inst = n_inst;
-    d.n_cells = (int)(ncell * n_inst);
     ctx->n_cells = d.n_cells;
     ctx->n_tiles = (ctx->n_cells + 1 + kScanTile - 1) / kScanTile;
     for (int a = 0; a < cfg->n_tags; ++a) {
@@ -711,14 +734,17 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
         delete ctx;
         return EPP_ERR_CUDA;
     }
-    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&ctx->arena.base, need) != cudaSuccess) {
-        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         cudaGetLastError();
-        return EPP_ERR_OUT_OF_MEMORY;
+        return EPP_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
+    if (dev_alloc(ctx, &ctx->arena.base, need) != cudaSuccess) {
+        cudaGetLastError();
+        epp_destroy(ctx);
+        return EPP_ERR_OUT_OF_MEMORY;
+    }
     ctx->arena.size = need;
     Arena& a = ctx->arena;
     fill_state(a, ctx->S[0], ctx->cap);
@@ -754,20 +780,20 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
         epp_destroy(ctx);
         return EPP_ERR_OUT_OF_MEMORY;
     }
-    const size_t lcap = D == 2 ? ListConf<2>::LCAP : ListConf<3>::LCAP;
-    if (cfg->hbm_budget_bytes > 0 && (long long)(need + sizeof(int) * lcap * ctx->cap) > cfg->hbm_budget_bytes) {
+    if (cfg->hbm_budget_bytes > 0 && (long long)(need + nlist_bytes(D, ctx->cap)) > cfg->hbm_budget_bytes) {
         epp_destroy(ctx);
         return EPP_ERR_BUDGET;
     }
-    if (cudaMalloc(&ctx->nlist, sizeof(int) * lcap * ctx->cap) != cudaSuccess ||
-        cudaMalloc(&ctx->inst_table, sizeof(InstPhys) * n_inst) != cudaSuccess ||
-        cudaMalloc(&ctx->inst_out, sizeof(double) * 9 * n_inst) != cudaSuccess) {
+    if (dev_alloc(ctx, &ctx->nlist, nlist_bytes(D, ctx->cap)) != cudaSuccess ||
+        dev_alloc(ctx, &ctx->inst_table, sizeof(InstPhys) * n_inst) != cudaSuccess ||
+        dev_alloc(ctx, &ctx->inst_out, sizeof(double) * 9 * n_inst) != cudaSuccess) {
+        cudaGetLastError();
         epp_destroy(ctx);
         return EPP_ERR_OUT_OF_MEMORY;
     }
     // zeroed lists: a list slot read before any search wrote it holds index 0, in bounds
     if (cudaMemsetAsync(ctx->arena.base, 0, need, ctx->stream) != cudaSuccess ||
-        cudaMemsetAsync(ctx->nlist, 0, sizeof(int) * lcap * ctx->cap, ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(ctx->nlist, 0, nlist_bytes(D, ctx->cap), ctx->stream) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         epp_destroy(ctx);
@@ -786,15 +812,16 @@ int32_t epp_destroy(epp_ctx* ctx) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->stream = ctx->own_stream;   // the frees below are ordered on the context's own stream
     for (int c = 0; c < 2; ++c)
         if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
-    if (ctx->accel) cudaFree(ctx->accel);
-    if (ctx->inst_table) cudaFree(ctx->inst_table);
-    if (ctx->nlist) cudaFree(ctx->nlist);
-    if (ctx->inst_out) cudaFree(ctx->inst_out);
-    if (ctx->list_mem) cudaFree(ctx->list_mem);
-    if (ctx->list_stage) cudaFree(ctx->list_stage);
-    if (ctx->arena.base) cudaFree(ctx->arena.base);
+    dev_free(ctx, ctx->accel);
+    dev_free(ctx, ctx->inst_table);
+    dev_free(ctx, ctx->nlist);
+    dev_free(ctx, ctx->inst_out);
+    dev_free(ctx, ctx->list_mem);
+    dev_free(ctx, ctx->list_stage);
+    dev_free(ctx, ctx->arena.base);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -1214,6 +1241,49 @@ extern "C" int32_t epp_checked_slot(int32_t* out4) {
 }
 #endif
 
+int32_t epp_context_bytes(const epp_config* cfg, int64_t* bytes) {
+    if (!cfg || !bytes) return EPP_ERR_INVALID_ARGUMENT;
+    const int D = cfg->domain.dim;
+    if ((D != 2 && D != 3) || cfg->n_capacity < 1 || !(cfg->domain.gap > 0.0f)) return EPP_ERR_INVALID_ARGUMENT;
+    DevDomain d;
+    long long ncell = 1;
+    if (!plan_cells(cfg, d, ncell)) return EPP_ERR_INVALID_ARGUMENT;
+    const int n_tiles = (d.n_cells + 1 + kScanTile - 1) / kScanTile;
+    const size_t b = arena_bytes(cfg->n_capacity, d.n_cells, D, n_tiles) + nlist_bytes(D, cfg->n_capacity) +
+                     (sizeof(InstPhys) + sizeof(double) * 9) * (size_t)d.n_inst + 3 * 256;
+    *bytes = (int64_t)b;
+    return EPP_OK;
+}
+
+int32_t epp_query(epp_ctx* ctx, int32_t* done) {
+    if (!ctx || !done) return EPP_ERR_INVALID_ARGUMENT;
+    const cudaError_t e = cudaStreamQuery(ctx->stream);
+    if (e == cudaErrorNotReady) {
+        *done = 0;
+        return EPP_OK;
+    }
+    *done = 1;
+    if (e != cudaSuccess) return fail(ctx, EPP_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+    return EPP_OK;
+}
+
+int32_t epp_set_priority(epp_ctx* ctx, int32_t priority, int32_t* applied) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    int lo = 0, hi = 0;   // numerically: hi (greatest priority) <= lo
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    const int p = priority < hi ? hi : priority > lo ? lo : priority;
+    cudaStream_t s = nullptr;
+    CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, p));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const bool was_own = ctx->stream == ctx->own_stream;
+    cudaStreamDestroy(ctx->own_stream);
+    ctx->own_stream = s;
+    if (was_own) ctx->stream = s;
+    if (applied) *applied = p;
+    return EPP_OK;
+}
+
 int32_t epp_set_stream(epp_ctx* ctx, void* stream) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
@@ -1264,12 +1334,10 @@ int32_t epp_set_accel_output(epp_ctx* ctx, int32_t enable) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
     if (enable && !ctx->accel) {
-        CK(cudaMalloc(&ctx->accel, sizeof(float4) * ctx->cap));
+        CK(dev_alloc(ctx, &ctx->accel, sizeof(float4) * ctx->cap));
         CK(cudaMemsetAsync(ctx->accel, 0, sizeof(float4) * ctx->cap, ctx->stream));
     } else if (!enable && ctx->accel) {
-        CK(cudaStreamSynchronize(ctx->stream));
-        cudaFree(ctx->accel);
-        ctx->accel = nullptr;
+        dev_free(ctx, ctx->accel);
     }
     return EPP_OK;
 }

@@ -18,8 +18,19 @@ EXPORTS = [
     "epp_get_integrals", "epp_cell_stats", "epp_synchronize", "epp_last_step_timing",
     "epp_pairs_total", "epp_set_accel_output", "epp_get_accel", "epp_set_stream",
     "epp_profile_step", "epp_set_tuning", "epp_cell_sort_noalloc", "epp_noalloc_limits",
-    "epp_set_instance_physics", "epp_get_instance_integrals",
+    "epp_set_instance_physics", "epp_get_instance_integrals", "epp_context_bytes", "epp_query",
+    "epp_set_priority",
 ]
+
+
+def context_bytes(config):
+    """Device bytes a context of this configuration allocates (epp_context_bytes)."""
+    lib = load()
+    b = C.c_int64(0)
+    rc = lib.epp_context_bytes(C.byref(config), C.byref(b))
+    if rc != abi.EPP_OK:
+        raise EppError(rc, "epp_context_bytes")
+    return b.value
 
 
 class EppError(RuntimeError):
@@ -71,6 +82,9 @@ def load(path=LIB_PATH):
     lib.epp_noalloc_limits.argtypes = [i32p, i32p, P(C.c_int64)]
     lib.epp_set_instance_physics.argtypes = [ctx, C.c_int32, f32p, f32p]
     lib.epp_get_instance_integrals.argtypes = [ctx, P(abi.epp_physics), P(abi.epp_integrals), C.c_int32]
+    lib.epp_context_bytes.argtypes = [P(abi.epp_config), P(C.c_int64)]
+    lib.epp_query.argtypes = [ctx, i32p]
+    lib.epp_set_priority.argtypes = [ctx, C.c_int32, i32p]
     for name in EXPORTS:
         if name not in ("epp_last_error", "epp_abi_version"):
             getattr(lib, name).restype = C.c_int32
@@ -191,6 +205,18 @@ class Context:
         out = (abi.epp_integrals * n)()
         self._ck(self.lib.epp_get_instance_integrals(self.h, C.byref(phys), out, n), "epp_get_instance_integrals")
         return [o.as_dict() for o in out]
+
+    def done(self):
+        """True when all work queued on this context has finished (non-blocking)."""
+        d = C.c_int32(0)
+        self._ck(self.lib.epp_query(self.h, C.byref(d)), "epp_query")
+        return bool(d.value)
+
+    def set_priority(self, priority):
+        """CUDA stream priority of the context's own stream (lower = first); returns the value used."""
+        a = C.c_int32(0)
+        self._ck(self.lib.epp_set_priority(self.h, priority, C.byref(a)), "epp_set_priority")
+        return a.value
 
     def set_tuning(self, lanes_per_particle):
         self._ck(self.lib.epp_set_tuning(self.h, lanes_per_particle), "epp_set_tuning")

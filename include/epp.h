@@ -215,6 +215,20 @@ int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
  * context's own stream).  Lets a host application order it with its own work and events. */
 int32_t epp_set_stream(epp_ctx* ctx, void* stream);
 
+/* Serving support (no reference counterpart: the reference runs one simulation per process).
+ * epp_context_bytes: device bytes epp_create would allocate for this configuration, without
+ * allocating (the optional neighbour-list emission and dv/dt output are extra); a server admits
+ * simulations against an HBM budget with it.  Context memory comes from the stream-ordered
+ * allocator, so creating or destroying a context does not synchronise the device.
+ * epp_query: *done = 1 when every call queued on the context has finished on the device, 0 while
+ * work is pending; never blocks. */
+int32_t epp_context_bytes(const epp_config* cfg, int64_t* bytes);
+int32_t epp_query(epp_ctx* ctx, int32_t* done);
+/* Recreate the context's own stream with a CUDA stream priority (lower value = scheduled first;
+ * clamped to the device's range, the value used returned in *applied).  A server gives short
+ * runs the higher priorities so they finish first while long runs fill the remaining SMs. */
+int32_t epp_set_priority(epp_ctx* ctx, int32_t priority, int32_t* applied);
+
 /* One dam-break step launched kernel by kernel (no graph) with CUDA events between the
  * kernels; stage_ms[0 .. EPP_PROFILE_STAGES-1] = momentum+integrate+bin, scan, scatter,
  * rank+gather, search (neighbour lists), continuity (0 for pair-pass families that fuse the

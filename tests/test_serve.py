@@ -1,0 +1,167 @@
+"""Serving loop: request stream, HBM-budget admission, continuous batching, alone-vs-mix results.
+
+The host logic (stream, admission, accounting, percentiles) runs on the CPU against a simulated
+backend with a virtual clock; the GPU tests run real requests and compare each result with the
+same request run alone.
+"""
+import numpy as np
+import pytest
+
+from epp import serve
+
+
+# ---------------------------------------------------------------------------- host logic (CPU)
+
+class TickClock:
+    """Virtual clock that advances a fixed tick on every read."""
+
+    def __init__(self, tick=1e-4):
+        self.t = 0.0
+        self.tick = tick
+
+    def __call__(self):
+        self.t += self.tick
+        return self.t
+
+
+class FakeCase:
+    def __init__(self, n):
+        self.n = n
+
+
+class FakeHandle:
+    def __init__(self, case):
+        self.case = case
+        self.busy_until = 0.0
+
+
+class FakeBackend:
+    """A device that runs each resident simulation at `cost` seconds per particle-step, every
+    resident run concurrently (streams), and records the admission order."""
+
+    def __init__(self, clock, cost=1e-9):
+        self.clock = clock
+        self.cost = cost
+        self.admitted = []
+
+    def bytes_needed(self, case):
+        return case.n * 1000
+
+    def admit(self, case):
+        self.admitted.append(case)
+        h = FakeHandle(case)
+        h.busy_until = self.clock.t
+        return h
+
+    def enqueue(self, h, n):
+        h.busy_until = max(h.busy_until, self.clock.t) + n * h.case.n * self.cost
+
+    def idle(self, h):
+        return self.clock.t >= h.busy_until
+
+    def finish(self, h):
+        return {"n": h.case.n}
+
+
+def fake_runs(sizes, arrivals, steps=100):
+    runs = []
+    for i, (n, t) in enumerate(zip(sizes, arrivals)):
+        spec = serve.RequestSpec(i, t, 2, n, 1.0, steps)
+        runs.append(serve.Run(spec, FakeCase(n), n * 1000))
+    return runs
+
+
+def test_request_stream_is_seeded_and_shaped():
+    a = serve.request_stream(2000, seed=3)
+    b = serve.request_stream(2000, seed=3)
+    assert [(r.arrival, r.dim, r.n_fluid, r.aspect) for r in a] == [(r.arrival, r.dim, r.n_fluid, r.aspect) for r in b]
+    arr = np.array([r.arrival for r in a])
+    assert np.all(np.diff(arr) > 0)
+    assert abs(np.mean(np.diff(arr)) - 1.0 / 50.0) < 0.1 / 50.0          # Poisson, mean 50 / s
+    frac2 = np.mean([r.dim == 2 for r in a])
+    assert 0.66 < frac2 < 0.74                                            # 70% 2D
+    n = np.array([r.n_fluid for r in a])
+    assert n.min() >= 1000 and n.max() <= 1000000
+    assert abs(np.median(np.log10(n)) - 4.5) < 0.15                       # log-uniform 1e3 - 1e6
+    asp = np.array([r.aspect for r in a])
+    assert asp.min() >= 0.5 and asp.max() <= 2.5
+
+
+def test_fifo_admission_within_budget():
+    clock = TickClock()
+    be = FakeBackend(clock)
+    sizes = [5000, 40000, 2000, 30000, 8000, 60000, 1000, 20000]
+    runs = fake_runs(sizes, [0.001 * i for i in range(len(sizes))])
+    budget = 70000 * 1000
+    st = serve.Server(be, budget_bytes=budget, clock=clock, idle_wait=0.0).run(runs)
+    assert st["completed"] == len(sizes) and st["rejected"] == 0
+    assert st["peak_resident_bytes"] <= budget
+    assert [c.n for c in be.admitted] == sizes                            # FIFO order
+    adm = [r.admitted for r in runs]
+    assert adm == sorted(adm)
+    assert st["max_concurrent"] >= 2                                      # runs overlap
+
+
+def test_oversize_request_rejected_others_served():
+    clock = TickClock()
+    be = FakeBackend(clock)
+    runs = fake_runs([1000, 10**6, 2000], [0.0, 0.001, 0.002])
+    st = serve.Server(be, budget_bytes=5 * 10**6, clock=clock, idle_wait=0.0).run(runs)
+    assert st["completed"] == 2 and st["rejected"] == 1
+    assert runs[1].error and runs[1].result is None
+    assert runs[0].result == {"n": 1000} and runs[2].result == {"n": 2000}
+
+
+def test_one_at_a_time_is_sequential_and_slower():
+    sizes = [20000, 5000, 50000, 10000, 30000]
+    arr = [0.0, 0.0005, 0.001, 0.0015, 0.002]
+    c1 = TickClock()
+    seq = fake_runs(sizes, arr)
+    st1 = serve.Server(FakeBackend(c1), max_active=1, clock=c1, idle_wait=0.0).run(seq)
+    for a, b in zip(seq, seq[1:]):
+        assert b.admitted >= a.done                                       # no overlap
+    c2 = TickClock()
+    mix = fake_runs(sizes, arr)
+    st2 = serve.Server(FakeBackend(c2), clock=c2, idle_wait=0.0).run(mix)
+    assert st2["makespan_s"] < st1["makespan_s"]
+    assert st2["latency_p99_s"] < st1["latency_p99_s"]
+    lat = sorted(r.latency for r in mix)
+    assert abs(st2["latency_p50_s"] - float(np.percentile(lat, 50))) < 1e-12
+
+
+# ---------------------------------------------------------------------------- device (GPU)
+
+def _small_stream(n=6, steps=200, seed=1):
+    return serve.request_stream(n, seed=seed, rate=500.0, n_range=(1e3, 2e4), steps=steps)
+
+
+@pytest.mark.gpu
+def test_served_results_equal_alone():
+    specs = _small_stream()
+    be = serve.DeviceBackend(download=True)
+    runs = serve.make_runs(specs, be)
+    st = serve.Server(be, chunk=50).run(runs)
+    assert st["completed"] == len(specs)
+    assert st["max_concurrent"] >= 2
+    for r in runs:
+        alone = serve.DeviceBackend(download=True)
+        case = r.spec.case()
+        h = alone.admit(case)
+        alone.enqueue(h, r.spec.steps)
+        res = alone.finish(h)
+        assert r.result["status"] == res["status"]
+        for k, v in res["state"].items():
+            assert np.array_equal(r.result["state"][k], v), (r.spec.rid, k)
+        for k in ("mass_total", "kinetic", "potential", "internal", "n_pairs"):
+            assert r.result["integrals"][k] == res["integrals"][k], (r.spec.rid, k)
+
+
+@pytest.mark.gpu
+def test_budget_limits_resident_runs():
+    specs = _small_stream(n=5, steps=100, seed=2)
+    be = serve.DeviceBackend()
+    runs = serve.make_runs(specs, be)
+    budget = max(r.bytes for r in runs) + min(r.bytes for r in runs) // 2
+    st = serve.Server(be, budget_bytes=budget, chunk=50).run(runs)
+    assert st["completed"] == len(specs) and st["rejected"] == 0
+    assert st["peak_resident_bytes"] <= budget
