@@ -18,7 +18,7 @@ from oracle_lib import (ORC_FIELD_ACCEL, ORC_FIELD_ACCEL_ABS, ORC_FIELD_DDENSITY
 pytestmark = pytest.mark.gpu
 
 REL = 1e-5
-FAMILIES = [0, 1, 4]   # pair-pass kernels: mask passes (default), cell-centric queue, 4 lanes/particle
+FAMILIES = [0, 1, 4]   # pair-pass kernels: warp-tile search + list passes (default), cell-centric queue, 4 lanes/particle
 
 
 def rel_err(a, b, floor):
