@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--instances", type=int, default=256, help="batch: number of instances")
     ap.add_argument("--requests", type=int, default=32, help="serve: number of requests in the stream")
     ap.add_argument("--sim-steps", type=int, default=2000, help="serve: steps per request")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="batch / serve: skip the launch-configuration autotuner (serve)")
     ap.add_argument("--mix", default="stream", choices=["stream", "batch"],
                     help="serve: the Poisson request stream, or the batched form's 256-instance mix as a burst")
     ap.add_argument("--no-flush", action="store_true")
@@ -272,9 +274,13 @@ def run_batch(args):
     b = casegen.dam_break_batch(args.instances, seed=0, dx=0.01)
     phys = b.physics
     ns = NeighbourSystem(b.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    from epp import autotune
+    tuned, tune_ms = autotune.tune_case(b, n_instances=b.n_instances, inst=(b.inst_dt, b.inst_c0), steps=5,
+                                        device=local)
     dps = DeviceParticleSystem(b.ps, ns, device=local, n_instances=b.n_instances)
     ctx = dps.ctx
     ctx.set_instance_physics(b.inst_dt, b.inst_c0)
+    ctx.set_block_threads(tuned[1])
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     dps.syncto()
@@ -404,6 +410,8 @@ def run_batch(args):
                                      "timed per instance by CUDA events, summed over the %d instances"
                                      % (K2, len(cases))},
             "speedup_vs_plain": sims_s / world / plain_sims_s,
+            "autotune": {"family": tuned[0], "block_threads": tuned[1], "resort_every": 1,
+                         "ms_per_step": {"%d/%d" % k: round(v, 4) for k, v in tune_ms.items()}},
             "pairs_per_s": pairs / (ms * 1e-3) if world == 1 else None,
             "energy_drift": {"steps": S, "bar": 1e-4, "instances": drift,
                              "max_abs_diff": max(v["abs_diff"] for v in drift.values())},
@@ -445,7 +453,17 @@ def run_serve(args):
         specs = serve.batch_mix_requests(args.instances, steps=args.sim_steps)
     else:
         specs = serve.request_stream(args.requests, seed=0, steps=args.sim_steps)
-    be = serve.DeviceBackend(device=local)
+    from epp import autotune
+    tuner = autotune.Autotuner(device=local, steps=10)
+    be = serve.DeviceBackend(device=local, tuner=tuner if args.autotune else None)
+    # launch configuration per (dimension, size bucket) of the trace, tuned before the clock starts
+    tuned = {}
+    if args.autotune:
+        for s_ in specs:
+            c = s_.case()
+            k = autotune.TuneCache.key(tuner.gpu, c.meta["dim"], c.n, False)
+            if k not in tuned:
+                tuned[k] = tuner.best(c.meta["dim"], c.n, case=c)
     # warm-up: one small request of each dimension (module load, first graph build)
     warm = [s for s in serve.request_stream(16, seed=99, n_range=(1e3, 3e3), steps=10)]
     warm = [next(s for s in warm if s.dim == 2), next(s for s in warm if s.dim == 3)]
@@ -483,6 +501,7 @@ def run_serve(args):
                "served": st,
                "plain_path": dict(plain, method="same trace, one request at a time (max_active = 1), same kernels"),
                "speedup_vs_plain": st["sims_per_s"] / plain["sims_per_s"],
+               "autotune": {k: {"family": v[0], "block_threads": v[1]} for k, v in tuned.items()},
                "p99_vs_plain": st["latency_p99_s"] / plain["latency_p99_s"],
                "gpu_launches": 6 * args.sim_steps * len(specs),
                "clocks": clk,

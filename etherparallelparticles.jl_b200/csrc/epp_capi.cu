@@ -106,6 +106,7 @@ struct epp_ctx {
     int last_crit = EPP_CRITERION_SYMMETRY;
     unsigned adj[kMaxTags]{};
     int lanes = 0;             // pair-pass family: 0 warp tiles + lists, 1 cell-centric, 2..32 lane groups
+    int pass_threads = 128;    // threads per block of the family-0 search and list passes (32, 64, 128)
     int* nlist = nullptr;      // neighbour lists of the last search ([LCAP * cap])
     bool nlist_valid = false;   // the lists match the current order, positions and criterion
     int n_inst = 1;            // batch instances (independent layers of the cell grid)
@@ -281,7 +282,7 @@ template <int D>
 int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
     PairArgs A = pair_args(ctx, set, crit);
     TileMask M{ctx->cap, ctx->nlist};
-    k_build<D><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, ctx->ncount, pairs);
+    k_build<D><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(A, M, ctx->ncount, pairs);
     CK_LAUNCH();
     return EPP_OK;
 }
@@ -291,7 +292,8 @@ template <int D, class Act, bool EPI = false>
 int launch_list(epp_ctx* ctx, int set, int crit, const Act& act) {
     PairArgs A = pair_args(ctx, set, crit);
     TileMask M{ctx->cap, ctx->nlist};
-    k_list<D, Act, EPI><<<blocks_for(ctx->n), 128, 0, ctx->stream>>>(A, M, ctx->ncount, act, ctx->scan_state,
+    k_list<D, Act, EPI><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
+        A, M, ctx->ncount, act, ctx->scan_state,
                                                                      ctx->n_tiles + 1);
     CK_LAUNCH();
     return EPP_OK;
@@ -1227,6 +1229,8 @@ int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle) {
     const int g = lanes_per_particle;
     if (g != 0 && g != 1 && g != 2 && g != 4 && g != 8 && g != 16 && g != 32)
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pair-pass family %d not in {0,1,2,4,8,16,32}", g);
+    if (g != 0 && ctx->n_inst > 1)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "batches of %d instances use pair-pass family 0", ctx->n_inst);
     if (g != ctx->lanes) {
         ctx->lanes = g;
         ctx->nlist_valid = false;
@@ -1240,6 +1244,17 @@ extern "C" int32_t epp_checked_slot(int32_t* out4) {
     return cudaMemcpyFromSymbol(out4, epp_check_slot, sizeof(int) * 4) == cudaSuccess ? EPP_OK : EPP_ERR_CUDA;
 }
 #endif
+
+int32_t epp_set_block_threads(epp_ctx* ctx, int32_t threads) {
+    if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
+    if (threads != 32 && threads != 64 && threads != 128)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "threads per block %d not in {32, 64, 128}", threads);
+    if (threads != ctx->pass_threads) {
+        ctx->pass_threads = threads;
+        drop_graphs(ctx);
+    }
+    return EPP_OK;
+}
 
 int32_t epp_context_bytes(const epp_config* cfg, int64_t* bytes) {
     if (!cfg || !bytes) return EPP_ERR_INVALID_ARGUMENT;

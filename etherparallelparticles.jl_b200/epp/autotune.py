@@ -1,0 +1,154 @@
+"""Autotuner for the time step's launch configuration.
+
+Knobs (all leave the neighbour sets and cell lists bit-exact):
+* the pair-pass family (`epp_set_tuning`): 0 = warp-tile search + list passes, 1 = one warp per
+  occupied cell, 2..32 = lanes per particle (family changes round at the FP32 level only);
+* the threads per block of the family-0 passes (`epp_set_block_threads`): 128, 64 or 32 -- small
+  systems spread over more SMs with smaller blocks (no change in results).
+
+The re-sort cadence is not a knob: the reference re-sorts every step and the cell lists are
+compared bit-exactly per step, so the cadence is 1.
+
+A configuration is tuned on a representative dam break of the same dimension and size bucket
+(particle count rounded to a quarter decade), timed over a few steps, and cached in a JSON file
+keyed by GPU name, dimension, size bucket and batch-ness.  Batches (more than one instance) use
+family 0 and tune the block size only.
+"""
+import json
+import math
+import os
+import time
+
+from . import abi, casegen
+
+FAMILIES = (0, 4, 8, 1)
+THREADS = (128, 64, 32)
+SYM = abi.EPP_CRITERION_SYMMETRY
+CONT = abi.EPP_ACTION_DAMBREAK_CONTINUITY
+
+
+def size_bucket(n):
+    """Particle count rounded to a quarter decade (10^(k/4))."""
+    return int(round(4 * math.log10(max(n, 1))))
+
+
+def candidates(batch=False):
+    fam = (0,) if batch else FAMILIES
+    out = []
+    for f in fam:
+        for t in (THREADS if f == 0 else (128,)):
+            out.append((f, t))
+    return out
+
+
+def default_cache_path():
+    return os.environ.get("EPP_TUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "epp", "tune.json")
+
+
+class TuneCache:
+    """JSON cache {key: {"family": f, "threads": t, "ms": {...}}}."""
+
+    def __init__(self, path=None):
+        self.path = path or default_cache_path()
+        self.data = {}
+        if os.path.exists(self.path):
+            try:
+                with open(self.path) as f:
+                    self.data = json.load(f)
+            except (OSError, ValueError):
+                self.data = {}
+
+    @staticmethod
+    def key(gpu, dim, n, batch):
+        return "%s|%dD|b%d|%s" % (gpu, dim, size_bucket(n), "batch" if batch else "single")
+
+    def get(self, key):
+        return self.data.get(key)
+
+    def put(self, key, entry):
+        self.data[key] = entry
+        d = os.path.dirname(self.path)
+        if d:
+            os.makedirs(d, exist_ok=True)
+        tmp = self.path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(self.data, f, indent=1, sort_keys=True)
+        os.replace(tmp, self.path)
+
+
+def time_config(ctx, phys, family, threads, steps=20, warmup=3):
+    """Host-clock ms per step of `steps` fused steps after `warmup`, with this configuration."""
+    ctx.set_tuning(family)
+    if family == 0:
+        ctx.set_block_threads(threads)
+    ctx.step(warmup, phys)
+    ctx.synchronize(raise_on_status=False)
+    t0 = time.perf_counter()
+    ctx.step(steps, phys)
+    ctx.synchronize(raise_on_status=False)
+    return 1e3 * (time.perf_counter() - t0) / steps
+
+
+def tune_case(case, n_instances=1, inst=None, steps=20, device=0, timer=time_config, batch=None):
+    """Time every candidate on a fresh context holding `case`; returns (best, {cand: ms}).
+    `batch` restricts the candidates to those a batch can use (default: n_instances > 1)."""
+    from .algorithm import DeviceParticleSystem
+    from .classes import NeighbourSystem
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    ms = {}
+    for fam, thr in candidates(n_instances > 1 if batch is None else batch):
+        dps = DeviceParticleSystem(case.ps, ns, device=device, n_instances=n_instances)
+        if inst is not None:
+            dps.ctx.set_instance_physics(*inst)
+        dps.syncto()
+        dps.ctx.search(SYM, CONT, case.physics, 0)
+        ms[(fam, thr)] = timer(dps.ctx, case.physics, fam, thr, steps=steps)
+        dps.close()
+    best = min(ms, key=ms.get)
+    return best, ms
+
+
+def representative_case(dim, n):
+    """A dam break of about n particles (fluid and walls) in the benchmark tanks."""
+    if dim == 2:
+        dx = math.sqrt(1.0 * 2.0 / max(n * 0.9, 1.0))
+        return casegen.dam_break_2d(dx=dx, max_neighbour_number=1)
+    dx = (1.0 * 1.0 * 0.6 / max(n * 0.75, 1.0)) ** (1.0 / 3.0)
+    return casegen.dam_break_3d(dx=dx, max_neighbour_number=1)
+
+
+class Autotuner:
+    """best(dim, n, batch) -> (family, threads), from the cache or tuned once and stored."""
+
+    def __init__(self, cache=None, device=0, gpu=None, steps=20):
+        self.cache = cache if cache is not None else TuneCache()
+        self.device = device
+        self.steps = steps
+        self._gpu = gpu
+
+    @property
+    def gpu(self):
+        if self._gpu is None:
+            try:
+                import torch
+                self._gpu = torch.cuda.get_device_name(self.device).replace(" ", "_")
+            except Exception:
+                self._gpu = "gpu%d" % self.device
+        return self._gpu
+
+    def best(self, dim, n, batch=False, case=None):
+        key = TuneCache.key(self.gpu, dim, n, batch)
+        hit = self.cache.get(key)
+        if hit:
+            return hit["family"], hit["threads"]
+        case = case or representative_case(dim, n)
+        (fam, thr), ms = tune_case(case, steps=self.steps, device=self.device, batch=batch)
+        self.cache.put(key, {"family": fam, "threads": thr, "particles": case.n,
+                             "ms_per_step": {"%d/%d" % k: v for k, v in ms.items()}})
+        return fam, thr
+
+    def apply(self, ctx, dim, n, batch=False):
+        fam, thr = self.best(dim, n, batch)
+        ctx.set_tuning(fam)
+        ctx.set_block_threads(thr)
+        return fam, thr

@@ -19,7 +19,7 @@ EXPORTS = [
     "epp_pairs_total", "epp_set_accel_output", "epp_get_accel", "epp_set_stream",
     "epp_profile_step", "epp_set_tuning", "epp_cell_sort_noalloc", "epp_noalloc_limits",
     "epp_set_instance_physics", "epp_get_instance_integrals", "epp_context_bytes", "epp_query",
-    "epp_set_priority",
+    "epp_set_priority", "epp_set_block_threads",
 ]
 
 
@@ -85,6 +85,7 @@ def load(path=LIB_PATH):
     lib.epp_context_bytes.argtypes = [P(abi.epp_config), P(C.c_int64)]
     lib.epp_query.argtypes = [ctx, i32p]
     lib.epp_set_priority.argtypes = [ctx, C.c_int32, i32p]
+    lib.epp_set_block_threads.argtypes = [ctx, C.c_int32]
     for name in EXPORTS:
         if name not in ("epp_last_error", "epp_abi_version"):
             getattr(lib, name).restype = C.c_int32
@@ -217,6 +218,9 @@ class Context:
         a = C.c_int32(0)
         self._ck(self.lib.epp_set_priority(self.h, priority, C.byref(a)), "epp_set_priority")
         return a.value
+
+    def set_block_threads(self, threads):
+        self._ck(self.lib.epp_set_block_threads(self.h, threads), "epp_set_block_threads")
 
     def set_tuning(self, lanes_per_particle):
         self._ck(self.lib.epp_set_tuning(self.h, lanes_per_particle), "epp_set_tuning")

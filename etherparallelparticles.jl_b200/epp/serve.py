@@ -114,10 +114,11 @@ class Run:
 class DeviceBackend:
     """Runs each request on its own epp context (own stream) on one GPU."""
 
-    def __init__(self, device=0, download=False, priorities=True):
+    def __init__(self, device=0, download=False, priorities=True, tuner=None):
         self.device = device
         self.download = download
         self.priorities = priorities
+        self.tuner = tuner        # autotune.Autotuner: launch configuration per dimension and size
 
     def _config(self, case):
         from .classes import NeighbourSystem
@@ -137,6 +138,8 @@ class DeviceBackend:
         dps.physics = case.physics
         if self.priorities:
             dps.ctx.set_priority(priority_for(case.n))
+        if self.tuner is not None:
+            self.tuner.apply(dps.ctx, case.meta["dim"], case.n)
         dps.syncto()
         dps.ctx.search(SYM, CONT, case.physics, 0)
         return dps

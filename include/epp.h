@@ -210,6 +210,10 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
  * pair queue; 2, 4, 8, 16 or 32 = that many lanes of a warp per particle.  Chosen by the
  * autotuner; results change only at the FP32 rounding level (neighbour sets are identical). */
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
+/* Threads per block of the family-0 search and list passes: 128 (default), 64 or 32.  Smaller
+ * blocks spread a small system over more SMs; results do not change (the per-particle order is
+ * independent of the block size).  Chosen by the autotuner. */
+int32_t epp_set_block_threads(epp_ctx* ctx, int32_t threads);
 
 /* Queue the context's work on a caller-owned cudaStream_t (passed as void*; NULL restores the
  * context's own stream).  Lets a host application order it with its own work and events. */
