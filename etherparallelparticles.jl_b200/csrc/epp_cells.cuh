@@ -74,17 +74,28 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count,
     __syncthreads();
     const int tile = s_tile;
     const int base = tile * kScanTile + threadIdx.x * kScanItems;
+    const bool full = base + kScanItems <= m;   // the thread's 8 cells are all in range (aligned)
     int v[kScanItems];
+    if (full) {   // two 16-byte loads, then zero the counts for the next step
+        const int4 a = reinterpret_cast<const int4*>(count + base)[0];
+        const int4 b = reinterpret_cast<const int4*>(count + base)[1];
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        reinterpret_cast<int4*>(count + base)[0] = make_int4(0, 0, 0, 0);
+        reinterpret_cast<int4*>(count + base)[1] = make_int4(0, 0, 0, 0);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            v[k] = base + k < m ? count[base + k] : 0;
+            if (base + k < m) count[base + k] = 0;
+        }
+    }
     unsigned long long tsum = 0;   // (occupied << 32) | particles
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        int idx = base + k;
-        v[k] = idx < m ? count[idx] : 0;
+        const int idx = base + k;
         tsum += (unsigned long long)v[k] + ((idx < m - 1 && v[k] > 0) ? (1ull << 32) : 0ull);
     }
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k)
-        if (base + k < m) count[base + k] = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long incl = tsum;
 #pragma unroll
@@ -103,51 +114,70 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan(int m, int* count,
             if (lane >= o) wi += t;
         }
         if (lane < kScanThreads / 32) s_warp[lane] = wi - w;   // exclusive warp offsets
-        if (lane == kScanThreads / 32 - 1) {
-            const unsigned long long total = wi;   // block total (lane 7)
+        const unsigned long long total = __shfl_sync(0xffffffffu, wi, kScanThreads / 32 - 1);   // block total
+        unsigned long long prefix = 0;
+        if (tile == 0) {
+            if (lane == 0) atomicExch(&scan_state[1], pack_status(2, total));
+        } else {
+            if (lane == 0) atomicExch(&scan_state[1 + tile], pack_status(1, total));
+            // decoupled look-back, 32 predecessors per round: lane l reads tile p - l; the round
+            // ends at the nearest tile with its inclusive prefix published (flag 2), summing the
+            // aggregates (flag 1) of the tiles in between; waits (bounded) while any of those has
+            // published nothing yet
             volatile unsigned long long* st = scan_state + 1;
-            unsigned long long prefix = 0;
-            if (tile == 0) {
-                atomicExch(&scan_state[1 + tile], pack_status(2, total));
-            } else {
-                atomicExch(&scan_state[1 + tile], pack_status(1, total));
-                int p = tile - 1;
-                long long spins = 0;
-                while (p >= 0) {
-                    const unsigned long long w2 = st[p];
-                    const unsigned flag = (unsigned)(w2 >> 62);
-                    if (flag == 0) {
-                        if (++spins > kSpinLimit) {
-                            atomicOr(status, EPP_STATUS_SPIN_TIMEOUT);
-                            break;
-                        }
-                        __nanosleep(32);
-                        continue;
+            int p = tile - 1;
+            long long spins = 0;
+            for (;;) {
+                const int q = p - lane;
+                const unsigned long long w2 = q >= 0 ? st[q] : (2ull << 62);   // before tile 0: inclusive 0
+                const unsigned flag = (unsigned)(w2 >> 62);
+                const unsigned incl_mask = __ballot_sync(0xffffffffu, flag == 2);
+                const unsigned zero_mask = __ballot_sync(0xffffffffu, flag == 0);
+                const unsigned need = incl_mask ? ((incl_mask & (0u - incl_mask)) << 1) - 1u : 0xffffffffu;
+                if (zero_mask & need) {
+                    if (++spins > kSpinLimit) {
+                        if (lane == 0) atomicOr(status, EPP_STATUS_SPIN_TIMEOUT);
+                        break;
                     }
-                    prefix += unpack_status(w2);
-                    if (flag == 2) break;
-                    --p;
+                    __nanosleep(32);
+                    continue;
                 }
+                unsigned long long x = ((need >> lane) & 1u) ? unpack_status(w2) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                prefix += x;
+                if (incl_mask) break;
+                p -= 32;
+            }
+            if (lane == 0) {
                 __threadfence();
                 atomicExch(&scan_state[1 + tile], pack_status(2, prefix + total));
             }
-            s_prefix = prefix;
         }
+        if (lane == 0) s_prefix = prefix;
     }
     __syncthreads();
     unsigned long long run = s_prefix + s_warp[warp] + incl - tsum;
+    int out[kScanItems];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         const int idx = base + k;
-        const int cnt = (int)(run & 0xffffffffull);
+        out[k] = (int)(run & 0xffffffffull);
         const int oc = (int)(run >> 32);
-        if (idx < m) start[idx] = cnt;
         if (idx < m - 1 && v[k] > 0) occ[oc] = idx;
         run += (unsigned long long)v[k] + ((idx < m - 1 && v[k] > 0) ? (1ull << 32) : 0ull);
         if (idx == m - 1) {
             start[m] = (int)(run & 0xffffffffull);
             meta[0] = (int)(run >> 32);
         }
+    }
+    if (full) {
+        reinterpret_cast<int4*>(start + base)[0] = make_int4(out[0], out[1], out[2], out[3]);
+        reinterpret_cast<int4*>(start + base)[1] = make_int4(out[4], out[5], out[6], out[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k)
+            if (base + k < m) start[base + k] = out[k];
     }
 }
 
