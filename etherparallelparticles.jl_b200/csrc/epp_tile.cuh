@@ -434,7 +434,7 @@ __device__ __noinline__ float4 neighbours_by_stencil(const PairArgs& A, int i, f
 // in flight.  EPI: fused momentum step (integrate + bin for every
 // particle, dead bin included; block 0 clears the scan state).
 template <int D, class Act, bool EPI>
-__global__ void __launch_bounds__(128, D == 2 ? 8 : 4)
+__global__ void __launch_bounds__(128, D == 2 ? 10 : 4)   // 2D: 10 blocks (48 registers) beat 8 and 12
     k_list(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M, const int* ncount,
            const __grid_constant__ Act act, unsigned long long* scan_state, int n_scan_words) {
     if (EPI && blockIdx.x == 0)
@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 4)
                 HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
                 ListReader<D> lr;
                 lr.start(M, i, cnt);
-                if (D == 2) {   // 64 registers: no room for a second neighbour record
+                if (D == 2) {   // 48 registers: no room for a second neighbour record
                     for (int k = 0; k < cnt; ++k) {
                         const int j = lr.next(k);
                         EPP_CHECK(j >= 0 && j < A.n_max, 16, j);
