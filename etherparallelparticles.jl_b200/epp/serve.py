@@ -47,6 +47,16 @@ class RequestSpec:
         self.column = column      # explicit 2D column (width, height) and lattice spacing, or None
         self.dx = dx
 
+    def expected_particles(self):
+        """Fluid particles this request asks for (before the case is built)."""
+        if self.column is not None:
+            return int(round(self.column[0] * self.column[1] / (self.dx * self.dx)))
+        return self.n_fluid
+
+    def weight(self):
+        """Expected device work: particles x steps, 3D about 2.5x 2D per particle-step."""
+        return self.expected_particles() * self.steps * (2.5 if self.dim == 3 else 1.0)
+
     def case(self):
         """The dam break this request asks for.  2D: column 1.0 m wide, height aspect x width
         (at most 2.5 m) in the 4.0 x 3.0 m tank, dx = sqrt(W H / N).  3D: block 1.0 x 1.0 m, height
