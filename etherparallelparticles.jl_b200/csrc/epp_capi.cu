@@ -47,6 +47,10 @@ DevPhys to_dev(const epp_physics& p) {
     for (int a = 0; a < 3; ++a) d.g[a] = p.gravity[a];
     d.alpha = p.alpha;
     d.beta = p.beta;
+    d.mu = p.mu;
+    d.kernel = p.kernel;
+    d.eos = p.eos;
+    d.motion = p.motion;
     d.gamma = p.gamma;
     d.visc = p.viscosity;
     d.fluid = p.fluid_tag;
@@ -102,6 +106,10 @@ struct epp_ctx {
     bool lists_valid = false;
     bool dv_dirty = true;       // dVelocity may be non-zero (fused step assumes zero)
     bool rpn_valid = false;     // density preview matches rho, drho and rpn_phys
+    float* fwv = nullptr;       // kernel-filter sums (SumWeight, SumWeightedDensity) per sorted particle
+    float* fwr = nullptr;
+    bool filter_pending = false;   // interaction!(KERNEL_FILTER) done, selfaction!(KERNEL_FILTER_SELF) not yet
+    long long step_count = 0;      // epp_step steps since upload (the filter runs after every k-th)
     epp_physics rpn_phys{};
     int last_crit = EPP_CRITERION_SYMMETRY;
     unsigned adj[kMaxTags]{};
@@ -118,6 +126,7 @@ struct epp_ctx {
     double* inst_out = nullptr;         // device [n_inst * 9] integrals
     // fused step graphs, one per ping-pong parity
     cudaGraphExec_t graph[2]{};
+    cudaGraphExec_t graph_f[2]{};   // the same step followed by the kernel filter
     epp_physics graph_phys{};
     bool graph_accel = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -167,6 +176,7 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
     b += (size_t)kIntegralBlocks * 8 * 7 + 8 * 8 + 4 * 256;
+    b += 2 * ((size_t)cap * 4 + 256);                    // kernel-filter sums
     b += 2 * 256;                                                                  // instance tables (small)
     return b + (1 << 20);
 }
@@ -277,6 +287,12 @@ PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
 
 int lanes_of(const epp_ctx* ctx) { return ctx->lanes; }
 
+// Physics that needs the generic pair terms (any kernel, classic viscosity); the benchmark physics
+// (Wendland C2, artificial viscosity) runs the specialised ones.
+bool generic_physics(const epp_physics* p) {
+    return p && (p->kernel != EPP_KERNEL_WENDLAND_C2 || p->viscosity == EPP_VISCOSITY_CLASSIC);
+}
+
 // Family 0, the search pass: neighbour lists and nCount of set `set` under `crit`.
 template <int D>
 int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
@@ -376,6 +392,10 @@ int prepare_kernels(epp_ctx* ctx) {
     g |= cellpair_grid<D, CPCountDv<D>, false>(ctx) < 0;
     g |= cellpair_grid<D, CPMom<D, true>, true>(ctx) < 0;
     g |= cellpair_grid<D, CPMom<D, false>, false>(ctx) < 0;
+    g |= cellpair_grid<D, CPCont<D, true, true>, false>(ctx) < 0;
+    g |= cellpair_grid<D, CPCont<D, false, true>, false>(ctx) < 0;
+    g |= cellpair_grid<D, CPMom<D, true, true>, true>(ctx) < 0;
+    g |= cellpair_grid<D, CPMom<D, false, true>, false>(ctx) < 0;
     return g ? EPP_ERR_CUDA : EPP_OK;
 }
 
@@ -443,10 +463,15 @@ int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_ph
         CK_LAUNCH();
         return EPP_OK;
     }
+    const bool gen = generic_physics(phys);
     if (ctx->lanes == 0) {
         int rc;
-        if (fused) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
-        else if (cont) rc = launch_pass<D, true>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+        auto cont_pass = [&](auto G) {
+            constexpr bool GG = decltype(G)::value;
+            if (fused) return launch_pass<D, true>(ctx, set, crit, CPCont<D, true, GG>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+            return launch_pass<D, true>(ctx, set, crit, CPCont<D, false, GG>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+        };
+        if (fused || cont) rc = gen ? cont_pass(std::true_type{}) : cont_pass(std::false_type{});
         else rc = launch_pass<D, true>(ctx, set, crit, CPCount<D>{ctx->ncount}, ctx->pairs);
         ctx->nlist_valid = rc == EPP_OK;
         return rc;
@@ -463,6 +488,10 @@ int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_ph
         }
         ActContG<D, false, false> act{ctx->S[set], P, ctx->ncount};
         return launch_pair_g<D, decltype(act), false>(ctx, A, act, ctx->pairs, ctx->n);
+    }
+    if (gen) {
+        if (fused) return launch_cellpair<D>(ctx, set, crit, CPCont<D, true, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+        if (cont) return launch_cellpair<D>(ctx, set, crit, CPCont<D, false, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
     }
     if (fused) return launch_cellpair<D>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
     if (cont) return launch_cellpair<D>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
@@ -495,7 +524,7 @@ int run_search(epp_ctx* ctx, int crit, int action, const epp_physics* phys, bool
 // One fused step from set c to 1 - c (captured into a graph by the caller).  With `ev`, an
 // event is recorded before the first and after every kernel (profiling, no graph).
 template <int D>
-int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t* ev = nullptr) {
+int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t* ev = nullptr, bool filter = false) {
 #define EPP_MARK(k) do { if (ev) CK(cudaEventRecord(ev[k], ctx->stream)); } while (0)
     EPP_MARK(0);
     const int to = 1 - c;
@@ -509,12 +538,16 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     mom.F.n = n;
     mom.F.accel = ctx->graph_accel ? ctx->accel : nullptr;
     mom.status = ctx->status;
+    const bool gen = generic_physics(&phys);
     {
-        int rc0 = ctx->lanes >= 2 ? launch_pair_g<D, ActMomG<D, true>, true>(ctx, A, mom, nullptr, n)
-                  : ctx->lanes == 1 ? launch_cellpair<D, CPMom<D, true>, true>(ctx, c, EPP_CRITERION_SYMMETRY,
-                                                                               CPMom<D, true>{mom}, nullptr)
-                                    : launch_list<D, CPMom<D, true>, true>(ctx, c, EPP_CRITERION_SYMMETRY,
-                                                                           CPMom<D, true>{mom});
+        auto mom_pass = [&](auto G) {
+            constexpr bool GG = decltype(G)::value;
+            using M = CPMom<D, true, GG>;
+            return ctx->lanes >= 2 ? launch_pair_g<D, ActMomG<D, true>, true>(ctx, A, mom, nullptr, n)
+                   : ctx->lanes == 1 ? launch_cellpair<D, M, true>(ctx, c, EPP_CRITERION_SYMMETRY, M{mom}, nullptr)
+                                     : launch_list<D, M, true>(ctx, c, EPP_CRITERION_SYMMETRY, M{mom});
+        };
+        const int rc0 = gen ? mom_pass(std::true_type{}) : mom_pass(std::false_type{});
         if (rc0) return rc0;
     }
     EPP_MARK(1);
@@ -537,7 +570,8 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
         rc = launch_build<D>(ctx, to, EPP_CRITERION_SYMMETRY, ctx->pairs);
         if (rc) return rc;
         EPP_MARK(5);
-        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], mom.P, ctx->ncount});
+        rc = gen ? launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], mom.P, ctx->ncount})
+                 : launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], mom.P, ctx->ncount});
         if (rc) return rc;
     } else {
         rc = launch_search_pass<D>(ctx, to, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false,
@@ -546,6 +580,13 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
         EPP_MARK(5);
     }
     EPP_MARK(6);
+    if (filter) {   // the kernel filter after this step's search (main.jl:180-183), family 0
+        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPFilter<D>{ctx->S[to], mom.P, ctx->fwv, ctx->fwr});
+        if (rc) return rc;
+        k_filter_finish<D><<<blocks_for(n), kThreads, 0, ctx->stream>>>(ctx->start[to], ctx->n_cells, n, ctx->S[to],
+                                                                        mom.P, ctx->fwv, ctx->fwr, 1);
+        CK_LAUNCH();
+    }
 #undef EPP_MARK
     return EPP_OK;
 }
@@ -566,22 +607,28 @@ void drop_graphs(epp_ctx* ctx) {
             cudaGraphExecDestroy(ctx->graph[c]);
             ctx->graph[c] = nullptr;
         }
+        if (ctx->graph_f[c]) {
+            cudaGraphExecDestroy(ctx->graph_f[c]);
+            ctx->graph_f[c] = nullptr;
+        }
     }
 }
 
 template <int D>
 int build_graphs(epp_ctx* ctx, const epp_physics& phys) {
     drop_graphs(ctx);
-    for (int c = 0; c < 2; ++c) {
-        cudaGraph_t g;
-        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_fused_step<D>(ctx, c, phys);
-        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-        if (rc) return rc;
-        if (e != cudaSuccess) return fail(ctx, EPP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&ctx->graph[c], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return fail(ctx, EPP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    for (int f = 0; f < (phys.filter_interval > 0 ? 2 : 1); ++f) {
+        for (int c = 0; c < 2; ++c) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_fused_step<D>(ctx, c, phys, nullptr, f == 1);
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(ctx, EPP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(f ? &ctx->graph_f[c] : &ctx->graph[c], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(ctx, EPP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
     }
     ctx->graph_phys = phys;
     return EPP_OK;
@@ -590,6 +637,13 @@ int build_graphs(epp_ctx* ctx, const epp_physics& phys) {
 template <int D>
 int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
     DevPhys P = phys ? dev_phys(ctx, *phys) : DevPhys{};
+    if (action == EPP_ACTION_KERNEL_FILTER_SELF) {
+        k_filter_finish<D><<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], P, ctx->fwv, ctx->fwr, 0);
+        CK_LAUNCH();
+        ctx->filter_pending = false;
+        return EPP_OK;
+    }
     k_self<D><<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(action, ctx->start[ctx->cur], ctx->n_cells,
                                                                 ctx->n, ctx->S[ctx->cur], P, ctx->status,
                                                                 ctx->accel);
@@ -612,6 +666,12 @@ int launch_interaction_pass(epp_ctx* ctx, const Act& act) {
 template <int D>
 int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
     PairArgs A = pair_args(ctx, ctx->cur, ctx->last_crit);
+    if (action == EPP_ACTION_KERNEL_FILTER) {
+        if (ctx->lanes != 0) return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the kernel filter runs on pair-pass family 0");
+        const int rc = launch_interaction_pass<D>(ctx, CPFilter<D>{ctx->S[ctx->cur], dev_phys(ctx, *phys), ctx->fwv, ctx->fwr});
+        if (rc == EPP_OK) ctx->filter_pending = true;
+        return rc;
+    }
     if (action == EPP_ACTION_DAMBREAK_MOMENTUM) {
         k_prep_rp4<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(ctx->start[ctx->cur], ctx->n_cells, ctx->n,
                                                                       ctx->S[ctx->cur]);
@@ -623,6 +683,10 @@ int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
         act.F = FusedOut{};
         act.status = ctx->status;
         if (ctx->lanes >= 2) return launch_pair_g<D, decltype(act), false>(ctx, A, act, nullptr, ctx->n);
+        if (generic_physics(phys)) {
+            if (ctx->lanes == 1) return launch_cellpair<D>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false, true>{act}, nullptr);
+            return launch_interaction_pass<D>(ctx, CPMom<D, false, true>{act});
+        }
         if (ctx->lanes == 1) return launch_cellpair<D>(ctx, ctx->cur, ctx->last_crit, CPMom<D, false>{act}, nullptr);
         return launch_interaction_pass<D>(ctx, CPMom<D, false>{act});
     }
@@ -645,6 +709,14 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         if (!rc) rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_INTEGRATE, &phys);
         if (!rc) rc = run_search<D>(ctx, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false);
         if (rc) return rc;
+        ++ctx->step_count;
+        if (phys.filter_interval > 0 && ctx->step_count % phys.filter_interval == 0) {
+            rc = run_interaction<D>(ctx, EPP_ACTION_KERNEL_FILTER, &phys);
+            if (!rc) rc = run_selfaction<D>(ctx, EPP_ACTION_KERNEL_FILTER_SELF, &phys);
+            if (rc) return rc;
+            ctx->filter_pending = false;
+            ctx->rpn_valid = false;
+        }
         CK(cudaMemsetAsync(ctx->S[0].dv, 0, sizeof(float4) * ctx->cap, ctx->stream));
         CK(cudaMemsetAsync(ctx->S[1].dv, 0, sizeof(float4) * ctx->cap, ctx->stream));
         ctx->dv_dirty = false;
@@ -665,7 +737,9 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         if (rc) return rc;
     }
     for (int s = 0; s < n_steps; ++s) {
-        CK(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+        ++ctx->step_count;
+        const bool f = phys.filter_interval > 0 && ctx->step_count % phys.filter_interval == 0;
+        CK(cudaGraphLaunch(f ? ctx->graph_f[ctx->cur] : ctx->graph[ctx->cur], ctx->stream));
         ctx->cur = 1 - ctx->cur;
     }
     ctx->rpn_valid = true;
@@ -677,7 +751,24 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     return EPP_OK;
 }
 
+// The physics options a call may use with this context's pair-pass family.
+int check_physics(epp_ctx* ctx, const epp_physics* p) {
+    if (!p) return EPP_OK;
+    if (p->kernel < EPP_KERNEL_WENDLAND_C2 || p->kernel > EPP_KERNEL_WENDLAND_C4 || p->eos < EPP_EOS_TAIT ||
+        p->eos > EPP_EOS_LINEAR || p->motion < EPP_MOTION_SYMPLECTIC || p->motion > EPP_MOTION_ACCELERATE_MOVE ||
+        p->viscosity < EPP_VISCOSITY_REFERENCE || p->viscosity > EPP_VISCOSITY_CLASSIC || p->filter_interval < 0)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics option out of range (kernel %d, eos %d, motion %d, "
+                    "viscosity %d, filter_interval %d)", p->kernel, p->eos, p->motion, p->viscosity, p->filter_interval);
+    if (ctx->lanes >= 2 && (p->kernel != EPP_KERNEL_WENDLAND_C2 || p->viscosity == EPP_VISCOSITY_CLASSIC))
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION,
+                    "the lane-group pair passes run Wendland C2 with artificial viscosity; use family 0 or 1");
+    if (ctx->lanes != 0 && p->filter_interval > 0)
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the kernel filter runs on pair-pass family 0");
+    return EPP_OK;
+}
+
 }  // namespace
+
 
 // =========================================================================================
 extern "C" {
@@ -773,6 +864,8 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->iresult = a.take<double>(8);
     ctx->iticket = a.take<unsigned>(1);
     ctx->ihmin = a.take<double>(1);
+    ctx->fwv = a.take<float>(ctx->cap);
+    ctx->fwr = a.take<float>(ctx->cap);
     ctx->tmp.count = ctx->count;
     ctx->tmp.cs = ctx->cs;
     ctx->tmp.scan_state = ctx->scan_state;
@@ -815,8 +908,7 @@ int32_t epp_destroy(epp_ctx* ctx) {
     cudaSetDevice(ctx->dev);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->stream = ctx->own_stream;   // the frees below are ordered on the context's own stream
-    for (int c = 0; c < 2; ++c)
-        if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
+    drop_graphs(ctx);
     dev_free(ctx, ctx->accel);
     dev_free(ctx, ctx->inst_table);
     dev_free(ctx, ctx->nlist);
@@ -918,6 +1010,10 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     else launch(std::integral_constant<int, 3>{});
     CK_LAUNCH();
     drop_graphs(ctx);   // the captured launches hold the old particle count
+    CK(cudaMemsetAsync(ctx->fwv, 0, sizeof(float) * ctx->cap, ctx->stream));
+    CK(cudaMemsetAsync(ctx->fwr, 0, sizeof(float) * ctx->cap, ctx->stream));
+    ctx->filter_pending = false;
+    ctx->step_count = 0;
     ctx->searched = false;
     ctx->sorted_once = false;
     ctx->nlist_valid = false;
@@ -1020,6 +1116,9 @@ int32_t epp_search(epp_ctx* ctx, int32_t criterion, int32_t action, const epp_ph
         return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "search action %d", action);
     if (action == EPP_ACTION_DAMBREAK_CONTINUITY && !phys)
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
+    if (const int prc = check_physics(ctx, phys)) return prc;
+    if (ctx->filter_pending)
+        return fail(ctx, EPP_ERR_STATE, "kernel-filter sums pending: selfaction!(KERNEL_FILTER_SELF) first");
     cudaSetDevice(ctx->dev);
     if (ctx->n == 0) return EPP_OK;
     const bool emit = (flags & EPP_SEARCH_EMIT_LIST) != 0;
@@ -1030,10 +1129,12 @@ int32_t epp_search(epp_ctx* ctx, int32_t criterion, int32_t action, const epp_ph
 int32_t epp_interaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     if (action == EPP_ACTION_NONE) return EPP_OK;
-    if (action != EPP_ACTION_DAMBREAK_MOMENTUM && action != EPP_ACTION_COUNT_NEIGHBOURS)
+    if (action != EPP_ACTION_DAMBREAK_MOMENTUM && action != EPP_ACTION_COUNT_NEIGHBOURS &&
+        action != EPP_ACTION_KERNEL_FILTER)
         return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "interaction action %d", action);
-    if (action == EPP_ACTION_DAMBREAK_MOMENTUM && !phys)
+    if ((action == EPP_ACTION_DAMBREAK_MOMENTUM || action == EPP_ACTION_KERNEL_FILTER) && !phys)
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
+    if (const int prc = check_physics(ctx, phys)) return prc;
     if (!ctx->searched)
         return fail(ctx, EPP_ERR_STATE, "interaction! needs a search! at the current positions");
     cudaSetDevice(ctx->dev);
@@ -1046,10 +1147,11 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     if (action == EPP_ACTION_NONE) return EPP_OK;
     if (action != EPP_ACTION_DAMBREAK_DENSITY && action != EPP_ACTION_DAMBREAK_INTEGRATE &&
-        action != EPP_ACTION_ZERO_DVELOCITY)
+        action != EPP_ACTION_ZERO_DVELOCITY && action != EPP_ACTION_KERNEL_FILTER_SELF)
         return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "selfaction action %d", action);
     if (action != EPP_ACTION_ZERO_DVELOCITY && !phys)
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
+    if (const int prc = check_physics(ctx, phys)) return prc;
     if (!ctx->sorted_once)
         return fail(ctx, EPP_ERR_STATE, "selfaction! runs on the cell-sorted state: call search! first");
     cudaSetDevice(ctx->dev);
@@ -1060,7 +1162,7 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
         ctx->searched = false;   // positions moved: the next pass needs a search!
         ctx->rpn_valid = false;
     }
-    if (action == EPP_ACTION_DAMBREAK_DENSITY) ctx->rpn_valid = false;
+    if (action == EPP_ACTION_DAMBREAK_DENSITY || action == EPP_ACTION_KERNEL_FILTER_SELF) ctx->rpn_valid = false;
     if (action == EPP_ACTION_ZERO_DVELOCITY) ctx->dv_dirty = true;
     ctx->lists_valid = ctx->lists_valid && action != EPP_ACTION_DAMBREAK_INTEGRATE;
     return rc;
@@ -1069,6 +1171,9 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
 int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     if (!phys || n_steps < 0) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (const int prc = check_physics(ctx, phys)) return prc;
+    if (ctx->filter_pending)
+        return fail(ctx, EPP_ERR_STATE, "kernel-filter sums pending: selfaction!(KERNEL_FILTER_SELF) first");
     if (!ctx->searched)
         return fail(ctx, EPP_ERR_STATE, "epp_step needs an initial search! (main.jl:157-164)");
     cudaSetDevice(ctx->dev);

@@ -62,6 +62,18 @@ __device__ __forceinline__ void pair_consts(const TargetConst& tc, HPairCache& p
     hh = pc.hh;
 }
 
+// (dW/dr) / r of a pair: the cached Wendland C2 closed form, or (GEN) the selected kernel's; 0
+// outside the support.
+template <int D, bool GEN>
+__device__ __forceinline__ float pair_dwr(int kernel, float q, float hinv, float kdw) {
+    if (!GEN || kernel == EPP_KERNEL_WENDLAND_C2) {
+        if (!(q < 2.0f)) return 0.0f;   // W = dW = 0 at q >= 2 (WendlandC2.jl:23,44)
+        const float u = 2.0f - q;
+        return kdw * (u * u * u);
+    }
+    return kern_dwr<D>(kernel, q, hinv);
+}
+
 template <int D>
 struct CPShared {
     float4 cx[CPConf<D>::C];     // staged candidate (x, h)
@@ -91,8 +103,9 @@ struct PairGeo {
 };
 
 // ---------------------------------------------------------------------------------------------
-// Continuity (search! action of main.jl:74-90) as a per-pair contribution.
-template <int D, bool FUSED>
+// Continuity (search! action of main.jl:74-90) as a per-pair contribution.  GEN: any kernel of
+// EPP_KERNEL_*; otherwise Wendland C2 from its cached closed form (the benchmark physics).
+template <int D, bool FUSED, bool GEN = false>
 struct CPCont {
     State s;
     DevPhys P;
@@ -119,10 +132,8 @@ struct CPCont {
         const float r = sqrtf(g.dr2);
         float hinv, kdw, hh;
         pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
-        const float q = r * hinv;
-        if (!(q < 2.0f)) return out;     // W = dW = 0 at q >= 2 (WendlandC2.jl:23,44)
-        const float u = 2.0f - q;
-        const float dwr = kdw * (u * u * u);
+        const float dwr = pair_dwr<D, GEN>(P.kernel, r * hinv, hinv, kdw);
+        if (dwr == 0.0f) return out;
         float vdx = g.dx * (me.v.x - nb.v.x);
         vdx += g.dy * (me.v.y - nb.v.y);
         if (D == 3) vdx += g.dz * (me.v.z - nb.v.z);
@@ -202,8 +213,9 @@ struct CPCountDv {
 };
 
 // Momentum (interaction! of main.jl:107-118) as a per-pair contribution; FUSED adds the
-// integrate + bin epilogue of the fused step.
-template <int D, bool FUSED>
+// integrate + bin epilogue of the fused step.  GEN: any kernel and EPP_VISCOSITY_CLASSIC; otherwise
+// Wendland C2 with artificial viscosity (the benchmark physics).
+template <int D, bool FUSED, bool GEN = false>
 struct CPMom {
     ActMomG<D, FUSED> m;   // state, physics, fused outputs, integrate_and_bin
     static constexpr int NC = 3;
@@ -229,16 +241,24 @@ struct CPMom {
         const float r = sqrtf(g.dr2);
         float hinv, kdw, hh;
         pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
-        const float q = r * hinv;
-        if (!(q < 2.0f)) return out;
-        const float u = 2.0f - q;
-        const float dwr = kdw * (u * u * u);
+        const float dwr = pair_dwr<D, GEN>(P.kernel, r * hinv, hinv, kdw);
+        if (dwr == 0.0f) return out;
         const float4 rpi = me.rp, rpj = nb.rp, vi = me.v, vj = nb.v;
         const float p_rho_2 = ff ? rpi.z + rpj.z : (rpi.y + rpj.y) * rpi.w * rpj.w;
         const float fp = p_rho_2 * (-vj.w * dwr);
         out.x = fp * g.dx;
         out.y = fp * g.dy;
         if (D == 3) out.z = fp * g.dz;
+        if (GEN && P.visc == EPP_VISCOSITY_CLASSIC) {
+            // iClassicViscosity! (Viscosity.jl:10-26): 2 mu m_j r dW / (rho_i rho_j (r^2 + 0.01 h^2))
+            // times (u_i - u_j); r dW = r^2 (dW / r)
+            const float az = g.dr2 + 0.01f * hh * hh;
+            const float force = __fdividef(2.0f * P.mu * vj.w * g.dr2 * dwr * rpi.w * rpj.w, az);
+            out.x += force * (vi.x - vj.x);
+            out.y += force * (vi.y - vj.y);
+            if (D == 3) out.z += force * (vi.z - vj.z);
+            return out;
+        }
         float vdx = g.dx * (vi.x - vj.x);
         vdx += g.dy * (vi.y - vj.y);
         if (D == 3) vdx += g.dz * (vi.z - vj.z);
@@ -270,6 +290,45 @@ struct CPMom {
     __device__ __forceinline__ void end_idle(int i, int ti) const {
         if (FUSED) m.integrate_and_bin(i, ti, nullptr);
     }
+};
+
+// Kernel filter (iFilter of main.jl:128-134: iKernelFilter!, Filter.jl:10-23) over fluid-fluid
+// pairs: the sums wv += W V_j and wv_rho += W m_j, added to the per-particle filter sums.
+template <int D>
+struct CPFilter {
+    State s;
+    DevPhys P;
+    float* wv;
+    float* wvr;
+    static constexpr int NC = 2;
+    __device__ __forceinline__ bool wants(int ti) const { return ti == P.fluid; }
+    struct Self {};
+    struct Nb {
+        float vol, m;
+    };
+    __device__ __forceinline__ Self self(int) const { return Self{}; }
+    __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{s.vol[j], s.vm[j].w}; }
+    __device__ __forceinline__ float4 term(const Self&, const Nb& nb, int, int tj, float4 xj, const PairGeo& g,
+                                           const TargetConst& tc, HPairCache& pc) const {
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (tj != P.fluid) return out;
+        float hinv, kdw, hh;
+        pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
+        const float w = kern_value<D>(P.kernel, sqrtf(g.dr2), hinv);
+        out.x = w * nb.vol;
+        out.y = w * nb.m;
+        return out;
+    }
+    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4, float4 xj, const PairGeo& g,
+                                              const TargetConst& tc) const {
+        HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
+        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc, pc);
+    }
+    __device__ __forceinline__ void end(int i, int, float4 sum, int) const {
+        wv[i] += sum.x;
+        wvr[i] += sum.y;
+    }
+    __device__ __forceinline__ void end_idle(int, int) const {}
 };
 
 // Segmented inclusive scan over runs of equal key (keys are non-decreasing across lanes).

@@ -39,8 +39,9 @@ struct InstPhys {
 struct DevPhys {
     float dt, rho0, c0, p0, B;
     float g[3];
-    float alpha, beta;
+    float alpha, beta, mu;
     int gamma, visc, fluid, wall, kahan;
+    int kernel, eos, motion;   // EPP_KERNEL_*, EPP_EOS_*, EPP_MOTION_*
     const InstPhys* ip;
     __device__ __forceinline__ float dt_of(int inst) const { return ip ? ip[inst].dt : dt; }
     __device__ __forceinline__ float c0_of(int inst) const { return ip ? ip[inst].c0 : c0; }
@@ -164,9 +165,43 @@ __device__ __forceinline__ float wc2_gradient(float r, float hinv) {
     return 0.0f;
 }
 
-// Tait EOS: p = B ((rho / rho0)^gamma - 1) + p0 (replaces the linear eos of main.jl:64).
+// Tait EOS: p = B ((rho / rho0)^gamma - 1) + p0 (the benchmark's, replacing main.jl:64), or the
+// example's linear EOS p = c0^2 (rho - rho0) + p0 (main.jl:58,64; c0^2 rounded once).
 __device__ __forceinline__ float eos(const DevPhys& P, int inst, float rho) {
+    if (P.eos == EPP_EOS_LINEAR) {
+        const float c0 = P.c0_of(inst);
+        return __fadd_rn(__fmul_rn(__fmul_rn(c0, c0), __fsub_rn(rho, P.rho0)), P.p0);
+    }
     return P.B_of(inst) * (powi(__fdiv_rn(rho, P.rho0), P.gamma) - 1.0f) + P.p0;
+}
+
+// One fluid particle's velocity and position update from du (gravity already added), IEEE in the
+// reference's order.  EPP_MOTION_SYMPLECTIC: sAccelerate! then sMove! (Motion.jl:17-51),
+// u += du dt, x += u dt.  EPP_MOTION_ACCELERATE_MOVE: sAccelerateMove! (Motion.jl:61-75),
+// x += (u + du dt 0.5) dt with the old u, then u += du dt.  With P.kahan the position increment is
+// added with compensated (Kahan) summation (new; no reference counterpart).
+template <int D>
+__device__ __forceinline__ void advance(const DevPhys& P, float dt, const float (&du)[3], float (&vv)[3],
+                                        float (&xx)[3], float (&cc)[3]) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        float inc;
+        if (P.motion == EPP_MOTION_ACCELERATE_MOVE) {
+            inc = __fmul_rn(__fadd_rn(vv[k], __fmul_rn(__fmul_rn(du[k], dt), 0.5f)), dt);
+            vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], dt));
+        } else {
+            vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], dt));
+            inc = __fmul_rn(vv[k], dt);
+        }
+        if (P.kahan) {
+            const float y = __fsub_rn(inc, cc[k]);
+            const float t = __fadd_rn(xx[k], y);
+            cc[k] = __fsub_rn(__fsub_rn(t, xx[k]), y);
+            xx[k] = t;
+        } else {
+            xx[k] = __fadd_rn(xx[k], inc);
+        }
+    }
 }
 
 // (rho, p, p / rho^2, 1 / rho): what a momentum pass needs of a neighbour (Pressure.jl:24-60).

@@ -8,6 +8,7 @@
 // operations (no contraction) so the neighbour sets are bit-exact.
 #pragma once
 #include "epp_cells.cuh"
+#include "epp_kernels.cuh"
 
 namespace epp {
 
@@ -169,10 +170,10 @@ struct ActSearch {
             const bool wf = ti == P.wall && tj == P.fluid;
             if (ff || fw || wf) {
                 const float hinv = a.hc.pair_hinv(xj.w);
-                const float dw = wc2_gradient<D>(r, hinv);
+                const float dw = kern_gradient<D>(P.kernel, r, hinv);
                 if (EMIT && k < L.max_nb) {
                     L.hinv[(size_t)k * L.cap + i] = hinv;
-                    L.w[(size_t)k * L.cap + i] = wc2_value<D>(r, hinv);
+                    L.w[(size_t)k * L.cap + i] = kern_value<D>(P.kernel, r, hinv);
                     L.dw[(size_t)k * L.cap + i] = dw;
                 }
                 const float4 vj = s.vm[j];

@@ -282,21 +282,8 @@ struct ActMomG {
             float du[3] = {a->du[0], a->du[1], a->du[2]};
             float vv[3] = {v.x, v.y, v.z}, xx[3] = {x.x, x.y, x.z}, cc[3] = {cp.x, cp.y, cp.z};
 #pragma unroll
-            for (int k = 0; k < D; ++k) {
-                du[k] = __fadd_rn(du[k], P.g[k]);
-                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], dt));
-            }
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                if (P.kahan) {
-                    const float y = __fsub_rn(__fmul_rn(vv[k], dt), cc[k]);
-                    const float t = __fadd_rn(xx[k], y);
-                    cc[k] = __fsub_rn(__fsub_rn(t, xx[k]), y);
-                    xx[k] = t;
-                } else {
-                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], dt));
-                }
-            }
+            for (int k = 0; k < D; ++k) du[k] = __fadd_rn(du[k], P.g[k]);
+            advance<D>(P, dt, du, vv, xx, cc);
             x.x = xx[0]; x.y = xx[1]; x.z = xx[2];
             v.x = vv[0]; v.y = vv[1]; v.z = vv[2];
             cp.x = cc[0]; cp.y = cc[1]; cp.z = cc[2];

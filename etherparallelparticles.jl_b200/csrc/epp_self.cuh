@@ -7,7 +7,9 @@ namespace epp {
 
 // selfaction! (Action.jl:39-51) bodies.  Alive particles are the first start[n_cells] rows.
 // DAMBREAK_DENSITY: sContinuity! wrapper of main.jl:92-105 (Continuity.jl:10-21, State.jl:10-19).
-// DAMBREAK_INTEGRATE: sMomentum! of main.jl:120-126 with sAccelerate! + sMove! (Motion.jl:17-51).
+// DAMBREAK_INTEGRATE: sMomentum! of main.jl:120-126: sGravity!, then sAccelerate! + sMove! or
+// sAccelerateMove! (Motion.jl:17-75) by P.motion.
+// KERNEL_FILTER_SELF: sFilter of main.jl:136-144 (Filter.jl:25-38, State.jl:10-19).
 template <int D>
 __global__ void k_self(int action, const int* start, int n_cells, int n_max, State s, DevPhys P,
                        unsigned* status, float4* accel) {
@@ -35,21 +37,8 @@ __global__ void k_self(int action, const int* start, int n_cells, int n_max, Sta
             float du[3] = {d.x, d.y, d.z}, vv[3] = {v.x, v.y, v.z}, xx[3] = {x.x, x.y, x.z};
             float cc[3] = {c.x, c.y, c.z};
 #pragma unroll
-            for (int k = 0; k < D; ++k) {
-                du[k] = __fadd_rn(du[k], P.g[k]);
-                vv[k] = __fadd_rn(vv[k], __fmul_rn(du[k], dt));
-            }
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                if (P.kahan) {
-                    const float y = __fsub_rn(__fmul_rn(vv[k], dt), cc[k]);
-                    const float t = __fadd_rn(xx[k], y);
-                    cc[k] = __fsub_rn(__fsub_rn(t, xx[k]), y);
-                    xx[k] = t;
-                } else {
-                    xx[k] = __fadd_rn(xx[k], __fmul_rn(vv[k], dt));
-                }
-            }
+            for (int k = 0; k < D; ++k) du[k] = __fadd_rn(du[k], P.g[k]);
+            advance<D>(P, dt, du, vv, xx, cc);
             if (accel) accel[i] = make_float4(du[0], du[1], du[2], 0.0f);
             s.dv[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             s.vm[i] = make_float4(vv[0], vv[1], vv[2], v.w);
@@ -58,6 +47,37 @@ __global__ void k_self(int action, const int* start, int n_cells, int n_max, Sta
             if (!(isfinite(vv[0]) && isfinite(vv[1]) && isfinite(vv[2])))
                 atomicOr(status, EPP_STATUS_NONFINITE);
         }
+    }
+}
+
+// sFilter (main.jl:136-144: sKernelFilter!, Filter.jl:25-38; sVolume!; eos) for the fluid:
+// rho = (wv_rho + W0 m) / (wv + W0 V) with W0 = sigma (1/h)^N, the sums reset to zero, V = m / rho,
+// p = eos(rho).  `preview`: also refresh the next fused step's density preview (rp4) of fluid and
+// wall particles, which the filtered density changes.
+template <int D>
+__global__ void k_filter_finish(const int* start, int n_cells, int n_max, State s, DevPhys P, float* wv,
+                                float* wvr, int preview) {
+    const int n_alive = min(start[n_cells], n_max);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_alive) return;
+    const int tm = s.tagm[i];
+    const int ti = tag_of(tm);
+    const int inst = inst_of(tm);
+    if (ti == P.fluid) {
+        const float m = s.vm[i].w;
+        const float w0 = kern_value0<D>(P.kernel, __fdiv_rn(1.0f, s.xh[i].w));
+        const float a = __fadd_rn(wv[i], __fmul_rn(w0, s.vol[i]));
+        const float b = __fadd_rn(wvr[i], __fmul_rn(w0, m));
+        const float rho = __fdiv_rn(b, a);
+        wv[i] = 0.0f;
+        wvr[i] = 0.0f;
+        s.rho[i] = rho;
+        s.vol[i] = __fdiv_rn(m, rho);
+        s.p[i] = eos(P, inst, rho);
+    }
+    if (preview && (ti == P.fluid || ti == P.wall)) {
+        const float rn = __fadd_rn(s.rho[i], __fmul_rn(s.drho[i], P.dt_of(inst)));
+        s.rp4[i] = make_rp4(rn, eos(P, inst, rn));
     }
 }
 
@@ -127,9 +147,12 @@ __device__ __forceinline__ double powi_d(double x, int n) {
     return r;
 }
 
-// Weakly compressible internal energy per unit mass of the Tait EOS (as the oracle):
-// (B / rho0) ((rho/rho0)^(gamma-1) / (gamma-1) + rho0/rho - gamma/(gamma-1)) + p0 (1/rho0 - 1/rho).
-__device__ __forceinline__ double tait_energy(double r, double rho0, double B, int gam, double p0) {
+// Internal energy per unit mass of the EOS, zero at rho0 (as the oracle): the integral of p / rho^2.
+// Tait: (B / rho0) ((rho/rho0)^(gamma-1) / (gamma-1) + rho0/rho - gamma/(gamma-1)) + p0 (1/rho0 - 1/rho);
+// linear: c0^2 (ln(rho/rho0) + rho0/rho - 1) + p0 (1/rho0 - 1/rho).
+__device__ __forceinline__ double eos_energy(int eos_kind, double r, double rho0, double B, int gam, double p0,
+                                             double c0) {
+    if (eos_kind == EPP_EOS_LINEAR) return c0 * c0 * (log(r / rho0) + rho0 / r - 1.0) + p0 * (1.0 / rho0 - 1.0 / r);
     const double g1 = (double)(gam - 1);
     return (B / rho0) * (powi_d(r / rho0, gam - 1) / g1 + rho0 / r - (double)gam / g1) + p0 * (1.0 / rho0 - 1.0 / r);
 }
@@ -155,7 +178,7 @@ __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells
         const double u2 = (double)vm.x * vm.x + (double)vm.y * vm.y + (D == 3 ? (double)vm.z * vm.z : 0.0);
         v[2] += 0.5 * m * u2;
         v[3] += -m * (g0 * xh.x + g1 * xh.y + (D == 3 ? g2 * xh.z : 0.0));
-        v[4] += m * tait_energy((double)s.rho[i], rho0, B, gam, p0);
+        v[4] += m * eos_energy(P.eos, (double)s.rho[i], rho0, B, gam, p0, c0);
         v[5] = fmax(v[5], sqrt(u2));
         v[6] = fmin(v[6], (double)xh.w);
     }
@@ -221,7 +244,7 @@ __global__ void __launch_bounds__(256) k_integrals_inst(const int* start, DevDom
         const double u2 = (double)vm.x * vm.x + (double)vm.y * vm.y + (D == 3 ? (double)vm.z * vm.z : 0.0);
         v[2] += 0.5 * m * u2;
         v[3] += -m * (g0 * xh.x + g1 * xh.y + (D == 3 ? g2 * xh.z : 0.0));
-        v[4] += m * tait_energy((double)s.rho[i], rho0, B, gam, p0);
+        v[4] += m * eos_energy(P.eos, (double)s.rho[i], rho0, B, gam, p0, c0);
         v[5] = fmax(v[5], sqrt(u2));
         v[6] = fmin(v[6], (double)xh.w);
     }

@@ -5,7 +5,7 @@ the header cites the reference interface each entry point replaces.
 """
 import ctypes as C
 
-EPP_ABI_VERSION = 1
+EPP_ABI_VERSION = 2
 EPP_MAX_TAGS = 16
 
 # epp_status
@@ -54,6 +54,8 @@ EPP_ACTION_DAMBREAK_MOMENTUM = 3
 EPP_ACTION_DAMBREAK_INTEGRATE = 4
 EPP_ACTION_ZERO_DVELOCITY = 5
 EPP_ACTION_COUNT_NEIGHBOURS = 6
+EPP_ACTION_KERNEL_FILTER = 7
+EPP_ACTION_KERNEL_FILTER_SELF = 8
 
 EPP_SEARCH_EMIT_LIST = 1
 
@@ -61,6 +63,18 @@ EPP_PROFILE_STAGES = 6   # momentum+integrate+bin, scan, scatter, rank+gather, s
 
 EPP_VISCOSITY_REFERENCE = 0
 EPP_VISCOSITY_MONAGHAN = 1
+EPP_VISCOSITY_CLASSIC = 2
+
+EPP_KERNEL_WENDLAND_C2 = 0
+EPP_KERNEL_CUBIC_SPLINE = 1
+EPP_KERNEL_GAUSSIAN = 2
+EPP_KERNEL_WENDLAND_C4 = 3
+
+EPP_EOS_TAIT = 0
+EPP_EOS_LINEAR = 1
+
+EPP_MOTION_SYMPLECTIC = 0
+EPP_MOTION_ACCELERATE_MOVE = 1
 
 
 class epp_domain(C.Structure):
@@ -86,6 +100,11 @@ class epp_physics(C.Structure):
         ("fluid_tag", C.c_int32),
         ("wall_tag", C.c_int32),
         ("kahan", C.c_int32),
+        ("kernel", C.c_int32),
+        ("eos", C.c_int32),
+        ("mu", C.c_float),
+        ("motion", C.c_int32),
+        ("filter_interval", C.c_int32),
     ]
 
 
@@ -150,7 +169,8 @@ def make_domain(dim, gap, first, last):
 
 def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81, 0.0),
                  alpha=0.1, beta=0.1, viscosity=EPP_VISCOSITY_REFERENCE, fluid_tag=1,
-                 wall_tag=2, kahan=1):
+                 wall_tag=2, kahan=1, kernel=EPP_KERNEL_WENDLAND_C2, eos=EPP_EOS_TAIT, mu=0.0,
+                 motion=EPP_MOTION_SYMPLECTIC, filter_interval=0):
     p = epp_physics()
     p.dt = dt
     p.rho0 = rho0
@@ -165,6 +185,11 @@ def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81
     p.fluid_tag = fluid_tag
     p.wall_tag = wall_tag
     p.kahan = kahan
+    p.kernel = kernel
+    p.eos = eos
+    p.mu = mu
+    p.motion = motion
+    p.filter_interval = filter_interval
     return p
 
 

@@ -92,15 +92,55 @@ def _layout(dim, max_nb, instance=False):
 
 def dam_break_2d(dx=0.02, tank=(4.0, 3.0), column=(1.0, 2.0), wall_layers=3, h_factor=1.5,
                  max_neighbour_number=40, reference_quirk=False, kahan=1,
-                 viscosity=abi.EPP_VISCOSITY_REFERENCE, alpha=0.1, beta=0.1):
-    """2D dry dam break (casegen.jl:17-146 geometry; benchmark physics)."""
+                 viscosity=abi.EPP_VISCOSITY_REFERENCE, alpha=0.1, beta=0.1, physics="benchmark"):
+    """2D dry dam break (casegen.jl:17-146 geometry).  physics="benchmark": Wendland C2, Tait EOS,
+    artificial viscosity, symplectic Euler, hydrostatic initial density.  physics="example": the
+    reference example's own (main.jl:53-144): CubicSpline, linear EOS with c0 = 120, classic
+    viscosity mu = 1e-3, sAccelerateMove!, kernel filter every 20 steps, g = 9.8,
+    dt = 2 * 0.1 h0 / c0, uniform initial density rho0 and pressure p0."""
     height = column[1]
     c0 = 10.0 * math.sqrt(2.0 * GRAVITY * height)
     domain = _tank_domain_2d(dx, tank, wall_layers, h_factor)
     parts = _dam_parts_2d(dx, tank, column, wall_layers, reference_quirk)
+    if physics == "example":
+        return _assemble_example(domain, parts, h_factor, max_neighbour_number,
+                                 {"dx": dx, "tank": tank, "column": column, "reference_quirk": reference_quirk})
     return _assemble(2, domain, parts, h_factor, height, c0, max_neighbour_number, kahan,
                      viscosity, alpha, beta, {"dx": dx, "tank": tank, "column": column,
                                               "reference_quirk": reference_quirk})
+
+
+EXAMPLE_C0 = 120.0    # main.jl:57
+EXAMPLE_MU0 = 1e-3    # casegen.jl:78
+EXAMPLE_G = 9.8       # main.jl:56
+
+
+def _assemble_example(domain, parts, h_factor, max_nb, meta):
+    st = _state(2, parts, h_factor, 1.0, EXAMPLE_C0)
+    n = st["Tag"].shape[0]
+    st["Density"] = np.full(n, np.float32(RHO0), np.float32)          # casegen.jl:93,103
+    st["Mass"] = (st["Density"] * st["Volume"]).astype(np.float32)
+    st["Pressure"] = np.zeros(n, np.float32)                          # p0 = 0
+    ints, floats = _layout(2, max_nb)
+    params = OrderedDict([("rho0", RHO0), ("p0", 0.0), ("FLUID_TAG", FLUID_TAG), ("WALL_TAG", WALL_TAG),
+                          ("gap0", meta["dx"]), ("h0", h_factor * meta["dx"]), ("mu0", EXAMPLE_MU0)])
+    ps = ParticleSystem(domain, n, ints, floats, params)
+    for k, v in st.items():
+        ps[k] = v
+    h0 = np.float32(h_factor * meta["dx"])
+    c0f = np.float32(EXAMPLE_C0)
+    dt = float(np.float32(np.float32(0.1 * float(h0) / float(c0f))) * np.float32(2))   # main.jl:68
+    physics = abi.make_physics(dt, rho0=RHO0, c0=float(c0f), p0=0.0, gamma=GAMMA, gravity=(0.0, -EXAMPLE_G, 0.0),
+                               alpha=0.0, beta=0.0, viscosity=abi.EPP_VISCOSITY_CLASSIC, fluid_tag=FLUID_TAG,
+                               wall_tag=WALL_TAG, kahan=0, kernel=abi.EPP_KERNEL_CUBIC_SPLINE,
+                               eos=abi.EPP_EOS_LINEAR, mu=EXAMPLE_MU0, motion=abi.EPP_MOTION_ACCELERATE_MOVE,
+                               filter_interval=20)
+    fl = st["Tag"] == FLUID_TAG
+    meta = dict(meta)
+    meta.update({"n": n, "n_fluid": int(fl.sum()), "n_wall": int((~fl).sum()), "c0": float(c0f), "dt": dt,
+                 "h": float(h0), "dim": 2, "height": meta["column"][1], "n_cells": domain.get_n(),
+                 "physics": "example"})
+    return DamBreakCase(ps, domain, physics, meta)
 
 
 def _tank_domain_2d(dx, tank, wall_layers, h_factor):

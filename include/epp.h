@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define EPP_ABI_VERSION 1
+#define EPP_ABI_VERSION 2
 #define EPP_MAX_TAGS 16
 
 typedef enum epp_status {
@@ -69,13 +69,32 @@ typedef enum epp_status {
 #define EPP_ACTION_DAMBREAK_INTEGRATE    4 /* selfaction!: gravity, sAccelerate!, sMove!  main.jl:120-126 */
 #define EPP_ACTION_ZERO_DVELOCITY        5 /* selfaction!: dVelocity = 0 (test helper, ActionTest.jl:66-69) */
 #define EPP_ACTION_COUNT_NEIGHBOURS      6 /* interaction!: dVelocity += 1 per neighbour (ActionTest.jl:71-75) */
+#define EPP_ACTION_KERNEL_FILTER         7 /* interaction!: iFilter, fluid-fluid: wv += W V_j, wv_rho += W m_j
+                                            * (main.jl:128-134, Filter.jl:10-23) */
+#define EPP_ACTION_KERNEL_FILTER_SELF    8 /* selfaction!: sFilter, fluid: rho = (wv_rho + W0 m)/(wv + W0 V),
+                                            * V = m/rho, p = eos (main.jl:136-144, Filter.jl:25-38) */
 
 /* epp_search flags */
 #define EPP_SEARCH_EMIT_LIST 1 /* keep per-particle neighbour lists for epp_download */
 
-/* Artificial-viscosity forms */
-#define EPP_VISCOSITY_REFERENCE 0 /* Viscosity.jl:28-52 as written: extra 1/(rho_i rho_j) */
-#define EPP_VISCOSITY_MONAGHAN  1 /* textbook Monaghan: divide by the mean density only */
+/* Viscosity forms */
+#define EPP_VISCOSITY_REFERENCE 0 /* artificial, Viscosity.jl:28-52 as written: extra 1/(rho_i rho_j) */
+#define EPP_VISCOSITY_MONAGHAN  1 /* artificial, textbook Monaghan: divide by the mean density only */
+#define EPP_VISCOSITY_CLASSIC   2 /* physical, iClassicViscosity! (Viscosity.jl:10-26) with mu */
+
+/* Smoothing kernels (src/SPH/Kernel/: WendlandC2.jl, CubicSpline.jl, Gaussian.jl, WendlandC4.jl) */
+#define EPP_KERNEL_WENDLAND_C2  0
+#define EPP_KERNEL_CUBIC_SPLINE 1
+#define EPP_KERNEL_GAUSSIAN     2
+#define EPP_KERNEL_WENDLAND_C4  3
+
+/* Equations of state */
+#define EPP_EOS_TAIT   0 /* p = rho0 c0^2 / gamma ((rho/rho0)^gamma - 1) + p0 (benchmark) */
+#define EPP_EOS_LINEAR 1 /* p = c0^2 (rho - rho0) + p0 (main.jl:64) */
+
+/* Time integration of the fluid */
+#define EPP_MOTION_SYMPLECTIC       0 /* sAccelerate! + sMove!: u += du dt, x += u dt (Motion.jl:17-51) */
+#define EPP_MOTION_ACCELERATE_MOVE  1 /* sAccelerateMove!: x += (u + du dt/2) dt, u += du dt (Motion.jl:61-75) */
 
 typedef struct epp_domain {
     int32_t dim;      /* 2 (Domain2D, src/Class/Domain/Domain2D.jl:28-67) or 3 (new) */
@@ -97,6 +116,15 @@ typedef struct epp_physics {
     int32_t fluid_tag;    /* 1 in the reference example */
     int32_t wall_tag;     /* 2 in the reference example */
     int32_t kahan;        /* 1: compensated (Kahan) position update; 0: sMove! as written */
+    /* Zero in each field below is the benchmark physics (Wendland C2, Tait, symplectic Euler, no
+     * filter); the reference example (example/collapse_dry/same/main.jl) is CUBIC_SPLINE, LINEAR,
+     * EPP_VISCOSITY_CLASSIC with mu = 1e-3, ACCELERATE_MOVE and filter_interval = 20. */
+    int32_t kernel;           /* EPP_KERNEL_* */
+    int32_t eos;              /* EPP_EOS_* */
+    float mu;                 /* dynamic viscosity of EPP_VISCOSITY_CLASSIC */
+    int32_t motion;           /* EPP_MOTION_* */
+    int32_t filter_interval;  /* epp_step: kernel filter after the search of every k-th step
+                               * (steps counted from 1 after epp_upload, main.jl:180-183); 0 = never */
 } epp_physics;
 
 typedef struct epp_config {

@@ -166,11 +166,62 @@ inline T wc2_gradient(T r, T hinv, int dim) {   // _gradient :38-49
     return T(0.0);
 }
 
+/* The other kernels of src/SPH/Kernel/: CubicSpline.jl, Gaussian.jl, WendlandC4.jl (sigma, _value,
+ * _gradient), and _value0 = sigma hinv^N (Kernel.jl:16-22). */
+template <typename T>
+inline T kern_sigma(int kind, int dim) {
+    switch (kind) {
+        case EPP_KERNEL_CUBIC_SPLINE: return dim == 2 ? T(10.0 / 7.0 / M_PI) : T(1.0 / M_PI);
+        case EPP_KERNEL_GAUSSIAN: return dim == 2 ? T(1.0 / M_PI) : T(1.0 / std::sqrt(M_PI * M_PI * M_PI));
+        case EPP_KERNEL_WENDLAND_C4: return dim == 2 ? T(9.0 / 4.0 / M_PI) : T(495.0 / 256.0 / M_PI);
+        default: return wc2_sigma<T>(dim);
+    }
+}
+template <typename T>
+inline T kern_value(int kind, T r, T hinv, int dim) {
+    T q = r * hinv;
+    switch (kind) {
+        case EPP_KERNEL_CUBIC_SPLINE:
+            if (q < T(1.0)) return kern_sigma<T>(kind, dim) * power<T>(hinv, dim) * (3 * q * q * (q - 2) + 4) * T(0.25);
+            if (q < T(2.0)) return kern_sigma<T>(kind, dim) * power<T>(hinv, dim) * power<T>(T(2) - q, 3) * T(0.25);
+            return T(0.0);
+        case EPP_KERNEL_GAUSSIAN:
+            return q < T(3.0) ? kern_sigma<T>(kind, dim) * power<T>(hinv, dim) * std::exp(-q * q) : T(0.0);
+        case EPP_KERNEL_WENDLAND_C4:
+            return q < T(2.0) ? kern_sigma<T>(kind, dim) * power<T>(hinv, dim) * power<T>(T(2) - q, 6) *
+                                    (q * (35 * q + 36) + 12) * T(0.0013020833333333333)
+                              : T(0.0);
+        default: return wc2_value<T>(r, hinv, dim);
+    }
+}
+template <typename T>
+inline T kern_gradient(int kind, T r, T hinv, int dim) {
+    T q = r * hinv;
+    switch (kind) {
+        case EPP_KERNEL_CUBIC_SPLINE:
+            if (q < T(1.0)) return kern_sigma<T>(kind, dim) * power<T>(hinv, dim + 1) * q * (3 * q - 4) * T(0.75);
+            if (q < T(2.0)) {
+                T to_2 = T(2) - q;
+                return -kern_sigma<T>(kind, dim) * power<T>(hinv, dim + 1) * to_2 * to_2 * T(0.75);
+            }
+            return T(0.0);
+        case EPP_KERNEL_GAUSSIAN:
+            return q < T(3.0) ? -2 * kern_sigma<T>(kind, dim) * power<T>(hinv, dim + 1) * q * std::exp(-q * q) : T(0.0);
+        case EPP_KERNEL_WENDLAND_C4:
+            return q < T(2.0) ? -kern_sigma<T>(kind, dim) * power<T>(hinv, dim + 1) * q *
+                                    (T(0.3645833333333333) * q + T(0.14583333333333334)) * power<T>(T(2) - q, 5)
+                              : T(0.0);
+        default: return wc2_gradient<T>(r, hinv, dim);
+    }
+}
+template <typename T>
+inline T kern_value0(int kind, T hinv, int dim) { return kern_sigma<T>(kind, dim) * power<T>(hinv, dim); }
+
 /* Physics constants converted to FT as `parallel(x)` does (src/Environment/Parallel.jl:62-74). */
 template <typename T>
 struct Phys {
-    T dt, rho0, c0, p0, B, g[3], alpha, beta, coef;
-    int gamma, visc, fluid, wall, kahan;
+    T dt, rho0, c0, p0, B, g[3], alpha, beta, coef, mu, c02;
+    int gamma, visc, fluid, wall, kahan, kernel, eos, motion, filter_interval;
 };
 template <typename T>
 Phys<T> make_phys(const epp_physics& p) {
@@ -190,13 +241,20 @@ Phys<T> make_phys(const epp_physics& p) {
     o.fluid = p.fluid_tag;
     o.wall = p.wall_tag;
     o.kahan = p.kahan;
+    o.kernel = p.kernel;
+    o.eos = p.eos;
+    o.mu = T(p.mu);
+    o.c02 = o.c0 * o.c0;   // main.jl:58 const c02 = c0 * c0
+    o.motion = p.motion;
+    o.filter_interval = p.filter_interval;
     return o;
 }
 
 /* Tait EOS (the benchmark cases replace the linear eos of main.jl:64):
- * p = B ((rho / rho0)^gamma - 1) + p0 */
+ * p = B ((rho / rho0)^gamma - 1) + p0; or the example's linear eos p = c0^2 (rho - rho0) + p0 */
 template <typename T>
 inline T eos(const Phys<T>& P, T rho) {
+    if (P.eos == EPP_EOS_LINEAR) return P.c02 * (rho - P.rho0) + P.p0;
     return P.B * (power<T>(rho / P.rho0, P.gamma) - T(1)) + P.p0;
 }
 
@@ -224,6 +282,8 @@ struct System : SysBase {
     /* float_properties_ columns */
     std::vector<T> pos, vel, dvel, comp, accel, accel_abs, drho_abs;
     std::vector<T> mass, vol, rho, drho, p, gapc, h;
+    std::vector<T> wv, wv_rho;   // kernel-filter sums (Filter.jl: SumWeight, SumWeightedDensity)
+    long long step_count = 0;    // steps since upload (main.jl:165 step += 1)
     std::vector<T> nw, ndw, nhinv, nr, nrvec;
     /* neighbour system */
     std::vector<int32_t> ccount, clist, nccount, nclist;
@@ -270,6 +330,7 @@ struct System : SysBase {
         drho_abs.assign(N, 0);
         mass.assign(N, 0); vol.assign(N, 0); rho.assign(N, 0); drho.assign(N, 0);
         p.assign(N, 0); gapc.assign(N, 0); h.assign(N, 0);
+        wv.assign(N, 0); wv_rho.assign(N, 0);
         nw.assign(N * max_nb, 0); ndw.assign(N * max_nb, 0); nhinv.assign(N * max_nb, 0);
         nr.assign(N * max_nb, 0); nrvec.assign(N * max_nb * D, 0);
         ccount.assign(dom.n_cells, 0);
@@ -407,8 +468,8 @@ struct System : SysBase {
             if (!(ff || fw || wf)) continue;
             T hinv = invharmonic<T>(h[I], h[J]);
             NH(ni, I) = hinv;
-            NW(ni, I) = wc2_value<T>(NR(ni, I), hinv, D);
-            NDW(ni, I) = wc2_gradient<T>(NR(ni, I), hinv, D);
+            NW(ni, I) = kern_value<T>(P.kernel, NR(ni, I), hinv, D);
+            NDW(ni, I) = kern_gradient<T>(P.kernel, NR(ni, I), hinv, D);
             T dw = NDW(ni, I);
             T term;
             if (ff) term = mass[J] * vdotx(I, ni, J) * dw / NR(ni, I);
@@ -422,7 +483,7 @@ struct System : SysBase {
     int interaction(int action, const Phys<T>& P) {
         if (!searched) return EPP_ERR_STATE;
         if (action != EPP_ACTION_DAMBREAK_MOMENTUM && action != EPP_ACTION_COUNT_NEIGHBOURS &&
-            action != EPP_ACTION_NONE)
+            action != EPP_ACTION_NONE && action != EPP_ACTION_KERNEL_FILTER)
             return EPP_ERR_UNSUPPORTED_ACTION;
 #pragma omp parallel for schedule(dynamic, 256)
         for (int I = 0; I < n; ++I) {
@@ -433,6 +494,14 @@ struct System : SysBase {
                     for (int a = 0; a < D; ++a) DU(a, I) += T(1.0);
                 } else if (action == EPP_ACTION_DAMBREAK_MOMENTUM) {
                     momentum_pair(I, ni, P);
+                } else if (action == EPP_ACTION_KERNEL_FILTER) {
+                    /* iFilter, main.jl:128-134: iKernelFilter! (Filter.jl:10-23) on fluid-fluid pairs
+                     * with the kernel value cached by the search */
+                    int J = NIDX(ni, I) - 1;
+                    if (tag[I] == P.fluid && tag[J] == P.fluid) {
+                        wv[I] += NW(ni, I) * vol[J];
+                        wv_rho[I] += NW(ni, I) * mass[J];
+                    }
                 }
             }
         }
@@ -458,6 +527,17 @@ struct System : SysBase {
             DU(a, I) += p_rho_2 * RV(ni, a, I);
             accel_abs[(size_t)a * n_cap + I] += std::fabs(p_rho_2 * RV(ni, a, I));
         }
+        if (P.visc == EPP_VISCOSITY_CLASSIC) {
+            /* iClassicViscosity!, Viscosity.jl:10-26 (the example's viscosity, main.jl:110,114) */
+            T hinv = NH(ni, I);
+            T hh = T(1) / hinv;
+            T force = 2 * P.mu * mass[J] * r * dw / (rho[I] * rho[J] * (r * r + T(0.01) * hh * hh));
+            for (int a = 0; a < D; ++a) {
+                DU(a, I) += force * (U(a, I) - U(a, J));
+                accel_abs[(size_t)a * n_cap + I] += std::fabs(force * (U(a, I) - U(a, J)));
+            }
+            return;
+        }
         /* sArtificialViscosity! */
         T v_dot_x = vdotx(I, ni, J);
         if (v_dot_x > 0) return;
@@ -479,13 +559,25 @@ struct System : SysBase {
     int selfaction(int action, const Phys<T>& P) {
         if (action == EPP_ACTION_NONE) return EPP_OK;
         if (action != EPP_ACTION_DAMBREAK_DENSITY && action != EPP_ACTION_DAMBREAK_INTEGRATE &&
-            action != EPP_ACTION_ZERO_DVELOCITY)
+            action != EPP_ACTION_ZERO_DVELOCITY && action != EPP_ACTION_KERNEL_FILTER_SELF)
             return EPP_ERR_UNSUPPORTED_ACTION;
 #pragma omp parallel for schedule(static)
         for (int I = 0; I < n; ++I) {
             if (alive[I] != 1) continue;
             if (action == EPP_ACTION_ZERO_DVELOCITY) {
                 for (int a = 0; a < D; ++a) DU(a, I) = T(0.0);
+            } else if (action == EPP_ACTION_KERNEL_FILTER_SELF) {
+                /* sFilter, main.jl:136-144: sKernelFilter! (Filter.jl:25-38), sVolume!, eos */
+                if (tag[I] == P.fluid) {
+                    T w0 = kern_value0<T>(P.kernel, T(1) / h[I], D);
+                    wv[I] += w0 * vol[I];
+                    wv_rho[I] += w0 * mass[I];
+                    rho[I] = wv_rho[I] / wv[I];
+                    wv[I] = T(0.0);
+                    wv_rho[I] = T(0.0);
+                    vol[I] = mass[I] / rho[I];
+                    p[I] = eos(P, rho[I]);
+                }
             } else if (action == EPP_ACTION_DAMBREAK_DENSITY) {
                 /* sContinuity! wrapper, main.jl:92-105: Continuity.jl:10-21, State.jl:10-19 */
                 if (tag[I] == P.fluid || tag[I] == P.wall) {
@@ -502,20 +594,29 @@ struct System : SysBase {
                         DU(a, I) += P.g[a];
                         accel_abs[(size_t)a * n_cap + I] += std::fabs(P.g[a]);
                     }
+                    T dx[3];
                     for (int a = 0; a < D; ++a) {
                         accel[(size_t)a * n_cap + I] = DU(a, I);
-                        U(a, I) += DU(a, I) * P.dt;
+                        if (P.motion == EPP_MOTION_ACCELERATE_MOVE) {
+                            /* sAccelerateMove!, Motion.jl:61-75: x += (u + du dt / 2) dt with the
+                             * old u, then u += du dt */
+                            dx[a] = (U(a, I) + DU(a, I) * P.dt * T(0.5)) * P.dt;
+                            U(a, I) += DU(a, I) * P.dt;
+                        } else {
+                            U(a, I) += DU(a, I) * P.dt;
+                            dx[a] = U(a, I) * P.dt;
+                        }
                         DU(a, I) = T(0.0);
                     }
                     for (int a = 0; a < D; ++a) {
                         if (P.kahan) {   // compensated summation (new; no reference counterpart)
                             T& c = comp[(size_t)a * n_cap + I];
-                            T y = U(a, I) * P.dt - c;
+                            T y = dx[a] - c;
                             T t = X(a, I) + y;
                             c = (t - X(a, I)) - y;
                             X(a, I) = t;
                         } else {
-                            X(a, I) += U(a, I) * P.dt;
+                            X(a, I) += dx[a];
                         }
                     }
                 }
@@ -538,10 +639,15 @@ struct System : SysBase {
     int step(int nsteps, const Phys<T>& P) {
         if (!searched) return EPP_ERR_STATE;
         for (int s = 0; s < nsteps; ++s) {
+            ++step_count;
             selfaction(EPP_ACTION_DAMBREAK_DENSITY, P);
             interaction(EPP_ACTION_DAMBREAK_MOMENTUM, P);
             selfaction(EPP_ACTION_DAMBREAK_INTEGRATE, P);
             search(EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, P);
+            if (P.filter_interval > 0 && step_count % P.filter_interval == 0) {   // main.jl:180-183
+                interaction(EPP_ACTION_KERNEL_FILTER, P);
+                selfaction(EPP_ACTION_KERNEL_FILTER_SELF, P);
+            }
         }
         return EPP_OK;
     }
@@ -597,6 +703,9 @@ int upload(System<T>* s, int32_t n, const int32_t* alive, const int32_t* cell, c
     }
     for (int I = n; I < s->n_cap; ++I) s->alive[I] = 0;
     s->searched = false;
+    s->step_count = 0;
+    std::fill(s->wv.begin(), s->wv.end(), T(0));       // filter sums start at zero (not uploaded)
+    std::fill(s->wv_rho.begin(), s->wv_rho.end(), T(0));
     return EPP_OK;
 }
 
@@ -662,8 +771,10 @@ int integrals(System<T>* s, const epp_physics* ph, epp_integrals* out) {
         ke += 0.5 * m * v2;
         pe += -m * gx;
         double r = (double)s->rho[I];
-        double e = (B / rho0) * (std::pow(r / rho0, gam - 1.0) / (gam - 1.0) + rho0 / r - gam / (gam - 1.0)) +
-                   p0 * (1.0 / rho0 - 1.0 / r);
+        double e = ph->eos == EPP_EOS_LINEAR
+                       ? c0 * c0 * (std::log(r / rho0) + rho0 / r - 1.0) + p0 * (1.0 / rho0 - 1.0 / r)
+                       : (B / rho0) * (std::pow(r / rho0, gam - 1.0) / (gam - 1.0) + rho0 / r - gam / (gam - 1.0)) +
+                             p0 * (1.0 / rho0 - 1.0 / r);
         ie += m * e;
         vmax = std::max(vmax, std::sqrt(v2));
         hmin = std::min(hmin, (double)s->h[I]);
@@ -757,6 +868,14 @@ int32_t orc_neighbour_cell_table(const epp_domain* d, int32_t* counts, int32_t* 
     neighbour_cells(d->dim, D.n, c, l);
     if (counts) std::copy(c.begin(), c.end(), counts);
     if (lists) std::copy(l.begin(), l.end(), lists);
+    return EPP_OK;
+}
+
+int32_t orc_kernel(int32_t kind, int32_t dim, double r, double hinv, double* w, double* dw) {
+    if ((dim != 2 && dim != 3) || kind < EPP_KERNEL_WENDLAND_C2 || kind > EPP_KERNEL_WENDLAND_C4 || !w || !dw)
+        return EPP_ERR_INVALID_ARGUMENT;
+    *w = kern_value<double>(kind, r, hinv, dim);
+    *dw = kern_gradient<double>(kind, r, hinv, dim);
     return EPP_OK;
 }
 
@@ -867,13 +986,15 @@ int32_t orc_search(orc_sys* s0, int32_t criterion, int32_t action, const epp_phy
 
 int32_t orc_interaction(orc_sys* s0, int32_t action, const epp_physics* phys) {
     SysBase* s = reinterpret_cast<SysBase*>(s0);
-    if (action == EPP_ACTION_DAMBREAK_MOMENTUM && !phys) return EPP_ERR_INVALID_ARGUMENT;
+    if ((action == EPP_ACTION_DAMBREAK_MOMENTUM || action == EPP_ACTION_KERNEL_FILTER) && !phys)
+        return EPP_ERR_INVALID_ARGUMENT;
     DISPATCH(s, S->interaction(action, P));
 }
 
 int32_t orc_selfaction(orc_sys* s0, int32_t action, const epp_physics* phys) {
     SysBase* s = reinterpret_cast<SysBase*>(s0);
-    if ((action == EPP_ACTION_DAMBREAK_DENSITY || action == EPP_ACTION_DAMBREAK_INTEGRATE) && !phys)
+    if ((action == EPP_ACTION_DAMBREAK_DENSITY || action == EPP_ACTION_DAMBREAK_INTEGRATE ||
+         action == EPP_ACTION_KERNEL_FILTER_SELF) && !phys)
         return EPP_ERR_INVALID_ARGUMENT;
     DISPATCH(s, S->selfaction(action, P));
 }

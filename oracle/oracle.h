@@ -48,6 +48,8 @@ int32_t orc_cell_of(const epp_domain* d, int32_t precision, const float* x, int3
 /* counts[n_cells]; lists[n_cells * 3^dim] (row per cell, 1-based cell ids) or NULL */
 int32_t orc_neighbour_cell_table(const epp_domain* d, int32_t* counts, int32_t* lists);
 
+/* Kernel value W and gradient dW/dr of EPP_KERNEL_* `kind` in `dim` dimensions (FP64). */
+int32_t orc_kernel(int32_t kind, int32_t dim, double r, double hinv, double* w, double* dw);
 orc_sys* orc_create(int32_t precision, const epp_config* cfg);
 void orc_destroy(orc_sys* s);
 int32_t orc_set_threads(int32_t n);

@@ -43,6 +43,8 @@ def load():
     lib.orc_domain_info.argtypes = [P(abi.epp_domain), C.c_int32, i32p, f64p, f64p]
     lib.orc_cell_of.argtypes = [P(abi.epp_domain), C.c_int32, f32p, i32p, i32p, i32p]
     lib.orc_neighbour_cell_table.argtypes = [P(abi.epp_domain), i32p, i32p]
+    lib.orc_kernel.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, f64p, f64p]
+    lib.orc_kernel.restype = C.c_int32
     lib.orc_create.restype = C.c_void_p
     lib.orc_create.argtypes = [C.c_int32, P(abi.epp_config)]
     lib.orc_destroy.argtypes = [C.c_void_p]
@@ -148,3 +150,13 @@ class Oracle:
 
 def set_threads(n):
     load().orc_set_threads(n)
+
+
+def kernel(kind, dim, r, hinv):
+    """(W, dW/dr) of the oracle's kernel `kind` (FP64)."""
+    lib = load()
+    w, dw = C.c_double(0), C.c_double(0)
+    rc = lib.orc_kernel(kind, dim, r, hinv, C.byref(w), C.byref(dw))
+    if rc:
+        raise RuntimeError("orc_kernel %d" % rc)
+    return w.value, dw.value
