@@ -94,7 +94,6 @@ struct epp_ctx {
     double* ipartial = nullptr;
     double* iresult = nullptr;
     unsigned* iticket = nullptr;
-    double* ihmin = nullptr;
     float4* accel = nullptr;   // optional dv/dt output of the fused momentum pass
     // lazily allocated neighbour lists (EPP_SEARCH_EMIT_LIST)
     NeighbourList L{};
@@ -175,7 +174,7 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += (size_t)cap * 4 + 256;                          // ncount
     b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
-    b += (size_t)kIntegralBlocks * 8 * 7 + 8 * 8 + 4 * 256;
+    b += (size_t)kIntegralBlocks * 8 * 8 + 8 * 8 + 4 * 256;
     b += 2 * ((size_t)cap * 4 + 256);                    // kernel-filter sums
     b += 2 * 256;                                                                  // instance tables (small)
     return b + (1 << 20);
@@ -860,10 +859,9 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->ncount = a.take<int>(ctx->cap);
     ctx->stage_f = a.take<float>((size_t)ctx->cap * (3 * D + 6));
     ctx->stage_i = a.take<int>((size_t)ctx->cap * SI_COUNT);
-    ctx->ipartial = a.take<double>(kIntegralBlocks * 7);
+    ctx->ipartial = a.take<double>(kIntegralBlocks * 8);
     ctx->iresult = a.take<double>(8);
     ctx->iticket = a.take<unsigned>(1);
-    ctx->ihmin = a.take<double>(1);
     ctx->fwv = a.take<float>(ctx->cap);
     ctx->fwr = a.take<float>(ctx->cap);
     ctx->tmp.count = ctx->count;
@@ -871,7 +869,7 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->tmp.scan_state = ctx->scan_state;
     ctx->tmp.n_scan_words = ctx->n_tiles + 1;
     ctx->tmp.accel = nullptr;
-    if (!ctx->ihmin) {
+    if (!ctx->fwr) {   // the last part taken: the arena held everything
         epp_destroy(ctx);
         return EPP_ERR_OUT_OF_MEMORY;
     }
@@ -1193,12 +1191,13 @@ int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* 
     std::memset(out, 0, sizeof *out);
     if (ctx->n == 0) return EPP_OK;
     if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
-    IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket, ctx->ihmin};
+    IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket};
     DevPhys P = dev_phys(ctx, *phys);
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;
         k_integrals<DD><<<kIntegralBlocks, 256, 0, ctx->stream>>>(
-            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], P, phys->rho0, phys->c0, phys->gamma, phys->p0,
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], ctx->ncount, P, phys->rho0, phys->c0,
+            phys->gamma, phys->p0,
             phys->gravity[0], phys->gravity[1], phys->gravity[2], O);
     };
     if (ctx->D == 2) launch(std::integral_constant<int, 2>{});
@@ -1206,11 +1205,9 @@ int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* 
     CK_LAUNCH();
     double r[8];
     int n_alive = 0;
-    CK(cudaMemcpyAsync(r, ctx->iresult, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(&r[6], ctx->ihmin, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(r, ctx->iresult, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(&n_alive, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
                        ctx->stream));
-    std::vector<int> nc;
     CK(cudaStreamSynchronize(ctx->stream));
     out->mass_total = r[0];
     out->mass_fluid = r[1];
@@ -1220,14 +1217,7 @@ int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* 
     out->max_speed = r[5];
     out->cfl_dt = r[6] < 1e300 ? 0.1 * r[6] / ((double)phys->c0 + r[5]) : 0.0;
     out->n_alive = n_alive;
-    // directed pairs of the last search = sum of nCount over alive particles
-    nc.resize(n_alive);
-    if (n_alive > 0) {
-        CK(cudaMemcpy(nc.data(), ctx->ncount, sizeof(int) * n_alive, cudaMemcpyDeviceToHost));
-        long long s = 0;
-        for (int v : nc) s += v;
-        out->n_pairs = s;
-    }
+    out->n_pairs = (int64_t)r[7];   // directed pairs of the last search = sum of nCount over alive particles
     return EPP_OK;
 }
 

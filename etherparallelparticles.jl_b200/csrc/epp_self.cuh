@@ -130,10 +130,10 @@ struct MoverFused {
 
 // FP64 integrals: per-block partials, the last block folds them in block order (deterministic).
 struct IntegralsOut {
-    double* partial;       // [n_blocks * 7]: the 6 results and min h of each block
-    double* result;        // [6]: mass_total, mass_fluid, kinetic, potential, internal, max|v|
+    double* partial;       // [n_blocks * 8]: the 6 results, min h and the pair count of each block
+    double* result;        // [8]: mass_total, mass_fluid, kinetic, potential, internal, max|v|, min h,
+                           //      directed pairs of the last search (sum of nCount, exact in FP64)
     unsigned* ticket;
-    double* hmin;          // [1]
 };
 
 // x^n for an integer n >= 0 in FP64 (binary exponentiation; the Tait exponent is an integer).
@@ -159,19 +159,20 @@ __device__ __forceinline__ double eos_energy(int eos_kind, double r, double rho0
 
 template <int D>
 __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells, int n_max, State s,
-                                                   DevPhys P, double rho0, double c0,
+                                                   const int* ncount, DevPhys P, double rho0, double c0,
                                                    int gam, double p0, double g0, double g1,
                                                    double g2, IntegralsOut O) {
-    __shared__ double sh[7][256 / 32];
+    __shared__ double sh[8][256 / 32];
     __shared__ bool last;
     const int n_alive = min(start[n_cells], n_max);
     const double B = rho0 * c0 * c0 / (double)gam;
-    // v: mass, fluid mass, kinetic, potential, internal, max |v| (max), min h (min)
-    double v[7] = {0, 0, 0, 0, 0, 0, 1e300};
+    // v: mass, fluid mass, kinetic, potential, internal, max |v| (max), min h (min), pairs
+    double v[8] = {0, 0, 0, 0, 0, 0, 1e300, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_alive; i += gridDim.x * blockDim.x) {
         const float4 vm = s.vm[i];
         const double m = (double)vm.w;
         v[0] += m;
+        v[7] += (double)ncount[i];
         if (tag_of(s.tagm[i]) != P.fluid) continue;
         const float4 xh = s.xh[i];
         v[1] += m;
@@ -184,15 +185,15 @@ __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     auto combine = [](int k, double a, double b) { return k == 5 ? fmax(a, b) : k == 6 ? fmin(a, b) : a + b; };
-    auto block_reduce = [&](double (&x)[7]) {   // fixed tree: deterministic
+    auto block_reduce = [&](double (&x)[8]) {   // fixed tree: deterministic
 #pragma unroll
-        for (int k = 0; k < 7; ++k) {
+        for (int k = 0; k < 8; ++k) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) x[k] = combine(k, x[k], __shfl_down_sync(0xffffffffu, x[k], o));
             if (lane == 0) sh[k][warp] = x[k];
         }
         __syncthreads();
-        if (threadIdx.x < 7) {
+        if (threadIdx.x < 8) {
             const int k = threadIdx.x;
             double a = sh[k][0];
             for (int w = 1; w < 256 / 32; ++w) a = combine(k, a, sh[k][w]);
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells
         }
     };
     block_reduce(v);
-    if (threadIdx.x < 7) O.partial[blockIdx.x * 7 + threadIdx.x] = v[threadIdx.x];
+    if (threadIdx.x < 8) O.partial[blockIdx.x * 8 + threadIdx.x] = v[threadIdx.x];
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = atomicAdd(O.ticket, 1u) == gridDim.x - 1;
@@ -208,13 +209,12 @@ __global__ void __launch_bounds__(256) k_integrals(const int* start, int n_cells
     if (!last) return;
     __threadfence();
     // the last block combines the partials: thread t takes blocks t, t + 256, ... in order
-    double w[7] = {0, 0, 0, 0, 0, 0, 1e300};
+    double w[8] = {0, 0, 0, 0, 0, 0, 1e300, 0};
     for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
 #pragma unroll
-        for (int k = 0; k < 7; ++k) w[k] = combine(k, w[k], __ldcg(&O.partial[b * 7 + k]));
+        for (int k = 0; k < 8; ++k) w[k] = combine(k, w[k], __ldcg(&O.partial[b * 8 + k]));
     block_reduce(w);
-    if (threadIdx.x < 6) O.result[threadIdx.x] = w[threadIdx.x];
-    if (threadIdx.x == 6) O.hmin[0] = w[6];
+    if (threadIdx.x < 8) O.result[threadIdx.x] = w[threadIdx.x];
     if (threadIdx.x == 0) *O.ticket = 0;
 }
 

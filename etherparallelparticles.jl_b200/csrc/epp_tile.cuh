@@ -180,7 +180,7 @@ struct ListReader {
 // Candidate ranges (contiguous particle index ranges) of a warp tile or of one particle.
 template <int D>
 struct TileRanges {
-    int lo[TileConf<D>::NRMAX], len[TileConf<D>::NRMAX];
+    int lo[TileConf<D>::NRMAX], len[TileConf<D>::NRMAX], cum[TileConf<D>::NRMAX];   // cum: first candidate index
     int n, total;
 
     __device__ __forceinline__ void add(const PairArgs& A, int row, int xa, int xb) {
@@ -196,6 +196,7 @@ struct TileRanges {
         }
         lo[n] = l;
         len[n] = h - l;
+        cum[n] = total;
         total += h - l;
         ++n;
     }
@@ -213,15 +214,14 @@ struct TileRanges {
             }
         }
     }
-    // candidate index k (0 <= k < total) -> particle index
+    // candidate index k (0 <= k < total) -> particle index: the last range starting at or before k
+    // holds it (empty ranges share their successor's start, which comes after them)
     __device__ __forceinline__ int at(int k) const {
-        int j = 0;
+        int b = lo[0];
 #pragma unroll
-        for (int r = 0; r < TileConf<D>::NRMAX; ++r) {
-            if (r < n && k >= 0 && k < len[r]) j = lo[r] + k;
-            k -= r < n ? len[r] : 0;
-        }
-        return j;
+        for (int r = 1; r < TileConf<D>::NRMAX; ++r)
+            if (r < n && k >= cum[r]) b = lo[r] - cum[r];
+        return k + b;
     }
 };
 
