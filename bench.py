@@ -544,297 +544,6 @@ def run_serve(args):
     print(json.dumps(out))
 
 
-def run_reference_serve(args):
-    """--impl reference --case serve: the oracle serves requests one at a time (the reference has
-    no serving form); sims/s from a sample of the stream's requests timed for a few steps each."""
-    from epp import serve
-    specs = serve.request_stream(args.requests, seed=0, steps=args.sim_steps)
-    sample = specs[:: max(1, len(specs) // 6)]
-    total, cores = 0.0, 1
-    for s in sample:
-        case = s.case()
-        case.meta["label"] = "request %d" % s.rid
-        res = cpu_reference(case, steps_budget_s=2.0, max_steps=5)
-        total += res["seconds_per_step"] * s.steps
-        cores = res["cores"]
-    val = len(sample) / total
-    out = {"metric": "served sims/s (Poisson request stream, %d steps per simulation)" % args.sim_steps,
-           "value": val, "unit": "sims/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.sim_steps,
-           "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32", "data": "synthetic request stream (numpy default_rng(0))",
-           "config": {"workload": "%d requests" % args.requests},
-           "cpu_baseline": {"value": val, "unit": "sims/s", "cores": cores, "kind": "port",
-                            "sample": "requests %s, up to 5 steps each, one at a time" % [s.rid for s in sample]},
-           "e2e": {"value": val, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out))
-
-
-def energy(ig):
-    return ig["kinetic"] + ig["potential"] + ig["internal"]
-
-
-def run_batch(args):
-    """--case batch: the 256-instance mix of uneven 2D dam breaks (column width U[0.5, 1.5] m,
-    height U[1.0, 2.5] m, seed 0, dx = 0.01 m, each instance with its own c0 and dt), every pass
-    one launch over all instances.  value = sims/s at 2000 steps per simulation, against the
-    plain path running the same instances one at a time (each timed alone on the device)."""
-    import torch
-    import torch.distributed as dist
-    from epp import abi, casegen
-    from epp.algorithm import DeviceParticleSystem
-    from epp.classes import NeighbourSystem
-    import oracle_lib
-    from helpers import config_for
-
-    SIM_STEPS = 2000
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
-    torch.cuda.set_device(local)
-    SYM, CONT = abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY
-    b = casegen.dam_break_batch(args.instances, seed=0, dx=0.01)
-    phys = b.physics
-    ns = NeighbourSystem(b.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
-    from epp import autotune
-    tuned, tune_ms = autotune.tune_case(b, n_instances=b.n_instances, inst=(b.inst_dt, b.inst_c0), steps=5,
-                                        device=local)
-    dps = DeviceParticleSystem(b.ps, ns, device=local, n_instances=b.n_instances)
-    ctx = dps.ctx
-    ctx.set_instance_physics(b.inst_dt, b.inst_c0)
-    ctx.set_block_threads(tuned[1])
-    stream = torch.cuda.Stream()
-    ctx.set_stream(stream.cuda_stream)
-    dps.syncto()
-    ctx.search(SYM, CONT, phys, 0)
-    e0 = [energy(x) for x in ctx.instance_integrals(phys, b.n_instances)]
-    W = max(args.warmup, 3)
-    with torch.cuda.stream(stream):
-        ctx.step(W, phys)
-    ctx.synchronize()
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    clocks = Clocks(local)
-    p0 = ctx.pairs_total()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            starts[k].record(stream)
-            ctx.step(1, phys)
-            ends[k].record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    st = ctx.synchronize(raise_on_status=False)
-    ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
-    pairs = ctx.pairs_total() - p0
-    e1 = [energy(x) for x in ctx.instance_integrals(phys, b.n_instances)]
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t[0])
-    step_ms = ms / args.steps
-    sims_s = world * b.n_instances / (SIM_STEPS * step_ms * 1e-3)
-    with torch.cuda.stream(stream):
-        stage = np.mean([ctx.profile_step(phys) for _ in range(3)], axis=0)
-    # end to end through the C ABI with pinned host buffers (upload, search, K x (step +
-    # per-instance integrals read back), download)
-    h = dps.host
-    ip = np.asfortranarray(torch.from_numpy(np.asfortranarray(h.int_properties)).pin_memory().numpy())
-    fp = np.asfortranarray(torch.from_numpy(np.asfortranarray(h.float_properties)).pin_memory().numpy())
-    alive = torch.from_numpy(h.is_alive.copy()).pin_memory().numpy()
-    cell = torch.from_numpy(h.cell_index.copy()).pin_memory().numpy()
-    ctx.download(alive, cell, ip, fp, dps.cmap)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ctx.upload(h.n_particles, alive, cell, ip, fp, dps.cmap)
-    ctx.search(SYM, CONT, phys, 0)
-    for _ in range(args.steps):
-        ctx.step(1, phys)
-        ctx.instance_integrals(phys, b.n_instances)
-    ctx.download(alive, cell, ip, fp, dps.cmap)
-    t_e2e = time.perf_counter() - t0
-    n_cols = 2 * 3 + 6 + 5   # float columns moved (x, v, dv, m, V, rho, drho, p, h) + int (tag, mov, ncount, alive, cell, instance)
-    bytes_io = h.n_particles * 4 * (n_cols + 1)
-    dps.close()
-    out = None
-    if rank == 0:
-        # plain path: every instance alone, one after the other, on one context sized for the
-        # largest (the state of one instance stays resident in L2 between its own steps)
-        K2 = 20
-        cases = [casegen.dam_break_2d(dx=0.01, column=col, max_neighbour_number=1) for col in b.meta["columns"]]
-        big = max(cases, key=lambda c: c.n)
-        ns1 = NeighbourSystem(big.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
-        plain = DeviceParticleSystem(big.ps, ns1, device=local)
-        pctx = plain.ctx
-        pctx.set_stream(stream.cuda_stream)
-        per_step = []
-        for c in cases:
-            q = c.ps
-            pctx.upload(q.n_particles, q.is_alive, q.cell_index, q.int_properties, q.float_properties, plain.cmap)
-            pctx.search(SYM, CONT, c.physics, 0)
-            with torch.cuda.stream(stream):
-                pctx.step(3, c.physics)
-            torch.cuda.synchronize()
-            a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(stream):
-                a_.record(stream)
-                pctx.step(K2, c.physics)
-                b_.record(stream)
-            torch.cuda.synchronize()
-            per_step.append(a_.elapsed_time(b_) / K2)
-        plain.close()
-        plain_sims_s = len(cases) / (SIM_STEPS * sum(per_step) * 1e-3)
-        # energy drift against the FP64 oracle for sampled instances (the smallest three and the
-        # largest), same number of steps from the same initial state
-        S = W + args.steps
-        order = sorted(range(len(cases)), key=lambda k: cases[k].n)
-        sample = order[:3] + order[-1:]
-        drift = {}
-        oracle_lib.set_threads(os.cpu_count() or 1)
-        for k in sample:
-            c = casegen.dam_break_2d(dx=0.01, column=b.meta["columns"][k], max_neighbour_number=60)
-            nso = NeighbourSystem(c.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=60)
-            o = oracle_lib.Oracle(config_for(c.ps, nso, max_cell_particles=64), 64)
-            q = c.ps
-            o.upload(q.n_particles, q.is_alive, q.cell_index, q.int_properties, q.float_properties, q.column_map())
-            o.search(SYM, CONT, c.physics)
-            o0 = energy(o.integrals(c.physics))
-            o.step(S, c.physics)
-            o1 = energy(o.integrals(c.physics))
-            dg, do = (e1[k] - e0[k]) / abs(e0[k]), (o1 - o0) / abs(o0)
-            drift[str(k)] = {"particles": c.n, "gpu_fp32": dg, "oracle_fp64": do, "abs_diff": abs(dg - do)}
-        peaks = {}
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                peaks = json.load(f)
-        except Exception:
-            pass
-        out = {
-            "metric": "batched sims/s (256-instance 2D dam-break mix, 2000 steps per simulation)",
-            "value": sims_s, "unit": "sims/s", "n_gpus": world, "steps": args.steps, "warmup": W,
-            "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded column sizes, numpy default_rng(0))",
-            "config": {"workload": "%d uneven 2D dam breaks, width U[0.5,1.5] m, height U[1.0,2.5] m, dx=0.01 m"
-                       % b.n_instances, "instances": b.n_instances, "particles": b.n,
-                       "fluid": b.meta["n_fluid"], "walls": b.meta["n_wall"],
-                       "fluid_per_instance": [min(b.meta["inst_n_fluid"]), max(b.meta["inst_n_fluid"])],
-                       "cells": b.meta["n_cells"], "resort": "every step",
-                       "l2": "flushed (256 MB write) before every timed step",
-                       "parallelism": "instances per GPU, replicas across GPUs" if world > 1 else "single GPU"},
-            "plain_path": {"sims_per_s": plain_sims_s, "ms_per_instance_step_mean": float(np.mean(per_step)),
-                           "ms_per_instance_step_range": [float(min(per_step)), float(max(per_step))],
-                           "method": "each instance alone on the plain path (epp_step graph), %d steps "
-                                     "timed per instance by CUDA events, summed over the %d instances"
-                                     % (K2, len(cases))},
-            "speedup_vs_plain": sims_s / world / plain_sims_s,
-            "autotune": {"family": tuned[0], "block_threads": tuned[1], "resort_every": 1,
-                         "ms_per_step": {"%d/%d" % k: round(v, 4) for k, v in tune_ms.items()}},
-            "pairs_per_s": pairs / (ms * 1e-3) if world == 1 else None,
-            "energy_drift": {"steps": S, "bar": 1e-4, "instances": drift,
-                             "max_abs_diff": max(v["abs_diff"] for v in drift.values())},
-            "gpu_launches": 6 * args.steps,
-            "roofline": {"bound": "hbm", "stage_ms": dict(zip(STAGES, [round(float(x), 4) for x in stage])),
-                         "achieved": B_ALG_STEP[2] * b.n / (step_ms * 1e-3) / 1e9,
-                         "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
-                         "frac": B_ALG_STEP[2] * b.n / (step_ms * 1e-3) / 1e9 / peaks.get("hbm_gbs", 6650.0),
-                         "traffic": None, "note": "whole step, algorithmic bytes; pair kernels are issue/latency bound"},
-            "clocks": clk,
-            "e2e": {"value": b.n_instances * args.steps / SIM_STEPS / t_e2e, "unit": "sims/s",
-                    "h2d_bytes_per_step": int(bytes_io / args.steps), "d2h_bytes_per_step": int(bytes_io / args.steps + 72 * b.n_instances),
-                    "seconds": t_e2e,
-                    "note": "upload + search + K x (step + per-instance integrals read back) + download, host clock"},
-            "device_status": st,
-        }
-        print(json.dumps(out))
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-
-
-def run_serve(args):
-    """--case serve: the seeded request stream (Poisson arrivals, mean 50 / s; 70% 2D, 30% 3D; fluid
-    counts log-uniform in 1e3 - 1e6; 2000 steps each) served under a 120 GB HBM budget with
-    continuous batching, against the same trace served one request at a time on the plain path.
-    value = completed simulations / makespan (arrival of the first request to completion of the
-    last), latency = completion - arrival, both on the host clock; every request is uploaded,
-    searched, stepped and read back (FP64 integrals) inside the measured time."""
-    # more hardware queues than the default 8, so up to 32 resident runs get their own (set
-    # before the first CUDA call of the process)
-    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
-    import torch
-    from epp import serve
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if args.mix == "batch":
-        specs = serve.batch_mix_requests(args.instances, steps=args.sim_steps)
-    else:
-        specs = serve.request_stream(args.requests, seed=0, steps=args.sim_steps)
-    from epp import autotune
-    tuner = autotune.Autotuner(device=local, steps=10)
-    be = serve.DeviceBackend(device=local, tuner=tuner if args.autotune else None)
-    # launch configuration per (dimension, size bucket) of the trace, tuned before the clock starts
-    tuned = {}
-    if args.autotune:
-        for s_ in specs:
-            c = s_.case()
-            k = autotune.TuneCache.key(tuner.gpu, c.meta["dim"], c.n, False)
-            if k not in tuned:
-                tuned[k] = tuner.best(c.meta["dim"], c.n, case=c)
-    # warm-up: one small request of each dimension (module load, first graph build)
-    warm = [s for s in serve.request_stream(16, seed=99, n_range=(1e3, 3e3), steps=10)]
-    warm = [next(s for s in warm if s.dim == 2), next(s for s in warm if s.dim == 3)]
-    for s in warm:
-        s.arrival = 0.0
-    serve.Server(be).run(serve.make_runs(warm, be))
-    runs = serve.make_runs(specs, be)
-    clocks = Clocks(local)
-    clocks.start()
-    st = serve.Server(be, budget_bytes=120 * 10**9).run(runs)
-    clk = clocks.stop()
-    plain_runs = serve.make_runs(specs, be)
-    plain = serve.Server(be, budget_bytes=120 * 10**9, max_active=1).run(plain_runs)
-    n_p = [r.case.n for r in runs]
-    h2d = sum(n * 4 * 18 for n in n_p)
-    if rank == 0:
-        if args.mix == "batch":
-            workload = ("the batched form's %d-instance 2D mix as requests arriving at once (width U[0.5,1.5] m, "
-                        "height U[1.0,2.5] m, dx=0.01 m)" % len(specs))
-        else:
-            workload = ("%d requests, Poisson mean 50/s, 70%% 2D / 30%% 3D, fluid log-uniform 1e3-1e6, "
-                        "aspect U[0.5,2.5]" % len(specs))
-        out = {"metric": "served sims/s (%s, %d steps per simulation)"
-                         % ("256-instance mix" if args.mix == "batch" else "Poisson request stream", args.sim_steps),
-               "value": st["sims_per_s"], "unit": "sims/s", "n_gpus": 1, "steps": args.sim_steps,
-               "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f32",
-               "data": "synthetic request stream (numpy default_rng(0)): arrivals, sizes and aspects seeded",
-               "config": {"workload": workload, "requests": len(specs), "stream_priorities": "by size",
-                          "requests_2d": sum(1 for s in specs if s.dim == 2),
-                          "requests_3d": sum(1 for s in specs if s.dim == 3),
-                          "particles_total": int(sum(n_p)), "particles_range": [min(n_p), max(n_p)],
-                          "hbm_budget_bytes": 120 * 10**9, "chunk_steps": 100, "parallelism": "single GPU"},
-               "latency_p50_s": st["latency_p50_s"], "latency_p99_s": st["latency_p99_s"],
-               "served": st,
-               "plain_path": dict(plain, method="same trace, one request at a time (max_active = 1), same kernels"),
-               "speedup_vs_plain": st["sims_per_s"] / plain["sims_per_s"],
-               "autotune": {k: {"family": v[0], "block_threads": v[1]} for k, v in tuned.items()},
-               "p99_vs_plain": st["latency_p99_s"] / plain["latency_p99_s"],
-               "gpu_launches": 6 * args.sim_steps * len(specs),
-               "clocks": clk,
-               "e2e": {"value": st["sims_per_s"], "unit": "sims/s", "h2d_bytes_per_step": int(h2d / args.sim_steps / len(specs)),
-                       "d2h_bytes_per_step": 0,
-                       "note": "serving is end to end: each request's upload, search, steps and integrals read-back "
-                               "are inside the makespan"}}
-        print(json.dumps(out))
-
-
 def main():
     args = parse()
     if args.impl == "reference":
@@ -926,13 +635,15 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
+    tr_case = {}
     try:   # DRAM bytes of one launch of that kernel from an ncu capture of the same workload
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            tr = json.load(f).get(args.case, {}).get(dom_stage)
-            if tr:
-                traffic = tr["bytes_per_launch"]
+            tr_case = json.load(f).get(args.case, {})
+            if tr_case.get(dom_stage):
+                traffic = tr_case[dom_stage]["bytes_per_launch"]
     except Exception:
         pass
+    fp32_peak = fp32_peak_tflops(stream)
 
     # ---- end to end through the C ABI with host buffers (pinned) ----
     e2e = run_e2e(dps, case, args, stream)
@@ -970,6 +681,8 @@ def main():
                          "algorithmic_bytes_per_particle": B_ALG_STAGE[dom_stage][dim],
                          "kernel_ms": round(dom_ms, 5),
                          "stage_ms": dict(zip(STAGES, [round(x, 5) for x in stage])),
+                         "frac_of_nominal_8tbs": achieved / 8000.0,
+                         "compute": compute_roof(tr_case, stage, fp32_peak, clk),
                          "note": "pair kernels are issue/latency bound, not HBM bound (ncu summaries in profiles/)"},
             "clocks": clk,
             "e2e": e2e,
@@ -991,6 +704,56 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp32_peak_tflops(stream):
+    """FP32 (non-tensor) roof measured here: cuBLAS SGEMM 8192^3 with TF32 off, best of 5, CUDA
+    events on `stream`."""
+    import torch
+    prev = torch.get_float32_matmul_precision()
+    torch.set_float32_matmul_precision("highest")
+    try:
+        n = 8192
+        with torch.cuda.stream(stream):
+            a = torch.randn(n, n, device="cuda")
+            b = torch.randn(n, n, device="cuda")
+            c = torch.empty(n, n, device="cuda")
+            for _ in range(2):
+                torch.matmul(a, b, out=c)
+            best = float("inf")
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                torch.matmul(a, b, out=c)
+                e1.record(stream)
+                e1.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+        del a, b, c
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.set_float32_matmul_precision(prev)
+
+
+def compute_roof(tr_case, stage, fp32_peak, clk):
+    """Second roof of the three pair kernels: FP32 flops and warp instructions per launch (ncu
+    instruction-mix capture of the same workload) over this run's kernel times, against the
+    measured SGEMM FP32 rate and the issue rate 148 SMs x 4 schedulers x the sampled SM clock."""
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    issue_peak = 148 * 4 * mhz * 1e6
+    out = {"fp32_peak_tflops": fp32_peak, "fp32_peak_source": "cuBLAS SGEMM 8192^3, TF32 off (of measured)",
+           "issue_peak_warp_inst_per_s": issue_peak, "issue_clock_mhz": mhz, "stages": {}}
+    for st in B_ALG_STAGE:
+        e = tr_case.get(st) or {}
+        ms = float(stage[STAGES.index(st)])
+        if "flops_per_launch" not in e or ms <= 0:
+            continue
+        tf = e["flops_per_launch"] / (ms * 1e-3) / 1e12
+        out["stages"][st] = {"kernel": KERNEL_OF_STAGE[st], "kernel_ms": round(ms, 5),
+                             "flops_per_launch": e["flops_per_launch"], "achieved_tflops": tf,
+                             "fp32_frac": tf / fp32_peak,
+                             "warp_inst_per_launch": e["warp_inst_per_launch"],
+                             "issue_frac": e["warp_inst_per_launch"] / (ms * 1e-3) / issue_peak}
+    return out
 
 
 def run_e2e(dps, case, args, stream):

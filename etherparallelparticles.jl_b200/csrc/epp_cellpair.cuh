@@ -33,33 +33,26 @@ struct TargetConst {   // per target: h, invharmonic(h,h), dW/r factor, 1/hinv, 
     float h2sq;
 };
 
-// Kernel constants of the last neighbour h_j != h_i (a handful of distinct h values occur, so
-// the IEEE division of invharmonic runs once per change instead of once per pair).
-struct HPairCache {
-    float hj, hinv, kdw, hh;
-};
-
+// Kernel constants of a pair with h_j != h_i: the IEEE division of invharmonic, out of line.
+// Equal h (every pair of a uniform-h case) takes the target's cached constants instead.
 template <int D>
-__device__ __noinline__ void hpair_fill(HPairCache& c, float hi, float hj) {
-    c.hj = hj;
-    c.hinv = invharmonic_exact(hi, hj);
-    c.kdw = wc2_kdw<D>(c.hinv);
-    c.hh = __fdividef(1.0f, c.hinv);
+__device__ __noinline__ float4 hpair_consts(float hi, float hj) {
+    const float hinv = invharmonic_exact(hi, hj);
+    return make_float4(hinv, wc2_kdw<D>(hinv), __fdividef(1.0f, hinv), 0.0f);
 }
 
 template <int D>
-__device__ __forceinline__ void pair_consts(const TargetConst& tc, HPairCache& pc, float hj, float& hinv,
-                                            float& kdw, float& hh) {
+__device__ __forceinline__ void pair_consts(const TargetConst& tc, float hj, float& hinv, float& kdw, float& hh) {
     if (hj == tc.h) {
         hinv = tc.hinv;
         kdw = tc.kdw;
         hh = tc.hh;
         return;
     }
-    if (hj != pc.hj) hpair_fill<D>(pc, tc.h, hj);
-    hinv = pc.hinv;
-    kdw = pc.kdw;
-    hh = pc.hh;
+    const float4 c = hpair_consts<D>(tc.h, hj);
+    hinv = c.x;
+    kdw = c.y;
+    hh = c.z;
 }
 
 // (dW/dr) / r of a pair: the cached Wendland C2 closed form, or (GEN) the selected kernel's; 0
@@ -123,7 +116,7 @@ struct CPCont {
     __device__ __forceinline__ Self self(int i) const { return Self{s.vm[i], s.rho[i]}; }
     __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{s.vm[j], s.vol[j]}; }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
-                                           const PairGeo& g, const TargetConst& tc, HPairCache& pc) const {
+                                           const PairGeo& g, const TargetConst& tc) const {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const bool ff = ti == P.fluid && tj == P.fluid;
         const bool fw = ti == P.fluid && tj == P.wall;
@@ -131,7 +124,7 @@ struct CPCont {
         if (!(ff || fw || wf)) return out;
         const float r = sqrtf(g.dr2);
         float hinv, kdw, hh;
-        pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
+        pair_consts<D>(tc, xj.w, hinv, kdw, hh);
         const float dwr = pair_dwr<D, GEN>(P.kernel, r * hinv, hinv, kdw);
         if (dwr == 0.0f) return out;
         float vdx = g.dx * (me.v.x - nb.v.x);
@@ -143,8 +136,7 @@ struct CPCont {
     }
     __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
                                               const PairGeo& g, const TargetConst& tc) const {
-        HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
-        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc, pc);
+        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc);
     }
     __device__ __forceinline__ void end(int i, int ti, float4 sum, int cnt) const {
         ncount[i] = cnt;
@@ -172,7 +164,7 @@ struct CPCount {
     __device__ __forceinline__ Self self(int) const { return Self{}; }
     __device__ __forceinline__ Nb fetch(int, int, int) const { return Nb{}; }
     __device__ __forceinline__ float4 term(const Self&, const Nb&, int, int, float4, const PairGeo&,
-                                           const TargetConst&, HPairCache&) const {
+                                           const TargetConst&) const {
         return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     __device__ __forceinline__ bool wants(int) const { return true; }
@@ -194,7 +186,7 @@ struct CPCountDv {
     __device__ __forceinline__ Self self(int) const { return Self{}; }
     __device__ __forceinline__ Nb fetch(int, int, int) const { return Nb{}; }
     __device__ __forceinline__ float4 term(const Self&, const Nb&, int, int, float4, const PairGeo&,
-                                           const TargetConst&, HPairCache&) const {
+                                           const TargetConst&) const {
         return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     __device__ __forceinline__ bool wants(int) const { return true; }
@@ -232,7 +224,7 @@ struct CPMom {
     }
     __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{m.s.vm[j], m.s.rp4[j]}; }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
-                                           const PairGeo& g, const TargetConst& tc, HPairCache& pc) const {
+                                           const PairGeo& g, const TargetConst& tc) const {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const DevPhys& P = m.P;
         const bool ff = tj == P.fluid;
@@ -240,7 +232,7 @@ struct CPMom {
         if (!(ff || fw)) return out;
         const float r = sqrtf(g.dr2);
         float hinv, kdw, hh;
-        pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
+        pair_consts<D>(tc, xj.w, hinv, kdw, hh);
         const float dwr = pair_dwr<D, GEN>(P.kernel, r * hinv, hinv, kdw);
         if (dwr == 0.0f) return out;
         const float4 rpi = me.rp, rpj = nb.rp, vi = me.v, vj = nb.v;
@@ -277,8 +269,7 @@ struct CPMom {
     }
     __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
                                               const PairGeo& g, const TargetConst& tc) const {
-        HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
-        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc, pc);
+        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc);
     }
     __device__ __forceinline__ void end(int i, int ti, float4 sum, int) const {
         typename ActMomG<D, FUSED>::Acc a;
@@ -309,11 +300,11 @@ struct CPFilter {
     __device__ __forceinline__ Self self(int) const { return Self{}; }
     __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{s.vol[j], s.vm[j].w}; }
     __device__ __forceinline__ float4 term(const Self&, const Nb& nb, int, int tj, float4 xj, const PairGeo& g,
-                                           const TargetConst& tc, HPairCache& pc) const {
+                                           const TargetConst& tc) const {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (tj != P.fluid) return out;
         float hinv, kdw, hh;
-        pair_consts<D>(tc, pc, xj.w, hinv, kdw, hh);
+        pair_consts<D>(tc, xj.w, hinv, kdw, hh);
         const float w = kern_value<D>(P.kernel, sqrtf(g.dr2), hinv);
         out.x = w * nb.vol;
         out.y = w * nb.m;
@@ -321,8 +312,7 @@ struct CPFilter {
     }
     __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4, float4 xj, const PairGeo& g,
                                               const TargetConst& tc) const {
-        HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
-        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc, pc);
+        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc);
     }
     __device__ __forceinline__ void end(int i, int, float4 sum, int) const {
         wv[i] += sum.x;

@@ -410,7 +410,6 @@ __device__ __noinline__ float4 neighbours_by_stencil(const PairArgs& A, int i, f
     const unsigned amask = A.adj[ti - 1];
     unsigned st = 0;
     const typename Act::Self me = act.self(i);
-    HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
     float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     int cnt = 0;
     for (int r = 0; r < R.n; ++r)
@@ -418,7 +417,7 @@ __device__ __noinline__ float4 neighbours_by_stencil(const PairArgs& A, int i, f
             const float4 xj = A.s.xh[j];
             if (!accept<D>(A, i, xi, amask, tc.h2sq, j, xj, st)) continue;
             const int tj = tag_of(A.s.tagm[j]);
-            const float4 t = act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc, pc);
+            const float4 t = act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc);
             sum.x += t.x;
             sum.y += t.y;
             sum.z += t.z;
@@ -434,7 +433,7 @@ __device__ __noinline__ float4 neighbours_by_stencil(const PairArgs& A, int i, f
 // in flight.  EPI: fused momentum step (integrate + bin for every
 // particle, dead bin included; block 0 clears the scan state).
 template <int D, class Act, bool EPI>
-__global__ void __launch_bounds__(128, D == 2 ? 10 : 4)   // 2D: 10 blocks (48 registers) beat 8 and 12
+__global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 registers) beat 8, 10 and 12
     k_list(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M, const int* ncount,
            const __grid_constant__ Act act, unsigned long long* scan_state, int n_scan_words) {
     if (EPI && blockIdx.x == 0)
@@ -453,17 +452,16 @@ __global__ void __launch_bounds__(128, D == 2 ? 10 : 4)   // 2D: 10 blocks (48 r
             int got = cnt;
             if (cnt <= ListConf<D>::LCAP) {
                 const typename Act::Self me = act.self(i);
-                HPairCache pc{-1.0f, 0.0f, 0.0f, 0.0f};
                 ListReader<D> lr;
                 lr.start(M, i, cnt);
-                if (D == 2) {   // 48 registers: no room for a second neighbour record
+                if (D == 2) {   // 2D: a second neighbour record in flight costs more than it hides
                     for (int k = 0; k < cnt; ++k) {
                         const int j = lr.next(k);
                         EPP_CHECK(j >= 0 && j < A.n_max, 16, j);
                         const int tj = tag_of(A.s.tagm[j]);
                         const float4 xj = A.s.xh[j];
                         const float4 t =
-                            act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc, pc);
+                            act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc);
                         sum.x += t.x;
                         sum.y += t.y;
                         sum.z += t.z;
@@ -488,7 +486,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 10 : 4)   // 2D: 10 blocks (48 r
                         xn = A.s.xh[jn];
                         nn = act.fetch(jn, ti, 0);
                     }
-                    const float4 t = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc, pc);
+                    const float4 t = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc);
                     sum.x += t.x;
                     sum.y += t.y;
                     sum.z += t.z;
