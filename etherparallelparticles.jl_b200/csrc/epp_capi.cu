@@ -56,6 +56,11 @@ DevPhys to_dev(const epp_physics& p) {
     d.fluid = p.fluid_tag;
     d.wall = p.wall_tag;
     d.kahan = p.kahan;
+    d.pff = p.pressure_ff == EPP_PRESSURE_DEFAULT ? EPP_PRESSURE_CLASSIC : p.pressure_ff;    // main.jl:109
+    d.pfw = p.pressure_fw == EPP_PRESSURE_DEFAULT ? EPP_PRESSURE_BALANCED : p.pressure_fw;   // main.jl:113
+    d.tensile = p.tensile;
+    d.wallp = p.wall_pressure;
+    d.gap = nullptr;
     return d;
 }
 
@@ -107,7 +112,12 @@ struct epp_ctx {
     bool rpn_valid = false;     // density preview matches rho, drho and rpn_phys
     float* fwv = nullptr;       // kernel-filter sums (SumWeight, SumWeightedDensity) per sorted particle
     float* fwr = nullptr;
+    float* fwp = nullptr;       // SumWeightedPressure of the wall-pressure extrapolation (SumWeight: fwv)
+    float* gap = nullptr;       // Gap column per caller row (tensile correction)
+    bool has_gap = false;       // the last upload mapped the Gap column
     bool filter_pending = false;   // interaction!(KERNEL_FILTER) done, selfaction!(KERNEL_FILTER_SELF) not yet
+    bool extrap_pending = false;   // interaction!(EXTRAPOLATE_PRESSURE) done, its selfaction! not yet
+    bool rpn_walls = false;        // the density preview carries the extrapolated wall pressure
     long long step_count = 0;      // epp_step steps since upload (the filter runs after every k-th)
     epp_physics rpn_phys{};
     int last_crit = EPP_CRITERION_SYMMETRY;
@@ -175,7 +185,7 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
     b += (size_t)kIntegralBlocks * 8 * 8 + 8 * 8 + 4 * 256;
-    b += 2 * ((size_t)cap * 4 + 256);                    // kernel-filter sums
+    b += 4 * ((size_t)cap * 4 + 256);                    // filter / extrapolation sums, gap by row
     b += 2 * 256;                                                                  // instance tables (small)
     return b + (1 << 20);
 }
@@ -268,6 +278,7 @@ DevPhys dev_phys(epp_ctx* ctx, const epp_physics& p) {
         }
         d.ip = ctx->inst_table;
     }
+    d.gap = ctx->gap;
     return d;
 }
 
@@ -289,7 +300,10 @@ int lanes_of(const epp_ctx* ctx) { return ctx->lanes; }
 // Physics that needs the generic pair terms (any kernel, classic viscosity); the benchmark physics
 // (Wendland C2, artificial viscosity) runs the specialised ones.
 bool generic_physics(const epp_physics* p) {
-    return p && (p->kernel != EPP_KERNEL_WENDLAND_C2 || p->viscosity == EPP_VISCOSITY_CLASSIC);
+    return p && (p->kernel != EPP_KERNEL_WENDLAND_C2 || p->viscosity == EPP_VISCOSITY_CLASSIC ||
+                 (p->pressure_ff != EPP_PRESSURE_DEFAULT && p->pressure_ff != EPP_PRESSURE_CLASSIC) ||
+                 (p->pressure_fw != EPP_PRESSURE_DEFAULT && p->pressure_fw != EPP_PRESSURE_BALANCED) ||
+                 p->tensile != 0);
 }
 
 // Family 0, the search pass: neighbour lists and nCount of set `set` under `crit`.
@@ -517,6 +531,7 @@ int run_search(epp_ctx* ctx, int crit, int action, const epp_physics* phys, bool
     } else {
         ctx->rpn_valid = false;
     }
+    ctx->rpn_walls = false;
     return EPP_OK;
 }
 
@@ -586,6 +601,10 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
                                                                         mom.P, ctx->fwv, ctx->fwr, 1);
         CK_LAUNCH();
     }
+    if (phys.wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE) {   // wall pressure of the previewed density
+        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPExtrap<D, true>{ctx->S[to], mom.P, nullptr, nullptr});
+        if (rc) return rc;
+    }
 #undef EPP_MARK
     return EPP_OK;
 }
@@ -643,6 +662,13 @@ int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
         ctx->filter_pending = false;
         return EPP_OK;
     }
+    if (action == EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF) {
+        k_extrap_finish<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], P, ctx->fwv, ctx->fwp);
+        CK_LAUNCH();
+        ctx->extrap_pending = false;
+        return EPP_OK;
+    }
     k_self<D><<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(action, ctx->start[ctx->cur], ctx->n_cells,
                                                                 ctx->n, ctx->S[ctx->cur], P, ctx->status,
                                                                 ctx->accel);
@@ -669,6 +695,14 @@ int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
         if (ctx->lanes != 0) return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the kernel filter runs on pair-pass family 0");
         const int rc = launch_interaction_pass<D>(ctx, CPFilter<D>{ctx->S[ctx->cur], dev_phys(ctx, *phys), ctx->fwv, ctx->fwr});
         if (rc == EPP_OK) ctx->filter_pending = true;
+        return rc;
+    }
+    if (action == EPP_ACTION_EXTRAPOLATE_PRESSURE) {
+        if (ctx->lanes != 0)
+            return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the pressure extrapolation runs on pair-pass family 0");
+        const int rc = launch_interaction_pass<D>(
+            ctx, CPExtrap<D, false>{ctx->S[ctx->cur], dev_phys(ctx, *phys), ctx->fwv, ctx->fwp});
+        if (rc == EPP_OK) ctx->extrap_pending = true;
         return rc;
     }
     if (action == EPP_ACTION_DAMBREAK_MOMENTUM) {
@@ -704,6 +738,10 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     if (ctx->dv_dirty) {
         // the first step goes through the per-call kernels, which honour a non-zero dVelocity
         rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_DENSITY, &phys);
+        if (!rc && phys.wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE) {
+            rc = run_interaction<D>(ctx, EPP_ACTION_EXTRAPOLATE_PRESSURE, &phys);
+            if (!rc) rc = run_selfaction<D>(ctx, EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF, &phys);
+        }
         if (!rc) rc = run_interaction<D>(ctx, EPP_ACTION_DAMBREAK_MOMENTUM, &phys);
         if (!rc) rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_INTEGRATE, &phys);
         if (!rc) rc = run_search<D>(ctx, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false);
@@ -722,14 +760,21 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         --n_steps;
         if (n_steps == 0) return EPP_OK;
     }
+    const bool extrap = phys.wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE;
     if (!ctx->rpn_valid || !same_phys(ctx->rpn_phys, phys)) {
         k_density_preview<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
             ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], dev_phys(ctx, phys));
         CK_LAUNCH();
+        ctx->rpn_walls = false;
     }
     if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->nlist_valid = false;
     rc = ensure_nlist<D>(ctx);
     if (rc) return rc;
+    if (extrap && !ctx->rpn_walls) {   // the first step's wall pressure (later steps: the graph's tail)
+        rc = launch_list<D>(ctx, ctx->cur, EPP_CRITERION_SYMMETRY,
+                            CPExtrap<D, true>{ctx->S[ctx->cur], dev_phys(ctx, phys), nullptr, nullptr});
+        if (rc) return rc;
+    }
     if (!ctx->graph[0] || !same_phys(ctx->graph_phys, phys) || ctx->graph_accel != accel) {
         ctx->graph_accel = accel;
         rc = build_graphs<D>(ctx, phys);
@@ -742,6 +787,7 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         ctx->cur = 1 - ctx->cur;
     }
     ctx->rpn_valid = true;
+    ctx->rpn_walls = extrap;
     ctx->rpn_phys = phys;
     ctx->searched = true;
     ctx->lists_valid = false;
@@ -763,6 +809,19 @@ int check_physics(epp_ctx* ctx, const epp_physics* p) {
                     "the lane-group pair passes run Wendland C2 with artificial viscosity; use family 0 or 1");
     if (ctx->lanes != 0 && p->filter_interval > 0)
         return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the kernel filter runs on pair-pass family 0");
+    if (p->pressure_ff < EPP_PRESSURE_DEFAULT || p->pressure_ff > EPP_PRESSURE_DENSITY_WEIGHTED ||
+        p->pressure_fw < EPP_PRESSURE_DEFAULT || p->pressure_fw > EPP_PRESSURE_DENSITY_WEIGHTED ||
+        (p->tensile != 0 && p->tensile != 1) || p->wall_pressure < EPP_WALL_PRESSURE_EOS ||
+        p->wall_pressure > EPP_WALL_PRESSURE_EXTRAPOLATE)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pressure option out of range (ff %d, fw %d, tensile %d, wall %d)",
+                    p->pressure_ff, p->pressure_fw, p->tensile, p->wall_pressure);
+    if (p->tensile && !ctx->has_gap)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "the tensile correction needs the Gap column (epp_column_map.gap)");
+    if (ctx->lanes >= 2 && generic_physics(p))
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION,
+                    "the lane-group pair passes run the dam break's pressure terms; use family 0 or 1");
+    if (ctx->lanes != 0 && p->wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE)
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the pressure extrapolation runs on pair-pass family 0");
     return EPP_OK;
 }
 
@@ -863,6 +922,8 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->iresult = a.take<double>(8);
     ctx->iticket = a.take<unsigned>(1);
     ctx->fwv = a.take<float>(ctx->cap);
+    ctx->fwp = a.take<float>(ctx->cap);
+    ctx->gap = a.take<float>(ctx->cap);
     ctx->fwr = a.take<float>(ctx->cap);
     ctx->tmp.count = ctx->count;
     ctx->tmp.cs = ctx->cs;
@@ -1010,7 +1071,15 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     drop_graphs(ctx);   // the captured launches hold the old particle count
     CK(cudaMemsetAsync(ctx->fwv, 0, sizeof(float) * ctx->cap, ctx->stream));
     CK(cudaMemsetAsync(ctx->fwr, 0, sizeof(float) * ctx->cap, ctx->stream));
+    CK(cudaMemsetAsync(ctx->fwp, 0, sizeof(float) * ctx->cap, ctx->stream));
+    ctx->has_gap = m->gap >= 0;   // Gap per caller row: the pair passes index it by State::id
+    if (ctx->has_gap)
+        CK(cudaMemcpyAsync(ctx->gap, fp + (size_t)m->gap * ldf, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    else
+        CK(cudaMemsetAsync(ctx->gap, 0, sizeof(float) * ctx->cap, ctx->stream));
     ctx->filter_pending = false;
+    ctx->extrap_pending = false;
+    ctx->rpn_walls = false;
     ctx->step_count = 0;
     ctx->searched = false;
     ctx->sorted_once = false;
@@ -1117,6 +1186,8 @@ int32_t epp_search(epp_ctx* ctx, int32_t criterion, int32_t action, const epp_ph
     if (const int prc = check_physics(ctx, phys)) return prc;
     if (ctx->filter_pending)
         return fail(ctx, EPP_ERR_STATE, "kernel-filter sums pending: selfaction!(KERNEL_FILTER_SELF) first");
+    if (ctx->extrap_pending)
+        return fail(ctx, EPP_ERR_STATE, "extrapolation sums pending: selfaction!(EXTRAPOLATE_PRESSURE_SELF) first");
     cudaSetDevice(ctx->dev);
     if (ctx->n == 0) return EPP_OK;
     const bool emit = (flags & EPP_SEARCH_EMIT_LIST) != 0;
@@ -1128,9 +1199,9 @@ int32_t epp_interaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     if (action == EPP_ACTION_NONE) return EPP_OK;
     if (action != EPP_ACTION_DAMBREAK_MOMENTUM && action != EPP_ACTION_COUNT_NEIGHBOURS &&
-        action != EPP_ACTION_KERNEL_FILTER)
+        action != EPP_ACTION_KERNEL_FILTER && action != EPP_ACTION_EXTRAPOLATE_PRESSURE)
         return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "interaction action %d", action);
-    if ((action == EPP_ACTION_DAMBREAK_MOMENTUM || action == EPP_ACTION_KERNEL_FILTER) && !phys)
+    if (action != EPP_ACTION_COUNT_NEIGHBOURS && !phys)
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
     if (const int prc = check_physics(ctx, phys)) return prc;
     if (!ctx->searched)
@@ -1145,7 +1216,8 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     if (action == EPP_ACTION_NONE) return EPP_OK;
     if (action != EPP_ACTION_DAMBREAK_DENSITY && action != EPP_ACTION_DAMBREAK_INTEGRATE &&
-        action != EPP_ACTION_ZERO_DVELOCITY && action != EPP_ACTION_KERNEL_FILTER_SELF)
+        action != EPP_ACTION_ZERO_DVELOCITY && action != EPP_ACTION_KERNEL_FILTER_SELF &&
+        action != EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF)
         return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "selfaction action %d", action);
     if (action != EPP_ACTION_ZERO_DVELOCITY && !phys)
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "physics required");
@@ -1160,7 +1232,9 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
         ctx->searched = false;   // positions moved: the next pass needs a search!
         ctx->rpn_valid = false;
     }
-    if (action == EPP_ACTION_DAMBREAK_DENSITY || action == EPP_ACTION_KERNEL_FILTER_SELF) ctx->rpn_valid = false;
+    if (action == EPP_ACTION_DAMBREAK_DENSITY || action == EPP_ACTION_KERNEL_FILTER_SELF ||
+        action == EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF)
+        ctx->rpn_valid = false;
     if (action == EPP_ACTION_ZERO_DVELOCITY) ctx->dv_dirty = true;
     ctx->lists_valid = ctx->lists_valid && action != EPP_ACTION_DAMBREAK_INTEGRATE;
     return rc;
@@ -1172,6 +1246,8 @@ int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys) {
     if (const int prc = check_physics(ctx, phys)) return prc;
     if (ctx->filter_pending)
         return fail(ctx, EPP_ERR_STATE, "kernel-filter sums pending: selfaction!(KERNEL_FILTER_SELF) first");
+    if (ctx->extrap_pending)
+        return fail(ctx, EPP_ERR_STATE, "extrapolation sums pending: selfaction!(EXTRAPOLATE_PRESSURE_SELF) first");
     if (!ctx->searched)
         return fail(ctx, EPP_ERR_STATE, "epp_step needs an initial search! (main.jl:157-164)");
     cudaSetDevice(ctx->dev);

@@ -204,6 +204,14 @@ struct CPCountDv {
     __device__ __forceinline__ void end_idle(int, int) const {}
 };
 
+// p_rho_2 of a pair from the two (rho, p, p/rho^2, 1/rho) records: iClassicPressure!,
+// iBalancedPressure!, iDensityWeightedPressure! (Pressure.jl:24-83).
+__device__ __forceinline__ float pressure_term(int form, float4 rpi, float4 rpj) {
+    if (form == EPP_PRESSURE_CLASSIC) return rpi.z + rpj.z;
+    if (form == EPP_PRESSURE_BALANCED) return (rpi.y + rpj.y) * rpi.w * rpj.w;
+    return __fdiv_rn(2.0f * (rpi.y * rpi.x + rpj.y * rpj.x) * rpi.w * rpj.w, rpi.x + rpj.x);
+}
+
 // Momentum (interaction! of main.jl:107-118) as a per-pair contribution; FUSED adds the
 // integrate + bin epilogue of the fused step.  GEN: any kernel and EPP_VISCOSITY_CLASSIC; otherwise
 // Wendland C2 with artificial viscosity (the benchmark physics).
@@ -215,14 +223,19 @@ struct CPMom {
     struct Self {
         float4 v, rp;
         float c0;
+        float gap;   // GEN with the tensile correction only
     };
     struct Nb {
         float4 v, rp;
+        float gap;
     };
-    __device__ __forceinline__ Self self(int i) const {
-        return Self{m.s.vm[i], m.s.rp4[i], m.P.c0_of(inst_of(m.s.tagm[i]))};
+    __device__ __forceinline__ float gap_of(int i) const {
+        return GEN && m.P.tensile ? m.P.gap[m.s.id[i]] : 0.0f;
     }
-    __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{m.s.vm[j], m.s.rp4[j]}; }
+    __device__ __forceinline__ Self self(int i) const {
+        return Self{m.s.vm[i], m.s.rp4[i], m.P.c0_of(inst_of(m.s.tagm[i])), gap_of(i)};
+    }
+    __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{m.s.vm[j], m.s.rp4[j], gap_of(j)}; }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
                                            const PairGeo& g, const TargetConst& tc) const {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -236,7 +249,17 @@ struct CPMom {
         const float dwr = pair_dwr<D, GEN>(P.kernel, r * hinv, hinv, kdw);
         if (dwr == 0.0f) return out;
         const float4 rpi = me.rp, rpj = nb.rp, vi = me.v, vj = nb.v;
-        const float p_rho_2 = ff ? rpi.z + rpj.z : (rpi.y + rpj.y) * rpi.w * rpj.w;
+        float p_rho_2;
+        if (!GEN) {   // the dam break's pair: classic fluid-fluid, balanced fluid-wall
+            p_rho_2 = ff ? rpi.z + rpj.z : (rpi.y + rpj.y) * rpi.w * rpj.w;
+        } else {
+            p_rho_2 = pressure_term(ff ? P.pff : P.pfw, rpi, rpj);
+            if (P.tensile) {   // iPressureCorrection (Pressure.jl:10-22)
+                const float w = kern_value<D>(P.kernel, r, hinv);
+                const float w_gap = kern_value<D>(P.kernel, 0.5f * (me.gap + nb.gap), hinv);
+                p_rho_2 += fabsf(p_rho_2) * __fdiv_rn(0.01f * w, w_gap);
+            }
+        }
         const float fp = p_rho_2 * (-vj.w * dwr);
         out.x = fp * g.dx;
         out.y = fp * g.dy;
@@ -317,6 +340,64 @@ struct CPFilter {
     __device__ __forceinline__ void end(int i, int, float4 sum, int) const {
         wv[i] += sum.x;
         wvr[i] += sum.y;
+    }
+    __device__ __forceinline__ void end_idle(int, int) const {}
+};
+
+// Wall pressure extrapolation over wall-fluid pairs (iExtrapolatePressure!, Pressure.jl:85-131):
+// wv += W V_j and wv_p += W V_j (max(p_j, p0) + max(rho_j g.r_ij, p0)).  FUSED: inside epp_step,
+// right after the density preview, so rho_j and p_j are the preview's (rp4) with V_j = m_j / rho_j,
+// and each wall particle's thread finishes its own sums (sExtrapolatePressure!,
+// Pressure.jl:133-150) into its preview record; only fluid records are read and only wall
+// records are written, so the pass has no read-after-write hazard.  Otherwise the sums are added
+// to wv / wvp for EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF.
+template <int D, bool FUSED>
+struct CPExtrap {
+    State s;
+    DevPhys P;
+    float* wv;
+    float* wvp;
+    static constexpr int NC = 2;
+    __device__ __forceinline__ bool wants(int ti) const { return ti == P.wall; }
+    struct Self {};
+    struct Nb {
+        float rho, p, vol;
+    };
+    __device__ __forceinline__ Self self(int) const { return Self{}; }
+    __device__ __forceinline__ Nb fetch(int j, int, int) const {
+        if (FUSED) {
+            const float4 rp = s.rp4[j];
+            return Nb{rp.x, rp.y, __fdiv_rn(s.vm[j].w, rp.x)};
+        }
+        return Nb{s.rho[j], s.p[j], s.vol[j]};
+    }
+    __device__ __forceinline__ float4 term(const Self&, const Nb& nb, int, int tj, float4 xj, const PairGeo& g,
+                                           const TargetConst& tc) const {
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (tj != P.fluid) return out;
+        float hinv, kdw, hh;
+        pair_consts<D>(tc, xj.w, hinv, kdw, hh);
+        const float w = kern_value<D>(P.kernel, sqrtf(g.dr2), hinv);
+        float g_dot_x = g.dx * P.g[0];
+        g_dot_x += g.dy * P.g[1];
+        if (D == 3) g_dot_x += g.dz * P.g[2];
+        const float w_v = w * nb.vol;
+        out.x = w_v;
+        out.y = w_v * (fmaxf(nb.p, P.p0) + fmaxf(nb.rho * g_dot_x, P.p0));
+        return out;
+    }
+    __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4, float4 xj, const PairGeo& g,
+                                              const TargetConst& tc) const {
+        return term(self(i), fetch(j, ti, tj), ti, tj, xj, g, tc);
+    }
+    __device__ __forceinline__ void end(int i, int, float4 sum, int) const {
+        if (FUSED) {
+            const float p = sum.x > 0.0f ? __fdiv_rn(sum.y, sum.x) : P.p0;
+            s.rp4[i] = make_rp4(s.rp4[i].x, p);
+        } else {
+            wv[i] += sum.x;
+            wvp[i] += sum.y;
+        }
     }
     __device__ __forceinline__ void end_idle(int, int) const {}
 };

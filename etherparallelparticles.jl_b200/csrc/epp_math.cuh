@@ -42,7 +42,10 @@ struct DevPhys {
     float alpha, beta, mu;
     int gamma, visc, fluid, wall, kahan;
     int kernel, eos, motion;   // EPP_KERNEL_*, EPP_EOS_*, EPP_MOTION_*
+    int pff, pfw;              // EPP_PRESSURE_* of fluid-fluid and fluid-wall pairs (DEFAULT resolved)
+    int tensile, wallp;        // iPressureCorrection on / off, EPP_WALL_PRESSURE_*
     const InstPhys* ip;
+    const float* gap;          // Gap per caller row (indexed by State::id); tensile correction only
     __device__ __forceinline__ float dt_of(int inst) const { return ip ? ip[inst].dt : dt; }
     __device__ __forceinline__ float c0_of(int inst) const { return ip ? ip[inst].c0 : c0; }
     __device__ __forceinline__ float B_of(int inst) const { return ip ? ip[inst].B : B; }

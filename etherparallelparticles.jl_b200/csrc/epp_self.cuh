@@ -81,6 +81,23 @@ __global__ void k_filter_finish(const int* start, int n_cells, int n_max, State 
     }
 }
 
+// sExtrapolatePressure! (Pressure.jl:133-150) on wall particles: p = wv_p / wv and the sums
+// cleared, or p = p0 when no fluid neighbour contributed.
+__global__ void k_extrap_finish(const int* start, int n_cells, int n_max, State s, DevPhys P, float* wv,
+                                float* wvp) {
+    const int n_alive = min(start[n_cells], n_max);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_alive || tag_of(s.tagm[i]) != P.wall) return;
+    const float a = wv[i];
+    if (a > 0.0f) {
+        s.p[i] = __fdiv_rn(wvp[i], a);
+        wv[i] = 0.0f;
+        wvp[i] = 0.0f;
+    } else {
+        s.p[i] = P.p0;
+    }
+}
+
 // Density preview used when the fused step starts from a state whose rpn is not current.
 __global__ void k_density_preview(const int* start, int n_cells, int n_max, State s, DevPhys P) {
     const int n_alive = min(start[n_cells], n_max);

@@ -5,7 +5,7 @@ the header cites the reference interface each entry point replaces.
 """
 import ctypes as C
 
-EPP_ABI_VERSION = 2
+EPP_ABI_VERSION = 3
 EPP_MAX_TAGS = 16
 
 # epp_status
@@ -56,6 +56,8 @@ EPP_ACTION_ZERO_DVELOCITY = 5
 EPP_ACTION_COUNT_NEIGHBOURS = 6
 EPP_ACTION_KERNEL_FILTER = 7
 EPP_ACTION_KERNEL_FILTER_SELF = 8
+EPP_ACTION_EXTRAPOLATE_PRESSURE = 9
+EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF = 10
 
 EPP_SEARCH_EMIT_LIST = 1
 
@@ -75,6 +77,14 @@ EPP_EOS_LINEAR = 1
 
 EPP_MOTION_SYMPLECTIC = 0
 EPP_MOTION_ACCELERATE_MOVE = 1
+
+EPP_PRESSURE_DEFAULT = 0
+EPP_PRESSURE_CLASSIC = 1
+EPP_PRESSURE_BALANCED = 2
+EPP_PRESSURE_DENSITY_WEIGHTED = 3
+
+EPP_WALL_PRESSURE_EOS = 0
+EPP_WALL_PRESSURE_EXTRAPOLATE = 1
 
 
 class epp_domain(C.Structure):
@@ -105,6 +115,10 @@ class epp_physics(C.Structure):
         ("mu", C.c_float),
         ("motion", C.c_int32),
         ("filter_interval", C.c_int32),
+        ("pressure_ff", C.c_int32),
+        ("pressure_fw", C.c_int32),
+        ("tensile", C.c_int32),
+        ("wall_pressure", C.c_int32),
     ]
 
 
@@ -170,7 +184,8 @@ def make_domain(dim, gap, first, last):
 def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81, 0.0),
                  alpha=0.1, beta=0.1, viscosity=EPP_VISCOSITY_REFERENCE, fluid_tag=1,
                  wall_tag=2, kahan=1, kernel=EPP_KERNEL_WENDLAND_C2, eos=EPP_EOS_TAIT, mu=0.0,
-                 motion=EPP_MOTION_SYMPLECTIC, filter_interval=0):
+                 motion=EPP_MOTION_SYMPLECTIC, filter_interval=0, pressure_ff=EPP_PRESSURE_DEFAULT,
+                 pressure_fw=EPP_PRESSURE_DEFAULT, tensile=0, wall_pressure=EPP_WALL_PRESSURE_EOS):
     p = epp_physics()
     p.dt = dt
     p.rho0 = rho0
@@ -190,6 +205,10 @@ def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81
     p.mu = mu
     p.motion = motion
     p.filter_interval = filter_interval
+    p.pressure_ff = pressure_ff
+    p.pressure_fw = pressure_fw
+    p.tensile = tensile
+    p.wall_pressure = wall_pressure
     return p
 
 

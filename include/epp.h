@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define EPP_ABI_VERSION 2
+#define EPP_ABI_VERSION 3
 #define EPP_MAX_TAGS 16
 
 typedef enum epp_status {
@@ -73,6 +73,11 @@ typedef enum epp_status {
                                             * (main.jl:128-134, Filter.jl:10-23) */
 #define EPP_ACTION_KERNEL_FILTER_SELF    8 /* selfaction!: sFilter, fluid: rho = (wv_rho + W0 m)/(wv + W0 V),
                                             * V = m/rho, p = eos (main.jl:136-144, Filter.jl:25-38) */
+#define EPP_ACTION_EXTRAPOLATE_PRESSURE  9 /* interaction!: wall i, fluid j: iExtrapolatePressure!
+                                            * wv += W V_j, wv_p += W V_j (max(p_j, p0) + max(rho_j g.r_ij, p0))
+                                            * (Pressure.jl:85-131; p0 and g of the physics) */
+#define EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF 10 /* selfaction!: wall: sExtrapolatePressure! p = wv_p / wv,
+                                                * or p0 without fluid neighbours (Pressure.jl:133-150) */
 
 /* epp_search flags */
 #define EPP_SEARCH_EMIT_LIST 1 /* keep per-particle neighbour lists for epp_download */
@@ -96,6 +101,18 @@ typedef enum epp_status {
 #define EPP_MOTION_SYMPLECTIC       0 /* sAccelerate! + sMove!: u += du dt, x += u dt (Motion.jl:17-51) */
 #define EPP_MOTION_ACCELERATE_MOVE  1 /* sAccelerateMove!: x += (u + du dt/2) dt, u += du dt (Motion.jl:61-75) */
 
+/* Pressure term of a pair (Pressure.jl:24-83); DEFAULT is the dam break's choice per pair type:
+ * CLASSIC for fluid-fluid (main.jl:109), BALANCED for fluid-wall (main.jl:113) */
+#define EPP_PRESSURE_DEFAULT          0
+#define EPP_PRESSURE_CLASSIC          1 /* iClassicPressure!: p_i / rho_i^2 + p_j / rho_j^2 */
+#define EPP_PRESSURE_BALANCED         2 /* iBalancedPressure!: (p_i + p_j) / (rho_i rho_j) */
+#define EPP_PRESSURE_DENSITY_WEIGHTED 3 /* iDensityWeightedPressure!: 2 (p_i rho_i + p_j rho_j) /
+                                         * ((rho_i + rho_j) rho_i rho_j) */
+
+/* Wall pressure in epp_step */
+#define EPP_WALL_PRESSURE_EOS         0 /* p = eos(rho) like the fluid (main.jl:99-102) */
+#define EPP_WALL_PRESSURE_EXTRAPOLATE 1 /* after each density update, EXTRAPOLATE_PRESSURE(_SELF) */
+
 typedef struct epp_domain {
     int32_t dim;      /* 2 (Domain2D, src/Class/Domain/Domain2D.jl:28-67) or 3 (new) */
     float gap;        /* cell size; the reference uses 2h */
@@ -117,7 +134,8 @@ typedef struct epp_physics {
     int32_t wall_tag;     /* 2 in the reference example */
     int32_t kahan;        /* 1: compensated (Kahan) position update; 0: sMove! as written */
     /* Zero in each field below is the benchmark physics (Wendland C2, Tait, symplectic Euler, no
-     * filter); the reference example (example/collapse_dry/same/main.jl) is CUBIC_SPLINE, LINEAR,
+     * filter, the dam break's pressure terms, no tensile correction, wall pressure from the EOS);
+     * the reference example (example/collapse_dry/same/main.jl) is CUBIC_SPLINE, LINEAR,
      * EPP_VISCOSITY_CLASSIC with mu = 1e-3, ACCELERATE_MOVE and filter_interval = 20. */
     int32_t kernel;           /* EPP_KERNEL_* */
     int32_t eos;              /* EPP_EOS_* */
@@ -125,6 +143,11 @@ typedef struct epp_physics {
     int32_t motion;           /* EPP_MOTION_* */
     int32_t filter_interval;  /* epp_step: kernel filter after the search of every k-th step
                                * (steps counted from 1 after epp_upload, main.jl:180-183); 0 = never */
+    int32_t pressure_ff;      /* EPP_PRESSURE_* of fluid-fluid pairs */
+    int32_t pressure_fw;      /* EPP_PRESSURE_* of fluid-wall pairs */
+    int32_t tensile;          /* 1: iPressureCorrection (Pressure.jl:10-22) on both: the pressure term
+                               * grows by |term| 0.01 W(r) / W((gap_i + gap_j) / 2); needs the gap column */
+    int32_t wall_pressure;    /* EPP_WALL_PRESSURE_* */
 } epp_physics;
 
 typedef struct epp_config {

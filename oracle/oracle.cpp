@@ -222,6 +222,7 @@ template <typename T>
 struct Phys {
     T dt, rho0, c0, p0, B, g[3], alpha, beta, coef, mu, c02;
     int gamma, visc, fluid, wall, kahan, kernel, eos, motion, filter_interval;
+    int pff, pfw, tensile, wallp;   // resolved EPP_PRESSURE_* per pair type, tensile flag, EPP_WALL_PRESSURE_*
 };
 template <typename T>
 Phys<T> make_phys(const epp_physics& p) {
@@ -247,6 +248,10 @@ Phys<T> make_phys(const epp_physics& p) {
     o.c02 = o.c0 * o.c0;   // main.jl:58 const c02 = c0 * c0
     o.motion = p.motion;
     o.filter_interval = p.filter_interval;
+    o.pff = p.pressure_ff == EPP_PRESSURE_DEFAULT ? EPP_PRESSURE_CLASSIC : p.pressure_ff;    // main.jl:109
+    o.pfw = p.pressure_fw == EPP_PRESSURE_DEFAULT ? EPP_PRESSURE_BALANCED : p.pressure_fw;   // main.jl:113
+    o.tensile = p.tensile;
+    o.wallp = p.wall_pressure;
     return o;
 }
 
@@ -283,6 +288,7 @@ struct System : SysBase {
     std::vector<T> pos, vel, dvel, comp, accel, accel_abs, drho_abs;
     std::vector<T> mass, vol, rho, drho, p, gapc, h;
     std::vector<T> wv, wv_rho;   // kernel-filter sums (Filter.jl: SumWeight, SumWeightedDensity)
+    std::vector<T> wv_p;         // SumWeightedPressure of the wall-pressure extrapolation (Pressure.jl:85-131)
     long long step_count = 0;    // steps since upload (main.jl:165 step += 1)
     std::vector<T> nw, ndw, nhinv, nr, nrvec;
     /* neighbour system */
@@ -330,7 +336,7 @@ struct System : SysBase {
         drho_abs.assign(N, 0);
         mass.assign(N, 0); vol.assign(N, 0); rho.assign(N, 0); drho.assign(N, 0);
         p.assign(N, 0); gapc.assign(N, 0); h.assign(N, 0);
-        wv.assign(N, 0); wv_rho.assign(N, 0);
+        wv.assign(N, 0); wv_rho.assign(N, 0); wv_p.assign(N, 0);
         nw.assign(N * max_nb, 0); ndw.assign(N * max_nb, 0); nhinv.assign(N * max_nb, 0);
         nr.assign(N * max_nb, 0); nrvec.assign(N * max_nb * D, 0);
         ccount.assign(dom.n_cells, 0);
@@ -483,7 +489,8 @@ struct System : SysBase {
     int interaction(int action, const Phys<T>& P) {
         if (!searched) return EPP_ERR_STATE;
         if (action != EPP_ACTION_DAMBREAK_MOMENTUM && action != EPP_ACTION_COUNT_NEIGHBOURS &&
-            action != EPP_ACTION_NONE && action != EPP_ACTION_KERNEL_FILTER)
+            action != EPP_ACTION_NONE && action != EPP_ACTION_KERNEL_FILTER &&
+            action != EPP_ACTION_EXTRAPOLATE_PRESSURE)
             return EPP_ERR_UNSUPPORTED_ACTION;
 #pragma omp parallel for schedule(dynamic, 256)
         for (int I = 0; I < n; ++I) {
@@ -502,6 +509,17 @@ struct System : SysBase {
                         wv[I] += NW(ni, I) * vol[J];
                         wv_rho[I] += NW(ni, I) * mass[J];
                     }
+                } else if (action == EPP_ACTION_EXTRAPOLATE_PRESSURE) {
+                    /* iExtrapolatePressure!, Pressure.jl:85-131, on wall-fluid pairs with the kernel
+                     * value cached by the search; p0 and g of the physics */
+                    int J = NIDX(ni, I) - 1;
+                    if (tag[I] == P.wall && tag[J] == P.fluid) {
+                        T g_dot_x = T(0.0);
+                        for (int a = 0; a < D; ++a) g_dot_x += RV(ni, a, I) * P.g[a];
+                        T w_v = NW(ni, I) * vol[J];
+                        wv[I] += w_v;
+                        wv_p[I] += w_v * (std::max(p[J], P.p0) + std::max(rho[J] * g_dot_x, P.p0));
+                    }
                 }
             }
         }
@@ -519,9 +537,18 @@ struct System : SysBase {
         T dw = NDW(ni, I);
         T r = NR(ni, I);
         T p_rho_2;
-        if (ff) p_rho_2 = p[I] / (rho[I] * rho[I]) + p[J] / (rho[J] * rho[J]);
-        else p_rho_2 = (p[I] + p[J]) / (rho[I] * rho[J]);
-        p_rho_2 += std::fabs(p_rho_2) * P.coef;
+        const int form = ff ? P.pff : P.pfw;
+        if (form == EPP_PRESSURE_CLASSIC)   // iClassicPressure!, Pressure.jl:24-41
+            p_rho_2 = p[I] / (rho[I] * rho[I]) + p[J] / (rho[J] * rho[J]);
+        else if (form == EPP_PRESSURE_BALANCED)   // iBalancedPressure!, :43-60
+            p_rho_2 = (p[I] + p[J]) / (rho[I] * rho[J]);
+        else   // iDensityWeightedPressure!, :62-79
+            p_rho_2 = 2 * (p[I] * rho[I] + p[J] * rho[J]) / ((rho[I] + rho[J]) * rho[I] * rho[J]);
+        T coef = P.coef;
+        if (P.tensile)   // iPressureCorrection, :10-22: 0.01 w / W(mean gap, hinv), w = W(r) of the pair
+            coef = T(0.01) * kern_value<T>(P.kernel, r, NH(ni, I), D) /
+                   kern_value<T>(P.kernel, arithmetic<T>(gapc[I], gapc[J]), NH(ni, I), D);
+        p_rho_2 += std::fabs(p_rho_2) * coef;
         p_rho_2 *= -mass[J] * dw / r;
         for (int a = 0; a < D; ++a) {
             DU(a, I) += p_rho_2 * RV(ni, a, I);
@@ -559,13 +586,25 @@ struct System : SysBase {
     int selfaction(int action, const Phys<T>& P) {
         if (action == EPP_ACTION_NONE) return EPP_OK;
         if (action != EPP_ACTION_DAMBREAK_DENSITY && action != EPP_ACTION_DAMBREAK_INTEGRATE &&
-            action != EPP_ACTION_ZERO_DVELOCITY && action != EPP_ACTION_KERNEL_FILTER_SELF)
+            action != EPP_ACTION_ZERO_DVELOCITY && action != EPP_ACTION_KERNEL_FILTER_SELF &&
+            action != EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF)
             return EPP_ERR_UNSUPPORTED_ACTION;
 #pragma omp parallel for schedule(static)
         for (int I = 0; I < n; ++I) {
             if (alive[I] != 1) continue;
             if (action == EPP_ACTION_ZERO_DVELOCITY) {
                 for (int a = 0; a < D; ++a) DU(a, I) = T(0.0);
+            } else if (action == EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF) {
+                /* sExtrapolatePressure!, Pressure.jl:133-150, on wall particles */
+                if (tag[I] == P.wall) {
+                    if (wv[I] > T(0.0)) {
+                        p[I] = wv_p[I] / wv[I];
+                        wv[I] = T(0.0);
+                        wv_p[I] = T(0.0);
+                    } else {
+                        p[I] = P.p0;
+                    }
+                }
             } else if (action == EPP_ACTION_KERNEL_FILTER_SELF) {
                 /* sFilter, main.jl:136-144: sKernelFilter! (Filter.jl:25-38), sVolume!, eos */
                 if (tag[I] == P.fluid) {
@@ -641,6 +680,10 @@ struct System : SysBase {
         for (int s = 0; s < nsteps; ++s) {
             ++step_count;
             selfaction(EPP_ACTION_DAMBREAK_DENSITY, P);
+            if (P.wallp == EPP_WALL_PRESSURE_EXTRAPOLATE) {   // wall pressure from the fluid around it
+                interaction(EPP_ACTION_EXTRAPOLATE_PRESSURE, P);
+                selfaction(EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF, P);
+            }
             interaction(EPP_ACTION_DAMBREAK_MOMENTUM, P);
             selfaction(EPP_ACTION_DAMBREAK_INTEGRATE, P);
             search(EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, P);
@@ -706,6 +749,7 @@ int upload(System<T>* s, int32_t n, const int32_t* alive, const int32_t* cell, c
     s->step_count = 0;
     std::fill(s->wv.begin(), s->wv.end(), T(0));       // filter sums start at zero (not uploaded)
     std::fill(s->wv_rho.begin(), s->wv_rho.end(), T(0));
+    std::fill(s->wv_p.begin(), s->wv_p.end(), T(0));
     return EPP_OK;
 }
 

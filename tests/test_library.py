@@ -183,3 +183,132 @@ def test_filter_pending_and_family_errors():
     with pytest.raises(EppError) as e:
         c.step(1, bad)
     assert e.value.code == abi.EPP_ERR_INVALID_ARGUMENT
+
+
+DW, BAL, CLS = abi.EPP_PRESSURE_DENSITY_WEIGHTED, abi.EPP_PRESSURE_BALANCED, abi.EPP_PRESSURE_CLASSIC
+EXTRAP = abi.EPP_WALL_PRESSURE_EXTRAPOLATE
+PRESSURE_OPTIONS = [
+    (2, 0.04, dict(pressure_ff=DW, pressure_fw=DW, tensile=1)),
+    (3, 0.02, dict(pressure_ff=BAL, pressure_fw=CLS, tensile=1, kernel=abi.EPP_KERNEL_WENDLAND_C4)),
+    (2, 0.04, dict(kernel=abi.EPP_KERNEL_CUBIC_SPLINE, wall_pressure=EXTRAP)),
+    (3, 0.02, dict(pressure_ff=DW, wall_pressure=EXTRAP)),
+]
+
+
+@pytest.mark.parametrize("dim,dx,options", PRESSURE_OPTIONS)
+def test_pressure_stage_parity(dim, dx, options):
+    """Pressure.jl on the CUDA path, each stage from the device state loaded into the oracle: the
+    wall-pressure extrapolation (iExtrapolatePressure! + sExtrapolatePressure!), then momentum with
+    the chosen pressure terms and iPressureCorrection, integration and search + continuity."""
+    max_nb = 40 if dim == 2 else 100
+    case = with_physics(make_case(dim, dx, max_nb), **options)
+    phys = case.physics
+    dps, o = pair(case, max_nb)
+    n = case.n
+    c = dps.ctx
+    c.search(SYM, CONT, phys, 0)
+    o.search(SYM, CONT, phys)
+    wall = case.ps["Tag"][:n] == casegen.WALL_TAG
+    for _ in range(2):
+        sync_oracle(dps, o, case)
+        c.selfaction(abi.EPP_ACTION_DAMBREAK_DENSITY, phys)
+        o.selfaction(abi.EPP_ACTION_DAMBREAK_DENSITY, phys)
+        if options.get("wall_pressure") == EXTRAP:
+            sync_oracle(dps, o, case)
+            c.interaction(abi.EPP_ACTION_EXTRAPOLATE_PRESSURE, phys)
+            c.selfaction(abi.EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF, phys)
+            o.interaction(abi.EPP_ACTION_EXTRAPOLATE_PRESSURE, phys)
+            o.selfaction(abi.EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF, phys)
+            c.synchronize()
+            g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+            # a weighted mean of non-negative terms: relative error of a few FP32 roundings
+            assert rel_err(g["p"][wall], r["p"][wall], 1.0) < REL
+            assert np.array_equal(g["p"][~wall], r["p"][~wall].astype(np.float32))
+        sync_oracle(dps, o, case)
+        c.interaction(abi.EPP_ACTION_DAMBREAK_MOMENTUM, phys)
+        o.interaction(abi.EPP_ACTION_DAMBREAK_MOMENTUM, phys)
+        c.synchronize()
+        g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+        dv_abs = np.stack([o.field(ORC_FIELD_ACCEL_ABS, a, n) for a in range(dim)], 1)
+        assert cond_err(g["dv"], r["dv"], dv_abs) < REL
+        sync_oracle(dps, o, case)
+        c.selfaction(abi.EPP_ACTION_DAMBREAK_INTEGRATE, phys)
+        o.selfaction(abi.EPP_ACTION_DAMBREAK_INTEGRATE, phys)
+        c.synchronize()
+        g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+        assert rel_err(g["x"], r["x"], 1.0) < 1e-6
+        sync_oracle(dps, o, case)
+        c.search(SYM, CONT, phys, 0)
+        o.search(SYM, CONT, phys)
+        c.synchronize()
+        g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+        assert cond_err(g["drho"], r["drho"], o.field(ORC_FIELD_DDENSITY_ABS, 0, n)) < REL
+
+
+@pytest.mark.parametrize("dim,dx,options", PRESSURE_OPTIONS)
+def test_pressure_fused_steps(dim, dx, options):
+    """epp_step with the pressure options (the extrapolation inside the fused step, after each
+    density preview) against the oracle's loop from the same initial state."""
+    max_nb = 40 if dim == 2 else 100
+    steps = 20
+    case = with_physics(make_case(dim, dx, max_nb), **options)
+    phys = case.physics
+    dps, o = pair(case, max_nb)
+    n = case.n
+    dps.ctx.search(SYM, CONT, phys, 0)
+    o.search(SYM, CONT, phys)
+    dps.ctx.step(steps, phys)
+    o.step(steps, phys)
+    dps.ctx.synchronize()
+    g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+    assert np.max(np.abs(g["x"] - r["x"])) < 1e-6
+    assert np.max(np.abs(g["rho"] - r["rho"]) / r["rho"]) < 1e-5
+    assert np.max(np.abs(g["v"] - r["v"])) <= 1e-3 * max(np.max(np.abs(r["v"])), 1e-3)
+    assert np.max(np.abs(g["p"] - r["p"])) <= 1e-4 * max(np.max(np.abs(r["p"])), 1.0)
+    if options.get("wall_pressure") == EXTRAP:   # the walls' pressure is not the EOS of their density
+        wall = case.ps["Tag"][:n] == casegen.WALL_TAG
+        eos = copy.copy(phys)
+        eos.wall_pressure = abi.EPP_WALL_PRESSURE_EOS
+        d2, _ = pair(with_physics(make_case(dim, dx, max_nb), **dict(options, wall_pressure=0)), max_nb)
+        d2.ctx.search(SYM, CONT, eos, 0)
+        d2.ctx.step(steps, eos)
+        d2.ctx.synchronize()
+        assert not np.array_equal(gpu_fields(d2)["p"][wall], g["p"][wall])
+
+
+def test_pressure_option_errors():
+    case = with_physics(make_case(2, 0.04, 40), wall_pressure=EXTRAP)
+    phys = case.physics
+    dps, _ = pair(case, 40)
+    c = dps.ctx
+    c.search(SYM, CONT, phys, 0)
+    c.interaction(abi.EPP_ACTION_EXTRAPOLATE_PRESSURE, phys)
+    with pytest.raises(EppError) as e:   # the sums are indexed by the current order
+        c.search(SYM, CONT, phys, 0)
+    assert e.value.code == abi.EPP_ERR_STATE
+    with pytest.raises(EppError) as e:
+        c.step(1, phys)
+    assert e.value.code == abi.EPP_ERR_STATE
+    c.selfaction(abi.EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF, phys)
+    c.search(SYM, CONT, phys, 0)
+    for fam in (1, 4):
+        c.set_tuning(fam)
+        with pytest.raises(EppError) as e:
+            c.step(1, phys)
+        assert e.value.code == abi.EPP_ERR_UNSUPPORTED_ACTION
+    c.set_tuning(0)
+    for field, value in (("pressure_ff", 4), ("pressure_fw", -1), ("tensile", 2), ("wall_pressure", 2)):
+        bad = copy.copy(phys)
+        setattr(bad, field, value)
+        with pytest.raises(EppError) as e:
+            c.step(1, bad)
+        assert e.value.code == abi.EPP_ERR_INVALID_ARGUMENT, field
+    # the tensile correction reads the Gap column: refused when the upload did not map it
+    dps.cmap.gap = -1
+    dps.syncto()
+    c.search(SYM, CONT, case.physics, 0)
+    t = copy.copy(phys)
+    t.tensile = 1
+    with pytest.raises(EppError) as e:
+        c.step(1, t)
+    assert e.value.code == abi.EPP_ERR_INVALID_ARGUMENT
