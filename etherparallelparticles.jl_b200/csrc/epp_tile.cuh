@@ -336,13 +336,17 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                         hc_h = h0;
                         hc_r2 = dflt ? A.dom.gap_square : h0 == xi.w ? tc.h2sq : pair_r2(xi.w, h0);
                     }
-                    const float R2 = hc_r2;
+                    // dr2 <= R2 as integers: non-negative floats order like their bit patterns, so
+                    // bits(dr2) - bits(R2) - 1 is negative exactly for the accepted candidates, and
+                    // a funnel shift moves that sign bit into the chunk's word (candidate 0 ends in
+                    // the top bit; one bit reversal per chunk restores candidate order)
+                    const int nR2 = -__float_as_int(hc_r2) - 1;
                     // two candidates per packed sub / mul; dr2 = (dx dx + dy dy) + dz dz, IEEE
                     const f32x2 XI = f2_pack(xi.x, xi.x), YI = f2_pack(xi.y, xi.y), ZI = f2_pack(xi.z, xi.z);
                     const f32x2* px = reinterpret_cast<const f32x2*>(s_p[wib][0]);
                     const f32x2* py = reinterpret_cast<const f32x2*>(s_p[wib][1]);
                     const f32x2* pz = reinterpret_cast<const f32x2*>(s_p[wib][2]);
-#pragma unroll 8
+#pragma unroll
                     for (int b = 0; b < 16; ++b) {
                         const f32x2 dx = f2_sub(XI, px[b]);
                         const f32x2 dy = f2_sub(YI, py[b]);
@@ -357,8 +361,10 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                             d0 = __fadd_rn(d0, z0);
                             d1 = __fadd_rn(d1, z1);
                         }
-                        word |= ((unsigned)(d0 <= R2) | ((unsigned)(d1 <= R2) << 1)) << (2 * b);
+                        word = __funnelshift_l((unsigned)(__float_as_int(d0) + nR2), word, 1);
+                        word = __funnelshift_l((unsigned)(__float_as_int(d1) + nR2), word, 1);
                     }
+                    word = __brev(word);
                 } else {
 #pragma unroll 8
                     for (int b = 0; b < 32; ++b) {
