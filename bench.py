@@ -470,9 +470,10 @@ def run_serve(args):
     if args.autotune:
         for s_ in mine:
             c = s_.case()
-            k = autotune.TuneCache.key(tuner.gpu, c.meta["dim"], c.n, False)
+            cp = be.copies(c.n)
+            k = autotune.TuneCache.key(tuner.gpu, c.meta["dim"], c.n, False, cp)
             if k not in tuned:
-                tuned[k] = tuner.best(c.meta["dim"], c.n, case=c)
+                tuned[k] = tuner.best(c.meta["dim"], c.n, case=c, concurrent=cp)
     # warm-up: one small request of each dimension (module load, first graph build)
     warm = [s for s in serve.request_stream(16, seed=99, n_range=(1e3, 3e3), steps=10)]
     warm = [next(s for s in warm if s.dim == 2), next(s for s in warm if s.dim == 3)]

@@ -11,8 +11,11 @@ compared bit-exactly per step, so the cadence is 1.
 
 A configuration is tuned on a representative dam break of the same dimension and size bucket
 (particle count rounded to a quarter decade), timed over a few steps, and cached in a JSON file
-keyed by GPU name, dimension, size bucket and batch-ness.  Batches (more than one instance) use
-family 0 and tune the block size only.
+keyed by GPU name, dimension, size bucket and mode.  Batches (more than one instance) use family 0
+and tune the block size only.  Two objectives: "single" is one run's time per step (the plain
+path); "concurrent" is the time per step per run of several copies stepped together on their own
+streams (serving, where many runs share the GPU): a family that wins alone by launching fewer,
+wider kernels can lose once the GPU is full.
 """
 import json
 import math
@@ -59,8 +62,9 @@ class TuneCache:
                 self.data = {}
 
     @staticmethod
-    def key(gpu, dim, n, batch):
-        return "%s|%dD|b%d|%s" % (gpu, dim, size_bucket(n), "batch" if batch else "single")
+    def key(gpu, dim, n, batch, concurrent=0):
+        mode = "batch" if batch else "concurrent%d" % concurrent if concurrent > 1 else "single"
+        return "%s|%dD|b%d|%s" % (gpu, dim, size_bucket(n), mode)
 
     def get(self, key):
         return self.data.get(key)
@@ -89,13 +93,54 @@ def time_config(ctx, phys, family, threads, steps=20, warmup=3):
     return 1e3 * (time.perf_counter() - t0) / steps
 
 
-def tune_case(case, n_instances=1, inst=None, steps=20, device=0, timer=time_config, batch=None):
+def concurrent_copies(n, limit=16):
+    """Copies stepped together when tuning for serving: enough small runs to fill the GPU, fewer
+    of the large ones (about 4M particles in all)."""
+    return max(1, min(limit, int(4e6 // max(n, 1))))
+
+
+def time_concurrent(case, family, threads, copies, steps=20, warmup=3, device=0):
+    """Host-clock ms per step per copy: `copies` contexts holding `case`, each on its own
+    stream, enqueued together and waited for together."""
+    from .algorithm import DeviceParticleSystem
+    from .classes import NeighbourSystem
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    runs = []
+    try:
+        for _ in range(copies):
+            d = DeviceParticleSystem(case.ps, ns, device=device)
+            runs.append(d)
+            d.ctx.set_tuning(family)
+            if family == 0:
+                d.ctx.set_block_threads(threads)
+            d.syncto()
+            d.ctx.search(SYM, CONT, case.physics, 0)
+            d.ctx.step(warmup, case.physics)
+        for d in runs:
+            d.ctx.synchronize(raise_on_status=False)
+        t0 = time.perf_counter()
+        for d in runs:
+            d.ctx.step(steps, case.physics)
+        for d in runs:
+            d.ctx.synchronize(raise_on_status=False)
+        return 1e3 * (time.perf_counter() - t0) / (steps * copies)
+    finally:
+        for d in runs:
+            d.close()
+
+
+def tune_case(case, n_instances=1, inst=None, steps=20, device=0, timer=time_config, batch=None, concurrent=0):
     """Time every candidate on a fresh context holding `case`; returns (best, {cand: ms}).
-    `batch` restricts the candidates to those a batch can use (default: n_instances > 1)."""
+    `batch` restricts the candidates to those a batch can use (default: n_instances > 1);
+    `concurrent` > 1 times that many copies stepped together instead (time_concurrent)."""
     from .algorithm import DeviceParticleSystem
     from .classes import NeighbourSystem
     ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
     ms = {}
+    if concurrent > 1:
+        for fam, thr in candidates(False):
+            ms[(fam, thr)] = time_concurrent(case, fam, thr, concurrent, steps=steps, device=device)
+        return min(ms, key=ms.get), ms
     for fam, thr in candidates(n_instances > 1 if batch is None else batch):
         dps = DeviceParticleSystem(case.ps, ns, device=device, n_instances=n_instances)
         if inst is not None:
@@ -136,19 +181,20 @@ class Autotuner:
                 self._gpu = "gpu%d" % self.device
         return self._gpu
 
-    def best(self, dim, n, batch=False, case=None):
-        key = TuneCache.key(self.gpu, dim, n, batch)
+    def best(self, dim, n, batch=False, case=None, concurrent=0):
+        key = TuneCache.key(self.gpu, dim, n, batch, concurrent)
         hit = self.cache.get(key)
         if hit:
             return hit["family"], hit["threads"]
         case = case or representative_case(dim, n)
-        (fam, thr), ms = tune_case(case, steps=self.steps, device=self.device, batch=batch)
-        self.cache.put(key, {"family": fam, "threads": thr, "particles": case.n,
+        (fam, thr), ms = tune_case(case, steps=self.steps, device=self.device, batch=batch,
+                                   concurrent=0 if batch else concurrent)
+        self.cache.put(key, {"family": fam, "threads": thr, "particles": case.n, "copies": max(concurrent, 1),
                              "ms_per_step": {"%d/%d" % k: v for k, v in ms.items()}})
         return fam, thr
 
-    def apply(self, ctx, dim, n, batch=False):
-        fam, thr = self.best(dim, n, batch)
+    def apply(self, ctx, dim, n, batch=False, concurrent=0):
+        fam, thr = self.best(dim, n, batch, concurrent=concurrent)
         ctx.set_tuning(fam)
         ctx.set_block_threads(thr)
         return fam, thr

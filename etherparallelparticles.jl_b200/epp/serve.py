@@ -124,11 +124,12 @@ class Run:
 class DeviceBackend:
     """Runs each request on its own epp context (own stream) on one GPU."""
 
-    def __init__(self, device=0, download=False, priorities=True, tuner=None):
+    def __init__(self, device=0, download=False, priorities=True, tuner=None, tune_concurrent=True):
         self.device = device
         self.download = download
         self.priorities = priorities
         self.tuner = tuner        # autotune.Autotuner: launch configuration per dimension and size
+        self.tune_concurrent = tune_concurrent   # tune for throughput with several runs resident
 
     def _config(self, case):
         from .classes import NeighbourSystem
@@ -136,6 +137,11 @@ class DeviceBackend:
         adj = ns.active_pair.adjacency_matrix.tolist()
         return ns, abi.make_config(case.domain.to_abi(), case.ps.n_capacity, adj, max_neighbour_number=1,
                                    device=self.device)
+
+    def copies(self, n):
+        """Copies the tuner steps together for a run of n particles (0: tune one run alone)."""
+        from .autotune import concurrent_copies
+        return concurrent_copies(n) if self.tune_concurrent else 0
 
     def bytes_needed(self, case):
         from .lib import context_bytes
@@ -149,7 +155,7 @@ class DeviceBackend:
         if self.priorities:
             dps.ctx.set_priority(priority_for(case.n))
         if self.tuner is not None:
-            self.tuner.apply(dps.ctx, case.meta["dim"], case.n)
+            self.tuner.apply(dps.ctx, case.meta["dim"], case.n, concurrent=self.copies(case.n))
         dps.syncto()
         dps.ctx.search(SYM, CONT, case.physics, 0)
         return dps

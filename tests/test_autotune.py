@@ -35,6 +35,25 @@ def test_cache_roundtrip_and_reuse(tmp_path, monkeypatch):
     assert again.cache.get(key)["ms_per_step"]["4/128"] == 1.0
 
 
+def test_concurrent_mode_keys():
+    """Serving tunes for throughput with several runs resident: its own cache entries, and
+    fewer copies of large runs."""
+    assert autotune.TuneCache.key("B200", 2, 5000, False, 16).endswith("|concurrent16")
+    assert autotune.TuneCache.key("B200", 2, 5000, False, 1).endswith("|single")
+    assert autotune.TuneCache.key("B200", 2, 5000, True, 16).endswith("|batch")
+    assert autotune.concurrent_copies(3e4) == 16
+    assert autotune.concurrent_copies(1e6) == 4
+    assert autotune.concurrent_copies(1e8) == 1
+
+
+@pytest.mark.gpu
+def test_tune_concurrent_small_case():
+    case = casegen.dam_break_2d(dx=0.05, max_neighbour_number=1)
+    best, ms = autotune.tune_case(case, steps=3, concurrent=3)
+    assert best in autotune.candidates()
+    assert set(ms) == set(autotune.candidates()) and all(v > 0 for v in ms.values())
+
+
 @pytest.mark.gpu
 def test_block_threads_bit_identical():
     outs = []
