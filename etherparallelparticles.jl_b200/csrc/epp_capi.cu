@@ -849,6 +849,7 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     if ((D != 2 && D != 3) || cfg->n_capacity < 1 || cfg->n_tags < 1 || cfg->n_tags > EPP_MAX_TAGS ||
         !(cfg->domain.gap > 0.0f))
         return EPP_ERR_INVALID_ARGUMENT;
+    if (cfg->n_capacity > (1 << kEntryBits)) return EPP_ERR_CAPACITY;   // list entries hold 28-bit indices
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return EPP_ERR_NO_DEVICE;
     if (cfg->device < 0 || cfg->device >= ndev) return EPP_ERR_INVALID_ARGUMENT;
@@ -1431,6 +1432,7 @@ int32_t epp_context_bytes(const epp_config* cfg, int64_t* bytes) {
     if (!cfg || !bytes) return EPP_ERR_INVALID_ARGUMENT;
     const int D = cfg->domain.dim;
     if ((D != 2 && D != 3) || cfg->n_capacity < 1 || !(cfg->domain.gap > 0.0f)) return EPP_ERR_INVALID_ARGUMENT;
+    if (cfg->n_capacity > (1 << kEntryBits)) return EPP_ERR_CAPACITY;
     DevDomain d;
     long long ncell = 1;
     if (!plan_cells(cfg, d, ncell)) return EPP_ERR_INVALID_ARGUMENT;

@@ -97,6 +97,14 @@ struct TileConf {
     static constexpr int NRMAX = D == 2 ? 3 : 9;   // stencil rows: ranges of a tile or of one particle
 };
 
+// A neighbour-list entry carries the neighbour's sorted index in its low 28 bits and its tag - 1
+// in the top 4 (tags are 1..EPP_MAX_TAGS = 16), so the list passes get the tag with the index
+// instead of gathering it.  Contexts hold at most 2^28 particles.
+constexpr int kEntryBits = 28;
+__device__ __forceinline__ int list_entry(int j, int tag) { return j | ((tag - 1) << kEntryBits); }
+__device__ __forceinline__ int entry_index(int e) { return e & ((1 << kEntryBits) - 1); }
+__device__ __forceinline__ int entry_tag(int e) { return (int)((unsigned)e >> kEntryBits) + 1; }
+
 struct TileMask {
     int cap;
     int* list;   // [cap * LCAP]: row i holds the neighbours (sorted indices) of particle i in order
@@ -236,7 +244,7 @@ __device__ __forceinline__ int lane_stencil_list(const PairArgs& A, ListWriter<D
         for (int j = R.lo[r]; j < R.lo[r] + R.len[r]; ++j) {
             EPP_CHECK(j >= 0 && j < A.n_max, 14, j);
             if (!accept<D>(A, i, xi, amask, h2sq, j, A.s.xh[j], st)) continue;
-            L.put(cnt++, j);
+            L.put(cnt++, list_entry(j, tag_of(A.s.tagm[j])));
         }
     }
     return cnt;
@@ -308,7 +316,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                 s_p[wib][1][lane] = xn.y;
                 s_p[wib][2][lane] = xn.z;
                 s_p[wib][3][lane] = xn.w;
-                s_j[wib][lane] = jn;
+                s_j[wib][lane] = list_entry(jn, tn);   // appended as is (a real, allowed tag)
                 const int tj = tn;
                 const bool real_c = real;
                 if (__ballot_sync(0xffffffffu, real_c && (tj < 1 || tj > A.n_tags))) st |= EPP_STATUS_BAD_TAG;
@@ -388,9 +396,9 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                 while (word) {
                     const int b = __ffs(word) - 1;
                     word &= word - 1u;
-                    const int j = s_j[wib][b];
-                    if (j == i) continue;
-                    L.put(cnt++, j);
+                    const int e = s_j[wib][b];
+                    if (entry_index(e) == i) continue;
+                    L.put(cnt++, e);
                 }
                 __syncwarp();
             }
@@ -462,9 +470,10 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                 lr.start(M, i, cnt);
                 if (D == 2) {   // 2D: a second neighbour record in flight costs more than it hides
                     for (int k = 0; k < cnt; ++k) {
-                        const int j = lr.next(k);
-                        EPP_CHECK(j >= 0 && j < A.n_max, 16, j);
-                        const int tj = tag_of(A.s.tagm[j]);
+                        const int e = lr.next(k);
+                        const int j = entry_index(e);
+                        EPP_CHECK(j < A.n_max, 16, j);
+                        const int tj = entry_tag(e);
                         const float4 xj = A.s.xh[j];
                         const float4 t =
                             act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc);
@@ -476,19 +485,19 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                     return;
                 }
                 // 3D: software pipeline, neighbour k + 1's loads in flight while k's term runs
-                int jn = cnt > 0 ? lr.next(0) : 0;
-                EPP_CHECK(jn >= 0 && jn < A.n_max, 16, jn);
-                int tn = cnt > 0 ? A.s.tagm[jn] : 0;
+                int en = cnt > 0 ? lr.next(0) : list_entry(0, 1);
+                int jn = entry_index(en);
+                EPP_CHECK(jn < A.n_max, 16, jn);
                 float4 xn = cnt > 0 ? A.s.xh[jn] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 typename Act::Nb nn = act.fetch(jn, ti, 0);
                 for (int k = 0; k < cnt; ++k) {
-                    const int tj = tag_of(tn);
+                    const int tj = entry_tag(en);
                     const float4 xj = xn;
                     const typename Act::Nb nb = nn;
                     if (k + 1 < cnt) {
-                        jn = lr.next(k + 1);
-                        EPP_CHECK(jn >= 0 && jn < A.n_max, 16, jn);
-                        tn = A.s.tagm[jn];
+                        en = lr.next(k + 1);
+                        jn = entry_index(en);
+                        EPP_CHECK(jn < A.n_max, 16, jn);
                         xn = A.s.xh[jn];
                         nn = act.fetch(jn, ti, 0);
                     }

@@ -152,7 +152,7 @@ typedef struct epp_physics {
 
 typedef struct epp_config {
     epp_domain domain;
-    int32_t n_capacity;            /* rows of the property matrices */
+    int32_t n_capacity;            /* rows of the property matrices (at most 2^28: EPP_ERR_CAPACITY) */
     int32_t max_neighbour_number;  /* list capacity for EPP_SEARCH_EMIT_LIST (reference: 50) */
     int32_t max_cell_particles;    /* reference bucket capacity; only checked (0 = unchecked) */
     int32_t n_tags;                /* adjacency matrix is n_tags x n_tags, tags are 1-based */
