@@ -37,7 +37,7 @@ def test_library_loads_without_gpu():
     assert rc in (abi.EPP_OK, abi.EPP_ERR_NO_DEVICE)
 
 
-def test_struct_sizes_match_header():
+def test_struct_sizes_match_header(tmp_path):
     """Compile a tiny C probe against include/epp.h and compare sizeof/offsetof with ctypes."""
     src = r'''
 #include <stdio.h>
@@ -49,8 +49,7 @@ int main(void) {
   return 0;
 }
 '''
-    tmp = os.path.join(ROOT, "_work", "abi_probe")
-    os.makedirs(tmp, exist_ok=True)
+    tmp = str(tmp_path)
     with open(os.path.join(tmp, "p.c"), "w") as f:
         f.write(src)
     exe = os.path.join(tmp, "p")
@@ -71,3 +70,15 @@ def test_create_fails_loudly_without_gpu():
     cfg = abi.make_config(d, 10, [[1]])
     with pytest.raises(epplib.EppError):
         epplib.Context(cfg)
+
+
+def test_context_bytes_capacity_limit():
+    """epp_context_bytes is host arithmetic (no device): the footprint grows with the capacity,
+    and capacities above 2^28 are refused (neighbour-list entries hold 28-bit indices)."""
+    d = abi.make_domain(2, 0.006, [-0.02, -0.02], [4.02, 3.02])
+    small = epplib.context_bytes(abi.make_config(d, 100000, [[1, 1], [1, 0]]))
+    large = epplib.context_bytes(abi.make_config(d, 1000000, [[1, 1], [1, 0]]))
+    assert 0 < small < large
+    with pytest.raises(epplib.EppError) as e:
+        epplib.context_bytes(abi.make_config(d, (1 << 28) + 1, [[1, 1], [1, 0]]))
+    assert e.value.code == abi.EPP_ERR_CAPACITY
