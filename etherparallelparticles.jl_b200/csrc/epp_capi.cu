@@ -139,6 +139,12 @@ struct epp_ctx {
     epp_physics graph_phys{};
     bool graph_accel = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // epp_integrals_async: pinned host slots (8 results + n_alive each), their events and tickets
+    double* ihost = nullptr;
+    cudaEvent_t iev[EPP_INTEGRALS_SLOTS]{};
+    long long iticket_next = 0;
+    long long islot_ticket[EPP_INTEGRALS_SLOTS]{-1, -1, -1, -1};
+    float islot_c0[EPP_INTEGRALS_SLOTS]{};
     bool timed = false;
     std::string err;
 };
@@ -978,6 +984,9 @@ int32_t epp_destroy(epp_ctx* ctx) {
     dev_free(ctx, ctx->arena.base);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (int k = 0; k < EPP_INTEGRALS_SLOTS; ++k)
+        if (ctx->iev[k]) cudaEventDestroy(ctx->iev[k]);
+    if (ctx->ihost) cudaFreeHost(ctx->ihost);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return EPP_OK;
@@ -1262,12 +1271,10 @@ int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys) {
     return EPP_OK;
 }
 
-int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out) {
-    if (!ctx || !phys || !out) return EPP_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->dev);
-    std::memset(out, 0, sizeof *out);
-    if (ctx->n == 0) return EPP_OK;
-    if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
+namespace {
+
+// k_integrals on the context's stream: the 8 results land in ctx->iresult.
+int launch_integrals(epp_ctx* ctx, const epp_physics* phys) {
     IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket};
     DevPhys P = dev_phys(ctx, *phys);
     auto launch = [&](auto Dt) {
@@ -1280,21 +1287,83 @@ int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* 
     if (ctx->D == 2) launch(std::integral_constant<int, 2>{});
     else launch(std::integral_constant<int, 3>{});
     CK_LAUNCH();
-    double r[8];
-    int n_alive = 0;
-    CK(cudaMemcpyAsync(r, ctx->iresult, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(&n_alive, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
-                       ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    return EPP_OK;
+}
+
+void fill_integrals(epp_integrals* out, const double* r, int n_alive, float c0) {
     out->mass_total = r[0];
     out->mass_fluid = r[1];
     out->kinetic = r[2];
     out->potential = r[3];
     out->internal = r[4];
     out->max_speed = r[5];
-    out->cfl_dt = r[6] < 1e300 ? 0.1 * r[6] / ((double)phys->c0 + r[5]) : 0.0;
+    out->cfl_dt = r[6] < 1e300 ? 0.1 * r[6] / ((double)c0 + r[5]) : 0.0;
     out->n_alive = n_alive;
     out->n_pairs = (int64_t)r[7];   // directed pairs of the last search = sum of nCount over alive particles
+}
+
+}  // namespace
+
+int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out) {
+    if (!ctx || !phys || !out) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    std::memset(out, 0, sizeof *out);
+    if (ctx->n == 0) return EPP_OK;
+    if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
+    if (const int rc = launch_integrals(ctx, phys)) return rc;
+    double r[8];
+    int n_alive = 0;
+    CK(cudaMemcpyAsync(r, ctx->iresult, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&n_alive, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    fill_integrals(out, r, n_alive, phys->c0);
+    return EPP_OK;
+}
+
+int32_t epp_integrals_async(epp_ctx* ctx, const epp_physics* phys, int64_t* ticket) {
+    if (!ctx || !phys || !ticket) return EPP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->dev);
+    if (ctx->n > 0 && !ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
+    const long long t = ctx->iticket_next;
+    const int slot = (int)(t % EPP_INTEGRALS_SLOTS);
+    if (ctx->islot_ticket[slot] >= 0)
+        return fail(ctx, EPP_ERR_STATE, "%d integrals tickets outstanding: wait for one first", EPP_INTEGRALS_SLOTS);
+    if (!ctx->ihost) {   // pinned slots on first use (the copies below then run asynchronously)
+        CK(cudaMallocHost(reinterpret_cast<void**>(&ctx->ihost), sizeof(double) * 9 * EPP_INTEGRALS_SLOTS));
+        for (int k = 0; k < EPP_INTEGRALS_SLOTS; ++k) CK(cudaEventCreateWithFlags(&ctx->iev[k], cudaEventDisableTiming));
+    }
+    double* h = ctx->ihost + 9 * slot;
+    if (ctx->n == 0) {
+        for (int k = 0; k < 9; ++k) h[k] = 0.0;
+        h[6] = 1e300;
+    } else {
+        if (const int rc = launch_integrals(ctx, phys)) return rc;
+        CK(cudaMemcpyAsync(h, ctx->iresult, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(h + 8, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->iev[slot], ctx->stream));
+    ctx->islot_ticket[slot] = t;
+    ctx->islot_c0[slot] = phys->c0;
+    ctx->iticket_next = t + 1;
+    *ticket = t;
+    return EPP_OK;
+}
+
+int32_t epp_integrals_wait(epp_ctx* ctx, int64_t ticket, epp_integrals* out) {
+    if (!ctx || !out) return EPP_ERR_INVALID_ARGUMENT;
+    const int slot = ticket >= 0 ? (int)(ticket % EPP_INTEGRALS_SLOTS) : 0;
+    if (ticket < 0 || ctx->islot_ticket[slot] != ticket)
+        return fail(ctx, EPP_ERR_STATE, "integrals ticket %lld is not outstanding", (long long)ticket);
+    cudaSetDevice(ctx->dev);
+    CK(cudaEventSynchronize(ctx->iev[slot]));
+    const double* h = ctx->ihost + 9 * slot;
+    int n_alive = 0;
+    std::memcpy(&n_alive, h + 8, sizeof n_alive);
+    std::memset(out, 0, sizeof *out);
+    fill_integrals(out, h, n_alive, ctx->islot_c0[slot]);
+    ctx->islot_ticket[slot] = -1;
     return EPP_OK;
 }
 

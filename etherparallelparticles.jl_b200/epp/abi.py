@@ -61,6 +61,7 @@ EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF = 10
 
 EPP_SEARCH_EMIT_LIST = 1
 
+EPP_INTEGRALS_SLOTS = 4
 EPP_PROFILE_STAGES = 6   # momentum+integrate+bin, scan, scatter, rank+gather, search, continuity
 
 EPP_VISCOSITY_REFERENCE = 0

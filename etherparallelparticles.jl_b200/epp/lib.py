@@ -19,7 +19,7 @@ EXPORTS = [
     "epp_pairs_total", "epp_set_accel_output", "epp_get_accel", "epp_set_stream",
     "epp_profile_step", "epp_set_tuning", "epp_cell_sort_noalloc", "epp_noalloc_limits",
     "epp_set_instance_physics", "epp_get_instance_integrals", "epp_context_bytes", "epp_query",
-    "epp_set_priority", "epp_set_block_threads",
+    "epp_set_priority", "epp_set_block_threads", "epp_integrals_async", "epp_integrals_wait",
 ]
 
 
@@ -68,6 +68,8 @@ def load(path=LIB_PATH):
     lib.epp_selfaction.argtypes = [ctx, C.c_int32, P(abi.epp_physics)]
     lib.epp_step.argtypes = [ctx, C.c_int32, P(abi.epp_physics)]
     lib.epp_get_integrals.argtypes = [ctx, P(abi.epp_physics), P(abi.epp_integrals)]
+    lib.epp_integrals_async.argtypes = [ctx, P(abi.epp_physics), P(C.c_int64)]
+    lib.epp_integrals_wait.argtypes = [ctx, C.c_int64, P(abi.epp_integrals)]
     lib.epp_cell_stats.argtypes = [ctx, i32p, i32p, i32p, i32p]
     lib.epp_synchronize.argtypes = [ctx, P(C.c_uint32)]
     lib.epp_last_step_timing.argtypes = [ctx, f32p]
@@ -159,6 +161,17 @@ class Context:
     def integrals(self, phys):
         out = abi.epp_integrals()
         self._ck(self.lib.epp_get_integrals(self.h, C.byref(phys), C.byref(out)), "epp_get_integrals")
+        return out.as_dict()
+
+    def integrals_async(self, phys):
+        """Enqueue the integrals of the current state; returns a ticket for integrals_wait."""
+        t = C.c_int64(-1)
+        self._ck(self.lib.epp_integrals_async(self.h, C.byref(phys), C.byref(t)), "epp_integrals_async")
+        return t.value
+
+    def integrals_wait(self, ticket):
+        out = abi.epp_integrals()
+        self._ck(self.lib.epp_integrals_wait(self.h, C.c_int64(ticket), C.byref(out)), "epp_integrals_wait")
         return out.as_dict()
 
     def cell_stats(self):

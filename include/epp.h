@@ -220,12 +220,21 @@ int32_t epp_interaction(epp_ctx* ctx, int32_t action, const epp_physics* phys);
 int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys);
 
 /* The whole dam-break time step of main.jl:166-182 (density update, momentum,
- * integrate, search + continuity), fused into 5 kernels and replayed as a CUDA graph.
+ * integrate, search + continuity), fused into 6 kernels and replayed as a CUDA graph.
  * Requires one prior epp_search with EPP_ACTION_DAMBREAK_CONTINUITY (main.jl:157-164). */
 int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys);
 
 /* FP64 reductions of the current state. */
 int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out);
+
+/* The same reductions without blocking: epp_integrals_async enqueues them for the current state
+ * on the context's stream (their copy to the host included) and returns a ticket;
+ * epp_integrals_wait(ticket) waits for that point of the stream and fills `out`.  Work queued in
+ * between (the next epp_step) runs meanwhile.  At most EPP_INTEGRALS_SLOTS tickets may be
+ * outstanding (EPP_ERR_STATE beyond). */
+#define EPP_INTEGRALS_SLOTS 4
+int32_t epp_integrals_async(epp_ctx* ctx, const epp_physics* phys, int64_t* ticket);
+int32_t epp_integrals_wait(epp_ctx* ctx, int64_t ticket, epp_integrals* out);
 
 /* Parity access to the cell list: counts[n_cells] per cell, offsets[n_cells+1] exclusive
  * scan, sorted_ids[n_alive] 1-based particle ids in cell order (within a cell by id).

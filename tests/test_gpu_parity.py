@@ -324,6 +324,38 @@ def test_integrals_fp64():
     assert abs(gi["kinetic"] - oi["kinetic"]) <= 1e-4 * abs(oi["kinetic"]) + 1e-12
 
 
+def test_integrals_async_matches_blocking():
+    """epp_integrals_async / _wait give the blocking call's values while the next step runs;
+    at most EPP_INTEGRALS_SLOTS tickets are outstanding and a ticket is waited for once."""
+    from epp.lib import EppError
+    case = make_case(2, 0.04)
+    dps, _ = pair(case, 40)
+    phys = case.physics
+    c = dps.ctx
+    c.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    expect, tickets = [], []
+    for _ in range(3):
+        c.step(1, phys)
+        expect.append(c.integrals(phys))
+    fresh = make_case(2, 0.04)
+    d2, _ = pair(fresh, 40)
+    d2.ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    for _ in range(3):
+        d2.ctx.step(1, phys)
+        tickets.append(d2.ctx.integrals_async(phys))   # the next step is queued before the wait
+    got = [d2.ctx.integrals_wait(t) for t in tickets]
+    assert got == expect
+    with pytest.raises(EppError) as e:
+        d2.ctx.integrals_wait(tickets[0])
+    assert e.value.code == abi.EPP_ERR_STATE
+    more = [d2.ctx.integrals_async(phys) for _ in range(abi.EPP_INTEGRALS_SLOTS)]
+    with pytest.raises(EppError) as e:
+        d2.ctx.integrals_async(phys)
+    assert e.value.code == abi.EPP_ERR_STATE
+    for t in more:
+        d2.ctx.integrals_wait(t)
+
+
 def test_out_of_domain_killed():
     """NeighbourSearch.jl:41-43: particles outside the domain are killed (is_alive = 0, cell 0)."""
     case = make_case(2, 0.04)
