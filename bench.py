@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--instances", type=int, default=256, help="batch: number of instances")
     ap.add_argument("--requests", type=int, default=32, help="serve: number of requests in the stream")
     ap.add_argument("--sim-steps", type=int, default=2000, help="serve: steps per request")
+    ap.add_argument("--no-co-batch", dest="co_batch", action="store_false",
+                    help="serve: give every request its own context (no co-batching of waiting requests)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batch / serve: skip the launch-configuration autotuner (serve)")
     ap.add_argument("--mix", default="stream", choices=["stream", "batch"],
@@ -484,7 +486,7 @@ def run_serve(args):
     rk.barrier()
     clocks = Clocks(rk.local)
     clocks.start()
-    st = serve.Server(be, budget_bytes=120 * 10**9).run(runs)
+    st = serve.Server(be, budget_bytes=120 * 10**9, co_batch=args.co_batch).run(runs)
     clk = clocks.stop()
     plain_runs = serve.make_runs(mine, be)
     rk.barrier()
@@ -528,6 +530,7 @@ def run_serve(args):
                       "requests_3d": sum(1 for s in specs if s.dim == 3),
                       "particles_total": int(sum(n_all)), "particles_range": [min(n_all), max(n_all)],
                       "hbm_budget_bytes_per_gpu": 120 * 10**9, "chunk_steps": 100,
+                      "co_batching": bool(args.co_batch),
                       "parallelism": ("requests split over %d GPUs by expected work" % rk.world) if rk.world > 1
                       else "single GPU"},
            "latency_p50_s": served["latency_p50_s"], "latency_p99_s": served["latency_p99_s"],

@@ -193,6 +193,11 @@ class Autotuner:
                              "ms_per_step": {"%d/%d" % k: v for k, v in ms.items()}})
         return fam, thr
 
+    def cached(self, dim, n, batch=False, concurrent=0):
+        """The cached choice, or None (never tunes)."""
+        hit = self.cache.get(TuneCache.key(self.gpu, dim, n, batch, concurrent))
+        return (hit["family"], hit["threads"]) if hit else None
+
     def apply(self, ctx, dim, n, batch=False, concurrent=0):
         fam, thr = self.best(dim, n, batch, concurrent=concurrent)
         ctx.set_tuning(fam)

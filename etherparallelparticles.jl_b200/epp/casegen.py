@@ -310,5 +310,49 @@ def dam_break_batch(n_instances=256, seed=0, dx=0.01, tank=(4.0, 3.0), width=(0.
                      rows)
 
 
+def batch_key(case):
+    """Cases with equal keys can run as instances of one batch: 2D, the same domain (cell grid)
+    and neighbour capacity, and the same physics except each instance's dt and c0."""
+    if case.meta.get("dim") != 2 or isinstance(case, BatchCase):
+        return None
+    d = case.domain
+    p = case.physics
+    phys = tuple((f, repr(getattr(p, f)[:] if hasattr(getattr(p, f), "__len__") else getattr(p, f)))
+                 for f, _ in p._fields_ if f not in ("dt", "c0"))
+    nb = case.ps.named_index.int_table.capacity["nIndex"]
+    return (2, float(d.gap), tuple(float(v) for v in d.first), tuple(float(v) for v in d.last), nb, phys)
+
+
+def merge_cases(cases):
+    """One BatchCase holding `cases` (equal batch_key) as instances 0..K-1, in order: every
+    particle column copied, an Instance column added, each instance keeping its own dt and c0."""
+    if not cases:
+        raise ValueError("no cases")
+    key = batch_key(cases[0])
+    if key is None or any(batch_key(c) != key for c in cases):
+        raise ValueError("cases differ in domain or physics: they cannot share a batch")
+    first = cases[0]
+    nb = first.ps.named_index.int_table.capacity["nIndex"]
+    ints, floats = _layout(2, nb, instance=True)
+    rows, total = [], 0
+    for c in cases:
+        rows.append((total, total + c.n))
+        total += c.n
+    ps = ParticleSystem(first.domain, total, ints, floats, OrderedDict(first.ps.basic_parameters))
+    for name in list(ints) + list(floats):
+        if name == "Instance":
+            continue
+        ps[name] = np.concatenate([c.ps[name] for c in cases])
+    ps["Instance"] = np.concatenate([np.full(c.n, k, np.int32) for k, c in enumerate(cases)])
+    meta = dict(first.meta)
+    meta.update({"n": total, "n_fluid": int(sum(c.meta["n_fluid"] for c in cases)),
+                 "n_wall": int(sum(c.meta["n_wall"] for c in cases)),
+                 "inst_n_fluid": [c.meta["n_fluid"] for c in cases],
+                 "n_cells": first.domain.get_n() * len(cases)})
+    return BatchCase(ps, first.domain, first.physics, meta,
+                     np.array([c.physics.dt for c in cases], np.float32),
+                     np.array([c.physics.c0 for c in cases], np.float32), rows)
+
+
 # active pairs of casegen.jl:137: fluid-fluid, fluid-wall, wall-fluid
 DAM_BREAK_ACTIVE_PAIRS = [(FLUID_TAG, FLUID_TAG), (FLUID_TAG, WALL_TAG), (WALL_TAG, FLUID_TAG)]

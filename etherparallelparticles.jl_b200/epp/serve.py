@@ -17,7 +17,10 @@ small run is bound by launch latency, a large one fills the SMs.  The host loop
   stream-ordered allocator returns its memory without synchronising the device).
 
 Each request runs on its own context with the plain path's kernels and graphs, so its result is
-the same whether it runs alone or in the mix.
+the same whether it runs alone or in the mix.  With co-batching, requests that wait together and
+can share a cell grid and physics (2D, same tank and lattice spacing, same step count; dt and c0
+may differ) are admitted as the instances of one batch context, so their steps run as one launch
+per pass; an instance gives the same bits in a batch as alone.
 
 The device calls go through a backend object, so the admission and accounting logic also runs
 against a simulated backend on the CPU (tests).
@@ -105,20 +108,40 @@ def priority_for(n_particles):
 class Run:
     """Server-side record of one request."""
 
-    def __init__(self, spec, case, nbytes):
+    def __init__(self, spec, case, nbytes, group_key=None):
         self.spec = spec
         self.case = case
         self.bytes = nbytes
+        self.group_key = group_key   # equal keys (and step counts) may share one batch context
         self.handle = None
         self.queued = 0          # steps enqueued on the device
         self.admitted = None     # seconds after start
         self.done = None
         self.result = None
         self.error = None
+        self.runs = [self]       # the requests this resident unit serves
+
+    @property
+    def steps(self):
+        return self.spec.steps
 
     @property
     def latency(self):
         return None if self.done is None else self.done - self.spec.arrival
+
+
+class Group:
+    """Requests co-batched into one batch context: resident, stepped and retired together."""
+
+    def __init__(self, runs):
+        self.runs = runs
+        self.bytes = sum(r.bytes for r in runs)   # a batch needs at most its instances' sum
+        self.handle = None
+        self.queued = 0
+
+    @property
+    def steps(self):
+        return self.runs[0].spec.steps
 
 
 class DeviceBackend:
@@ -160,6 +183,39 @@ class DeviceBackend:
         dps.ctx.search(SYM, CONT, case.physics, 0)
         return dps
 
+    def group_key(self, case):
+        return casegen.batch_key(case)
+
+    def admit_group(self, cases):
+        """One batch context holding `cases` as instances 0..K-1 (casegen.merge_cases)."""
+        from .algorithm import DeviceParticleSystem
+        b = casegen.merge_cases(cases)
+        ns, _ = self._config(b)
+        dps = DeviceParticleSystem(b.ps, ns, device=self.device, n_instances=b.n_instances)
+        dps.physics = b.physics
+        dps.batch = b
+        dps.ctx.set_instance_physics(b.inst_dt, b.inst_c0)
+        if self.priorities:
+            dps.ctx.set_priority(priority_for(b.n))
+        best = self.tuner.cached(2, b.n, batch=True) if self.tuner is not None else None
+        if best is not None:   # batches run family 0; a block size is used only if already tuned
+            dps.ctx.set_block_threads(best[1])
+        dps.syncto()
+        dps.ctx.search(SYM, CONT, b.physics, 0)
+        return dps
+
+    def finish_group(self, dps, k):
+        st = dps.ctx.synchronize(raise_on_status=False)
+        integ = dps.ctx.instance_integrals(dps.physics, k)
+        out = [{"integrals": integ[i], "status": st} for i in range(k)]
+        if self.download:
+            dps.asyncto()
+            h = dps.host
+            for i, (a, e) in enumerate(dps.batch.rows):
+                out[i]["state"] = {c: h[c][a:e] for c in ("PositionVec", "VelocityVec", "Density", "Pressure", "nCount")}
+        dps.close()
+        return out
+
     def enqueue(self, dps, n_steps):
         dps.ctx.step(n_steps, dps.physics)
 
@@ -185,8 +241,10 @@ class Server:
     chunk, ahead: steps per enqueue and chunks kept queued on a stream."""
 
     def __init__(self, backend, budget_bytes=120 * 10**9, max_active=256, chunk=100, ahead=2,
-                 clock=time.perf_counter, idle_wait=50e-6):
+                 clock=time.perf_counter, idle_wait=50e-6, co_batch=False, batch_max=256):
         self.backend = backend
+        self.co_batch = co_batch      # admit waiting requests with equal group keys as one batch
+        self.batch_max = batch_max
         self.budget = int(budget_bytes)
         self.max_active = max_active
         self.chunk = chunk
@@ -200,15 +258,16 @@ class Server:
         now = lambda: self.clock() - t0  # noqa: E731
         arrivals = collections.deque(sorted(runs, key=lambda r: r.spec.arrival))
         waiting = collections.deque()
-        active = []
+        active = []              # resident units: Run, or Group of co-batched runs
         used = peak = 0
         max_conc = 0
+        n_res = 0                # resident requests
         while arrivals or waiting or active:
             t = now()
             while arrivals and arrivals[0].spec.arrival <= t:
                 waiting.append(arrivals.popleft())
             # FIFO admission while the head fits the budget and a slot is free
-            while waiting and len(active) < self.max_active:
+            while waiting and n_res < self.max_active:
                 r = waiting[0]
                 if r.bytes > self.budget:          # can never fit: reject, keep serving the rest
                     waiting.popleft()
@@ -218,25 +277,51 @@ class Server:
                 if used + r.bytes > self.budget:
                     break
                 waiting.popleft()
-                r.handle = self.backend.admit(r.case)
-                r.admitted = now()
-                used += r.bytes
+                members = [r]
+                if self.co_batch and r.group_key is not None:
+                    # the waiting requests that can share the head's batch, in arrival order
+                    room = self.budget - used - r.bytes
+                    for w in list(waiting):
+                        if len(members) >= min(self.batch_max, self.max_active - n_res):
+                            break
+                        if w.group_key == r.group_key and w.spec.steps == r.spec.steps and w.bytes <= room:
+                            members.append(w)
+                            waiting.remove(w)
+                            room -= w.bytes
+                if len(members) == 1:
+                    unit = r
+                    r.handle = self.backend.admit(r.case)
+                else:
+                    unit = Group(members)
+                    unit.handle = self.backend.admit_group([m.case for m in members])
+                t_adm = now()
+                for m in members:
+                    m.admitted = t_adm
+                used += unit.bytes
                 peak = max(peak, used)
-                active.append(r)
-                self._fill(r)
-            max_conc = max(max_conc, len(active))
+                n_res += len(members)
+                active.append(unit)
+                self._fill(unit)
+            max_conc = max(max_conc, n_res)
             progressed = False
             for r in list(active):
                 if not self.backend.idle(r.handle):
                     continue
                 progressed = True
-                if r.queued < r.spec.steps:
+                if r.queued < r.steps:
                     self._fill(r)
                     continue
-                r.result = self.backend.finish(r.handle)
+                if isinstance(r, Group):
+                    results = self.backend.finish_group(r.handle, len(r.runs))
+                else:
+                    results = [self.backend.finish(r.handle)]
+                t_done = now()
+                for m, res in zip(r.runs, results):
+                    m.result = res
+                    m.done = t_done
                 r.handle = None
-                r.done = now()
                 used -= r.bytes
+                n_res -= len(r.runs)
                 active.remove(r)
             if not progressed:
                 if not active and not waiting and arrivals:
@@ -247,7 +332,7 @@ class Server:
         return self.stats(runs, makespan, peak, max_conc)
 
     def _fill(self, r):
-        n = min(self.chunk * self.ahead, r.spec.steps - r.queued)
+        n = min(self.chunk * self.ahead, r.steps - r.queued)
         if n > 0:
             self.backend.enqueue(r.handle, n)
             r.queued += n
@@ -269,9 +354,11 @@ class Server:
 
 
 def make_runs(specs, backend):
-    """Build each request's case and its device footprint (before the clock starts)."""
+    """Build each request's case, its device footprint and its batch key (before the clock
+    starts)."""
     runs = []
     for s in specs:
         case = s.case()
-        runs.append(Run(s, case, backend.bytes_needed(case)))
+        key = backend.group_key(case) if hasattr(backend, "group_key") else None
+        runs.append(Run(s, case, backend.bytes_needed(case), key))
     return runs

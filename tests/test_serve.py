@@ -25,8 +25,9 @@ class TickClock:
 
 
 class FakeCase:
-    def __init__(self, n):
+    def __init__(self, n, key=None):
         self.n = n
+        self.key = key
 
 
 class FakeHandle:
@@ -62,12 +63,28 @@ class FakeBackend:
     def finish(self, h):
         return {"n": h.case.n}
 
+    def group_key(self, case):
+        return case.key
 
-def fake_runs(sizes, arrivals, steps=100):
+    def admit_group(self, cases):
+        self.admitted.append(tuple(c.n for c in cases))
+        h = FakeHandle(FakeCase(sum(c.n for c in cases)))
+        h.members = cases
+        h.busy_until = self.clock.t
+        return h
+
+    def finish_group(self, h, k):
+        assert k == len(h.members)
+        return [{"n": c.n, "batch": len(h.members)} for c in h.members]
+
+
+def fake_runs(sizes, arrivals, steps=100, keys=None):
     runs = []
     for i, (n, t) in enumerate(zip(sizes, arrivals)):
-        spec = serve.RequestSpec(i, t, 2, n, 1.0, steps)
-        runs.append(serve.Run(spec, FakeCase(n), n * 1000))
+        st = steps[i] if isinstance(steps, list) else steps
+        k = keys[i] if keys else None
+        spec = serve.RequestSpec(i, t, 2, n, 1.0, st)
+        runs.append(serve.Run(spec, FakeCase(n, k), n * 1000, k))
     return runs
 
 
@@ -129,6 +146,38 @@ def test_one_at_a_time_is_sequential_and_slower():
     assert abs(st2["latency_p50_s"] - float(np.percentile(lat, 50))) < 1e-12
 
 
+def test_co_batching_groups_waiting_requests():
+    """Waiting requests with equal keys and step counts are admitted as one batch (budget and
+    max_active respected); others run alone; every member gets its own result."""
+    clock = TickClock()
+    be = FakeBackend(clock)
+    sizes = [1000, 2000, 3000, 4000, 5000, 6000, 7000]
+    keys = ["a", "a", "b", "a", None, "a", "a"]
+    steps = [100, 100, 100, 100, 100, 50, 100]
+    runs = fake_runs(sizes, [0.0] * len(sizes), steps=steps, keys=keys)
+    st = serve.Server(be, clock=clock, idle_wait=0.0, co_batch=True).run(runs)
+    assert st["completed"] == len(sizes)
+    # the head "a" takes every waiting "a" with 100 steps; the 50-step "a" runs alone
+    assert be.admitted[0] == (1000, 2000, 4000, 7000)
+    assert [getattr(c, "n", c) for c in be.admitted[1:]] == [3000, 5000, 6000]
+    for r in runs:
+        assert r.result["n"] == r.spec.n_fluid
+    grouped = [runs[i] for i in (0, 1, 3, 6)]
+    assert len({r.done for r in grouped}) == 1 and all(r.result["batch"] == 4 for r in grouped)
+    # a budget that holds two of them: the group stops growing at the budget
+    clock2 = TickClock()
+    be2 = FakeBackend(clock2)
+    runs2 = fake_runs([1000, 1000, 1000], [0.0] * 3, keys=["a"] * 3)
+    st2 = serve.Server(be2, budget_bytes=2000 * 1000, clock=clock2, idle_wait=0.0, co_batch=True).run(runs2)
+    assert st2["completed"] == 3 and st2["peak_resident_bytes"] <= 2000 * 1000
+    assert be2.admitted[0] == (1000, 1000)
+    # without co-batching nothing is grouped
+    clock3 = TickClock()
+    be3 = FakeBackend(clock3)
+    serve.Server(be3, clock=clock3, idle_wait=0.0).run(fake_runs([1000, 1000], [0.0, 0.0], keys=["a", "a"]))
+    assert all(not isinstance(c, tuple) for c in be3.admitted)
+
+
 # ---------------------------------------------------------------------------- device (GPU)
 
 def _small_stream(n=6, steps=200, seed=1):
@@ -165,3 +214,27 @@ def test_budget_limits_resident_runs():
     st = serve.Server(be, budget_bytes=budget, chunk=50).run(runs)
     assert st["completed"] == len(specs) and st["rejected"] == 0
     assert st["peak_resident_bytes"] <= budget
+
+
+@pytest.mark.gpu
+def test_co_batched_results_equal_alone():
+    """Requests of the 256-instance mix served co-batched (one batch context) give each
+    instance's state bit-identical to that request run alone; its FP64 integrals agree to the
+    rounding of the per-instance reduction order (1e-12)."""
+    specs = serve.batch_mix_requests(6, steps=60)
+    be = serve.DeviceBackend(download=True)
+    runs = serve.make_runs(specs, be)
+    assert len({r.group_key for r in runs}) == 1
+    st = serve.Server(be, chunk=20, co_batch=True).run(runs)
+    assert st["completed"] == len(specs)
+    assert len({r.done for r in runs}) == 1          # one batch
+    for r in runs:
+        alone = serve.DeviceBackend(download=True)
+        h = alone.admit(r.spec.case())
+        alone.enqueue(h, r.spec.steps)
+        res = alone.finish(h)
+        for k, v in res["state"].items():
+            assert np.array_equal(r.result["state"][k], v), (r.spec.rid, k)
+        assert r.result["integrals"]["n_pairs"] == res["integrals"]["n_pairs"]
+        for k in ("mass_total", "kinetic", "potential", "internal"):
+            assert abs(r.result["integrals"][k] - res["integrals"][k]) <= 1e-12 * abs(res["integrals"][k]), (r.spec.rid, k)
