@@ -145,8 +145,9 @@ class Clocks:
                 "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml, 2 ms poll"}
 
 
-def cpu_reference(case, steps_budget_s=20.0, max_steps=3):
-    """The oracle (C++ restatement of the reference's CPU algorithm) on all host cores."""
+def cpu_reference(case, steps_budget_s=20.0, max_steps=3, warmup=0):
+    """The oracle (C++ restatement of the reference's CPU algorithm) on all host cores, after
+    `warmup` untimed steps."""
     from epp import abi
     from epp.classes import NeighbourSystem
     from epp import casegen
@@ -162,6 +163,8 @@ def cpu_reference(case, steps_budget_s=20.0, max_steps=3):
     cm = ps.column_map()
     o.upload(ps.n_particles, ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, cm)
     o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys)
+    if warmup:
+        o.step(warmup, phys)
     pairs, t_total, steps = 0, 0.0, 0
     while steps < max_steps and (steps == 0 or t_total < steps_budget_s):
         t0 = time.perf_counter()
@@ -187,10 +190,11 @@ def run_reference(args):
     case.meta["label"] = label
     probe = cpu_reference(case, steps_budget_s=0.0, max_steps=1)      # cost of one step
     k = max(1, min(args.steps, int(120.0 / max(probe["seconds_per_step"], 1e-3))))
-    res = cpu_reference(case, steps_budget_s=150.0, max_steps=k)
+    w = max(0, min(args.warmup, int(30.0 / max(probe["seconds_per_step"], 1e-3))))
+    res = cpu_reference(case, steps_budget_s=150.0, max_steps=k, warmup=w)
     val = res["value"]
     out = {"metric": "SPH pair-interactions/s", "value": val, "unit": "pair-interactions/s",
-           "impl": "reference", "n_gpus": args.gpus, "steps": k, "warmup": 1,
+           "impl": "reference", "n_gpus": args.gpus, "steps": k, "warmup": w,
            "ms_per_step": res["seconds_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (dam-break lattice generated in-process)",
            "config": {"workload": label, "particles": case.n},
