@@ -707,6 +707,11 @@ def main():
                 out["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
             except Exception as exc:  # reported, not fatal
                 out["cpu_baseline"] = {"value": None, "error": str(exc)}
+            try:   # 2D: this workload; 3D: the dx = 0.01 block (the FP64 oracle at 6.2M particles is slow)
+                dcase = make_case(args.case, args.physics)[0] if dim == 2 else casegen.dam_break_3d(dx=0.01, max_neighbour_number=1)
+                out["energy_drift"] = energy_drift_fp64(dcase, 20 if dim == 2 else 10, device=local)
+            except Exception as exc:
+                out["energy_drift"] = {"error": str(exc)}
         print(json.dumps(out))
     dps.close()
     if world > 1:
@@ -762,6 +767,40 @@ def compute_roof(tr_case, stage, fp32_peak, clk):
                              "warp_inst_per_launch": e["warp_inst_per_launch"],
                              "issue_frac": e["warp_inst_per_launch"] / (ms * 1e-3) / issue_peak}
     return out
+
+
+def energy_drift_fp64(case, steps, device=0):
+    """North-star check on this workload: relative energy drift (kinetic + potential + internal,
+    FP64 integrals) over `steps` fused steps, the FP32 CUDA path against the FP64 oracle from the
+    same initial state; the bar is |drift_gpu - drift_fp64| <= 1e-4."""
+    from epp import abi, casegen
+    from epp.algorithm import DeviceParticleSystem
+    from epp.classes import NeighbourSystem
+    import oracle_lib
+    from helpers import config_for
+    SYM, CONT = abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY
+    phys = case.physics
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    d = DeviceParticleSystem(case.ps, ns, device=device)
+    d.syncto()
+    d.ctx.search(SYM, CONT, phys, 0)
+    g0 = energy(d.ctx.integrals(phys))
+    d.ctx.step(steps, phys)
+    g1 = energy(d.ctx.integrals(phys))
+    d.close()
+    dim = case.meta["dim"]
+    nso = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=40 if dim == 2 else 100)
+    oracle_lib.set_threads(os.cpu_count() or 1)
+    o = oracle_lib.Oracle(config_for(case.ps, nso, max_cell_particles=64 if dim == 2 else 128), 64)
+    q = case.ps
+    o.upload(q.n_particles, q.is_alive, q.cell_index, q.int_properties, q.float_properties, q.column_map())
+    o.search(SYM, CONT, phys)
+    o0 = energy(o.integrals(phys))
+    o.step(steps, phys)
+    o1 = energy(o.integrals(phys))
+    dg, do = (g1 - g0) / abs(g0), (o1 - o0) / abs(o0)
+    return {"steps": steps, "particles": case.n, "gpu_fp32": dg, "oracle_fp64": do, "abs_diff": abs(dg - do),
+            "bar": 1e-4, "within_bar": abs(dg - do) <= 1e-4}
 
 
 def run_e2e(dps, case, args, stream):

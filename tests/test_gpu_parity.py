@@ -396,3 +396,49 @@ def test_empty_and_state_errors():
     dps.ctx.synchronize()
     with pytest.raises(EppError):
         dps.ctx.search(7, abi.EPP_ACTION_NONE, case.physics, 0)
+
+
+@pytest.mark.parametrize("dim,h_factor,max_nb", [(2, 3.0, 160), (3, 2.0, 400)])
+def test_dense_neighbourhoods_beyond_list_capacity(dim, h_factor, max_nb):
+    """Smoothing lengths large enough that particles have more neighbours than a list keeps
+    (64 in 2D, 160 in 3D): the search still counts them all (nCount exact), and the pair passes
+    take those particles' neighbours from their own stencil, in the same order; the fused step
+    stays with the oracle stage by stage."""
+    if dim == 2:
+        case = casegen.dam_break_2d(dx=0.04, h_factor=h_factor, max_neighbour_number=max_nb)
+    else:
+        case = casegen.dam_break_3d(dx=0.02, tank=(0.6, 0.3, 0.4), column=(0.2, 0.3, 0.24), h_factor=h_factor,
+                                    max_neighbour_number=max_nb)
+    phys = case.physics
+    dps, _ = pair(case, max_nb)
+    # the oracle keeps the reference's fixed buckets (64 particles per cell unless configured);
+    # at 2h = 4 dx a 3D cell holds more, so give it room (the device has no bucket limit)
+    cfg = type(dps.config).from_buffer_copy(dps.config)
+    cfg.max_cell_particles = 256
+    o = Oracle(cfg, 32)
+    ps = case.ps
+    o.upload(ps.n_particles, ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, dps.cmap)
+    n = case.n
+    c = dps.ctx
+    c.set_accel_output(True)
+    c.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    fluid = case.ps["Tag"] == casegen.FLUID_TAG
+    lcap = 64 if dim == 2 else 160
+    for s in range(3):
+        sync_oracle(dps, o, case)
+        c.step(1, phys)
+        o.step(1, phys)
+        c.synchronize()
+        g, r = gpu_fields(dps), oracle_fields(o, n, dim)
+        acc = c.accel(n, dim)
+        racc = np.stack([o.field(ORC_FIELD_ACCEL, a, n) for a in range(dim)], 1)
+        acc_abs = np.stack([o.field(ORC_FIELD_ACCEL_ABS, a, n) for a in range(dim)], 1)
+        drho, drho_abs, ncount = oracle_continuity(dps, o, case)
+        assert np.array_equal(g["ncount"], ncount.astype(np.int32)), "step %d" % s
+        assert int(np.sum(g["ncount"] > lcap)) > n // 10   # the fallback path really runs
+        assert cond_err(acc[fluid], racc[fluid], acc_abs[fluid]) < REL
+        assert cond_err(g["drho"], drho, drho_abs) < REL
+        assert rel_err(g["rho"], r["rho"], 1.0) < REL
+        assert rel_err(g["x"], r["x"], 1.0) < 1e-6
+    assert o.status() & abi.EPP_STATUS_CELL_OVERFLOW == 0
+    assert c.synchronize(raise_on_status=False) == 0
