@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--instances", type=int, default=256, help="batch: number of instances")
     ap.add_argument("--requests", type=int, default=32, help="serve: number of requests in the stream")
     ap.add_argument("--sim-steps", type=int, default=2000, help="serve: steps per request")
+    ap.add_argument("--native", action="store_true",
+                    help="serve: run the trace through the native serving loop of the C ABI (epp_server_*)")
     ap.add_argument("--no-co-batch", dest="co_batch", action="store_false",
                     help="serve: give every request its own context (no co-batching of waiting requests)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -473,7 +475,7 @@ def run_serve(args):
     be = serve.DeviceBackend(device=rk.local, tuner=tuner if args.autotune else None)
     # launch configuration per (dimension, size bucket) of this rank's share, tuned before the clock starts
     tuned = {}
-    if args.autotune:
+    if args.autotune and not args.native:
         for s_ in mine:
             c = s_.case()
             cp = be.copies(c.n)
@@ -490,14 +492,23 @@ def run_serve(args):
     rk.barrier()
     clocks = Clocks(rk.local)
     clocks.start()
-    st = serve.Server(be, budget_bytes=120 * 10**9, co_batch=args.co_batch).run(runs)
+    if args.native:   # the C-ABI loop (epp_server_*), default launch configuration, no co-batching
+        st = serve.serve_native(mine, device=rk.local, budget_bytes=120 * 10**9)
+        lat = st.pop("latencies")
+    else:
+        st = serve.Server(be, budget_bytes=120 * 10**9, co_batch=args.co_batch).run(runs)
+        lat = [r.latency for r in runs if r.latency is not None]
     clk = clocks.stop()
     plain_runs = serve.make_runs(mine, be)
     rk.barrier()
-    plain = serve.Server(be, budget_bytes=120 * 10**9, max_active=1).run(plain_runs)
+    if args.native:
+        plain = serve.serve_native(mine, device=rk.local, budget_bytes=120 * 10**9, max_active=1)
+        lat_plain = plain.pop("latencies")
+    else:
+        plain = serve.Server(be, budget_bytes=120 * 10**9, max_active=1).run(plain_runs)
+        lat_plain = [r.latency for r in plain_runs if r.latency is not None]
     n_p = [r.case.n for r in runs]
-    mine_stats = {"served": st, "plain": plain, "lat": [r.latency for r in runs if r.latency is not None],
-                  "lat_plain": [r.latency for r in plain_runs if r.latency is not None], "particles": n_p,
+    mine_stats = {"served": st, "plain": plain, "lat": lat, "lat_plain": lat_plain, "particles": n_p,
                   "tuned": {k: list(v) for k, v in tuned.items()}, "clocks": clk}
     every = rk.gather(mine_stats)
     rk.finish()
@@ -534,7 +545,8 @@ def run_serve(args):
                       "requests_3d": sum(1 for s in specs if s.dim == 3),
                       "particles_total": int(sum(n_all)), "particles_range": [min(n_all), max(n_all)],
                       "hbm_budget_bytes_per_gpu": 120 * 10**9, "chunk_steps": 100,
-                      "co_batching": bool(args.co_batch),
+                      "co_batching": bool(args.co_batch) and not args.native,
+                      "loop": "native C ABI (epp_server_*)" if args.native else "Python (epp.serve.Server)",
                       "parallelism": ("requests split over %d GPUs by expected work" % rk.world) if rk.world > 1
                       else "single GPU"},
            "latency_p50_s": served["latency_p50_s"], "latency_p99_s": served["latency_p99_s"],

@@ -155,6 +155,21 @@ class epp_column_map(C.Structure):
         return m
 
 
+class epp_server_stats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("peak_resident_bytes", C.c_int64),
+        ("max_concurrent", C.c_int32),
+        ("waiting", C.c_int32),
+        ("active", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class epp_integrals(C.Structure):
     _fields_ = [
         ("mass_total", C.c_double),

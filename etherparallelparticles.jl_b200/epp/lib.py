@@ -20,6 +20,8 @@ EXPORTS = [
     "epp_profile_step", "epp_set_tuning", "epp_cell_sort_noalloc", "epp_noalloc_limits",
     "epp_set_instance_physics", "epp_get_instance_integrals", "epp_context_bytes", "epp_query",
     "epp_set_priority", "epp_set_block_threads", "epp_integrals_async", "epp_integrals_wait",
+    "epp_server_create", "epp_server_destroy", "epp_server_submit", "epp_server_poll", "epp_server_drain",
+    "epp_server_result", "epp_server_download",
 ]
 
 
@@ -69,6 +71,17 @@ def load(path=LIB_PATH):
     lib.epp_step.argtypes = [ctx, C.c_int32, P(abi.epp_physics)]
     lib.epp_get_integrals.argtypes = [ctx, P(abi.epp_physics), P(abi.epp_integrals)]
     lib.epp_integrals_async.argtypes = [ctx, P(abi.epp_physics), P(C.c_int64)]
+    srv = C.c_void_p
+    lib.epp_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.c_int32, P(C.c_void_p)]
+    lib.epp_server_destroy.argtypes = [srv]
+    lib.epp_server_submit.argtypes = [srv, P(abi.epp_config), C.c_int32, i32p, i32p, i32p, C.c_int64, f32p,
+                                      C.c_int64, P(abi.epp_column_map), P(abi.epp_physics), C.c_int32, C.c_int32,
+                                      P(C.c_int64)]
+    lib.epp_server_poll.argtypes = [srv, P(abi.epp_server_stats)]
+    lib.epp_server_drain.argtypes = [srv, P(abi.epp_server_stats)]
+    lib.epp_server_result.argtypes = [srv, C.c_int64, P(abi.epp_integrals), P(C.c_uint32), P(C.c_double),
+                                      P(C.c_double)]
+    lib.epp_server_download.argtypes = [srv, C.c_int64, i32p, i32p, i32p, C.c_int64, f32p, C.c_int64]
     lib.epp_integrals_wait.argtypes = [ctx, C.c_int64, P(abi.epp_integrals)]
     lib.epp_cell_stats.argtypes = [ctx, i32p, i32p, i32p, i32p]
     lib.epp_synchronize.argtypes = [ctx, P(C.c_uint32)]
@@ -254,3 +267,65 @@ class Context:
         out = np.zeros(dim * n, np.float32)
         self._ck(self.lib.epp_get_accel(self.h, _ptr(out, C.c_float), n), "epp_get_accel")
         return out.reshape(dim, n).T.copy()
+
+
+class NativeServer:
+    """The native serving loop (epp_server_*): submit reference-layout states, poll or drain,
+    read each request's integrals and (with keep_state) its final state."""
+
+    def __init__(self, device=0, budget_bytes=120 * 10**9, max_active=256, chunk_steps=100, ahead=2):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.epp_server_create(device, int(budget_bytes), max_active, chunk_steps, ahead, C.byref(h))
+        if rc != abi.EPP_OK:
+            raise EppError(rc, "epp_server_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.epp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc, what):
+        if rc != abi.EPP_OK:
+            raise EppError(rc, what)
+
+    def submit(self, config, ps, cmap, phys, steps, keep_state=False):
+        """Queue the simulation held by particle system `ps` (copied now); returns its id."""
+        rid = C.c_int64(-1)
+        self._ck(self.lib.epp_server_submit(
+            self.h, C.byref(config), ps.n_particles, _ptr(ps.is_alive, C.c_int32), _ptr(ps.cell_index, C.c_int32),
+            _ptr(ps.int_properties, C.c_int32), ps.int_properties.shape[0], _ptr(ps.float_properties, C.c_float),
+            ps.float_properties.shape[0], C.byref(cmap), C.byref(phys), steps, 1 if keep_state else 0,
+            C.byref(rid)), "epp_server_submit")
+        return rid.value
+
+    def poll(self):
+        st = abi.epp_server_stats()
+        self._ck(self.lib.epp_server_poll(self.h, C.byref(st)), "epp_server_poll")
+        return st.as_dict()
+
+    def drain(self):
+        st = abi.epp_server_stats()
+        self._ck(self.lib.epp_server_drain(self.h, C.byref(st)), "epp_server_drain")
+        return st.as_dict()
+
+    def result(self, rid):
+        out = abi.epp_integrals()
+        status, a, d = C.c_uint32(0), C.c_double(0), C.c_double(0)
+        self._ck(self.lib.epp_server_result(self.h, rid, C.byref(out), C.byref(status), C.byref(a), C.byref(d)),
+                 "epp_server_result")
+        return {"integrals": out.as_dict(), "status": status.value, "admit_s": a.value, "done_s": d.value}
+
+    def download(self, rid, ps):
+        """The final state of a keep_state request, into particle system `ps` (same layout)."""
+        self._ck(self.lib.epp_server_download(
+            self.h, rid, _ptr(ps.is_alive, C.c_int32), _ptr(ps.cell_index, C.c_int32),
+            _ptr(ps.int_properties, C.c_int32), ps.int_properties.shape[0], _ptr(ps.float_properties, C.c_float),
+            ps.float_properties.shape[0]), "epp_server_download")

@@ -362,3 +362,49 @@ def make_runs(specs, backend):
         key = backend.group_key(case) if hasattr(backend, "group_key") else None
         runs.append(Run(s, case, backend.bytes_needed(case), key))
     return runs
+
+
+def serve_native(specs, device=0, budget_bytes=120 * 10**9, max_active=256, chunk=100, ahead=2,
+                 clock=time.perf_counter, idle_wait=50e-6):
+    """The same request trace through the native serving loop (epp_server_*, the C ABI): each
+    request is submitted when its arrival time passes (its case built beforehand), the loop is
+    polled in between; returns the stats of Server.run (latency = completion - arrival)."""
+    from .lib import EppError, NativeServer
+    be = DeviceBackend(device=device)
+    prepared = []
+    for s in specs:
+        c = s.case()
+        prepared.append((s, c, be._config(c)[1], c.ps.column_map()))
+    srv = NativeServer(device=device, budget_bytes=budget_bytes, max_active=max_active, chunk_steps=chunk,
+                       ahead=ahead)
+    order = collections.deque(sorted(prepared, key=lambda p: p[0].arrival))
+    ids = {}
+    t0 = clock()
+    st = {}
+    while order or not st or st["waiting"] or st["active"]:
+        t = clock() - t0
+        while order and order[0][0].arrival <= t:
+            s, c, cfg, cmap = order.popleft()
+            ids[s.rid] = (s, srv.submit(cfg, c.ps, cmap, c.physics, s.steps))
+        st = srv.poll()
+        if not order and not st["waiting"] and not st["active"]:
+            break
+        time.sleep(idle_wait)
+    makespan = clock() - t0
+    lat, done = [], 0
+    for s, rid in ids.values():
+        try:
+            r = srv.result(rid)
+        except EppError:
+            continue
+        done += 1
+        lat.append(r["done_s"])   # submitted when its arrival time passed: completion - arrival
+    lat = np.array(lat) if lat else np.zeros(1)
+    out = {"completed": done, "rejected": int(st.get("failed", 0)), "makespan_s": makespan,
+           "sims_per_s": done / makespan if makespan > 0 else 0.0,
+           "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+           "latency_mean_s": float(lat.mean()), "peak_resident_bytes": int(st.get("peak_resident_bytes", 0)),
+           "max_concurrent": int(st.get("max_concurrent", 0)), "loop": "native (epp_server_*)",
+           "latencies": [float(x) for x in lat]}
+    srv.close()
+    return out

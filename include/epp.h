@@ -293,6 +293,48 @@ int32_t epp_query(epp_ctx* ctx, int32_t* done);
  * runs the higher priorities so they finish first while long runs fill the remaining SMs. */
 int32_t epp_set_priority(epp_ctx* ctx, int32_t priority, int32_t* applied);
 
+/* Native serving loop (no reference counterpart: the reference runs one simulation per
+ * process).  The same loop as the Python serving module, behind the C ABI so that a Julia or C
+ * host can use it: each submitted simulation (a dam-break state in the reference layout, its
+ * physics and step count) waits in a FIFO queue; epp_server_poll admits from the head while the
+ * resident contexts' epp_context_bytes stay within the budget (a request that can never fit
+ * fails with EPP_ERR_BUDGET), gives each admitted run its own context and a stream priority by
+ * size, keeps `ahead` chunks of `chunk_steps` steps queued on every resident stream (refilled
+ * when epp_query reports it drained), and retires a run after its last step with its FP64
+ * integrals (and, if asked at submit, its final state).  Every run uses the plain path's kernels
+ * and graphs, so its result equals the same simulation run alone.  A server is not thread-safe:
+ * drive it from one host thread.
+ *   epp_server_submit   copies the state (the caller's arrays may be reused at once); the
+ *                       initial search and all steps run later, inside epp_server_poll
+ *   epp_server_poll     one non-blocking pass of the loop; counts of waiting, resident, finished
+ *   epp_server_drain    polls until every submitted request has finished or failed
+ *   epp_server_result   a finished request's integrals, device status, and seconds from submit
+ *                       to admission and to completion; EPP_ERR_STATE while it is not finished,
+ *                       the request's own error code if it failed
+ *   epp_server_download its final state (submit with keep_state = 1), written like epp_download
+ *                       into arrays of the submitted layout */
+typedef struct epp_server epp_server;
+typedef struct epp_server_stats {
+    int64_t submitted, completed, failed;
+    int64_t peak_resident_bytes;
+    int32_t max_concurrent;
+    int32_t waiting, active;
+} epp_server_stats;
+int32_t epp_server_create(int32_t device, int64_t budget_bytes, int32_t max_active, int32_t chunk_steps,
+                          int32_t ahead, epp_server** out);
+int32_t epp_server_destroy(epp_server* server);
+int32_t epp_server_submit(epp_server* server, const epp_config* config, int32_t n_particles,
+                          const int32_t* is_alive, const int32_t* cell_index, const int32_t* int_props,
+                          int64_t ld_int, const float* float_props, int64_t ld_float,
+                          const epp_column_map* map, const epp_physics* phys, int32_t n_steps,
+                          int32_t keep_state, int64_t* request_id);
+int32_t epp_server_poll(epp_server* server, epp_server_stats* stats);
+int32_t epp_server_drain(epp_server* server, epp_server_stats* stats);
+int32_t epp_server_result(epp_server* server, int64_t request_id, epp_integrals* integrals,
+                          uint32_t* device_status, double* admit_s, double* done_s);
+int32_t epp_server_download(epp_server* server, int64_t request_id, int32_t* is_alive, int32_t* cell_index,
+                            int32_t* int_props, int64_t ld_int, float* float_props, int64_t ld_float);
+
 /* One dam-break step launched kernel by kernel (no graph) with CUDA events between the
  * kernels; stage_ms[0 .. EPP_PROFILE_STAGES-1] = momentum+integrate+bin, scan, scatter,
  * rank+gather, search (neighbour lists), continuity (0 for pair-pass families that fuse the

@@ -238,3 +238,91 @@ def test_co_batched_results_equal_alone():
         assert r.result["integrals"]["n_pairs"] == res["integrals"]["n_pairs"]
         for k in ("mass_total", "kinetic", "potential", "internal"):
             assert abs(r.result["integrals"][k] - res["integrals"][k]) <= 1e-12 * abs(res["integrals"][k]), (r.spec.rid, k)
+
+
+# ---------------------------------------------------------------------------- native loop (C ABI)
+
+def test_native_server_argument_checks():
+    """epp_server_create validates its arguments before touching a device, and without a GPU it
+    fails loudly (no CPU fallback)."""
+    import ctypes as C
+
+    from epp import abi, lib as epplib
+    lib = epplib.load()
+    h = C.c_void_p()
+    assert lib.epp_server_create(0, 0, 4, 100, 2, C.byref(h)) == abi.EPP_ERR_INVALID_ARGUMENT
+    assert lib.epp_server_create(0, 10**9, 0, 100, 2, C.byref(h)) == abi.EPP_ERR_INVALID_ARGUMENT
+    n = C.c_int32(0)
+    if lib.epp_device_count(C.byref(n)) != abi.EPP_OK:
+        with pytest.raises(epplib.EppError) as e:
+            epplib.NativeServer()
+        assert e.value.code == abi.EPP_ERR_NO_DEVICE
+
+
+def _native_submit(srv, specs, steps, keep_state=True):
+    be = serve.DeviceBackend()
+    cases, ids = [], []
+    for s in specs:
+        c = s.case()
+        _, cfg = be._config(c)
+        cases.append(c)
+        ids.append(srv.submit(cfg, c.ps, c.ps.column_map(), c.physics, steps, keep_state=keep_state))
+    return cases, ids
+
+
+@pytest.mark.gpu
+def test_native_server_results_equal_alone():
+    """The C-ABI serving loop: every request's integrals and final state equal the same
+    simulation run alone, with several requests resident at once."""
+    from epp.lib import EppError, NativeServer
+    from epp import abi
+    steps = 120
+    specs = _small_stream(n=5, steps=steps, seed=4)
+    srv = NativeServer(chunk_steps=50)
+    cases, ids = _native_submit(srv, specs, steps)
+    with pytest.raises(EppError) as e:   # not finished yet: nothing has run before a poll
+        srv.result(ids[0])
+    assert e.value.code == abi.EPP_ERR_STATE
+    st = srv.drain()
+    assert st["completed"] == len(specs) and st["failed"] == 0 and st["max_concurrent"] >= 2
+    for spec, rid in zip(specs, ids):
+        res = srv.result(rid)
+        assert 0 <= res["admit_s"] <= res["done_s"]
+        alone = serve.DeviceBackend(download=True)
+        h = alone.admit(spec.case())
+        alone.enqueue(h, steps)
+        ref = alone.finish(h)
+        assert res["status"] == ref["status"]
+        for k in ("mass_total", "kinetic", "potential", "internal", "n_pairs", "n_alive"):
+            assert res["integrals"][k] == ref["integrals"][k], (spec.rid, k)
+        out = spec.case()
+        srv.download(rid, out.ps)
+        for k, v in ref["state"].items():
+            assert np.array_equal(out.ps[k], v), (spec.rid, k)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_native_server_budget():
+    """Resident bytes stay within the budget; a request that can never fit fails with
+    EPP_ERR_BUDGET while the others are served."""
+    from epp.lib import EppError, NativeServer, context_bytes
+    from epp import abi
+    steps = 40
+    specs = _small_stream(n=4, steps=steps, seed=5)
+    be = serve.DeviceBackend()
+    sizes = [context_bytes(be._config(s.case())[1]) for s in specs]
+    budget = max(sizes) + min(sizes) // 2
+    srv = NativeServer(budget_bytes=budget, chunk_steps=20)
+    cases, ids = _native_submit(srv, specs, steps, keep_state=False)
+    st = srv.drain()
+    assert st["completed"] == len(specs) and st["peak_resident_bytes"] <= budget
+    srv.close()
+    small = NativeServer(budget_bytes=min(sizes) // 2, chunk_steps=20)
+    _, ids = _native_submit(small, specs[:2], steps, keep_state=False)
+    st = small.drain()
+    assert st["failed"] == 2 and st["completed"] == 0
+    with pytest.raises(EppError) as e:
+        small.result(ids[0])
+    assert e.value.code == abi.EPP_ERR_BUDGET
+    small.close()
