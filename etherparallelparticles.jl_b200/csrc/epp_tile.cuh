@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                 int jn = entry_index(en);
                 EPP_CHECK(jn < A.n_max, 16, jn);
                 float4 xn = cnt > 0 ? A.s.xh[jn] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                typename Act::Nb nn = act.fetch(jn, ti, 0);
+                typename Act::Nb nn = act.fetch(jn, ti, entry_tag(en));
                 for (int k = 0; k < cnt; ++k) {
                     const int tj = entry_tag(en);
                     const float4 xj = xn;
@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                         jn = entry_index(en);
                         EPP_CHECK(jn < A.n_max, 16, jn);
                         xn = A.s.xh[jn];
-                        nn = act.fetch(jn, ti, 0);
+                        nn = act.fetch(jn, ti, entry_tag(en));
                     }
                     const float4 t = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc);
                     sum.x += t.x;
