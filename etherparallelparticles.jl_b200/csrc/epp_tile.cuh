@@ -304,6 +304,9 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
             float hc_h = xi.w;   // exact bound of the last h_j seen
             float hc_r2 = dflt ? A.dom.gap_square : tc.h2sq;
             const int nchunk = (R.total + 31) >> 5;
+            // this lane's own particle in the union: the middle stencil row holds it
+            constexpr int RMID = D == 3 ? 4 : 1;
+            const int k_self = on ? R.cum[RMID] + (i - R.lo[RMID]) : -1;
             // chunk 0 in flight
             bool real = lane < R.total;
             int jn = real ? R.at(lane) : 0;
@@ -392,13 +395,12 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                     }
                 }
                 word &= allowed;
+                if ((k_self >> 5) == ch) word &= ~(1u << (k_self & 31));   // not its own neighbour
                 // this lane's neighbours among the chunk, in candidate order
                 while (word) {
                     const int b = __ffs(word) - 1;
                     word &= word - 1u;
-                    const int e = s_j[wib][b];
-                    if (entry_index(e) == i) continue;
-                    L.put(cnt++, e);
+                    L.put(cnt++, s_j[wib][b]);
                 }
                 __syncwarp();
             }
