@@ -127,8 +127,9 @@ struct ListWriter {
     int b0, b1, b2;
     __device__ __forceinline__ void put(int cnt, int j) {
         if (cnt >= ListConf<D>::LCAP) return;
-        if (!ListConf<D>::ROW) {
-            base[(size_t)cnt * cap] = j;
+        if (!ListConf<D>::ROW) {   // column-major: base advances one column per entry
+            *base = j;
+            base += cap;
             return;
         }
         const int s = cnt & 3;
@@ -172,7 +173,10 @@ struct ListReader {
     __device__ __forceinline__ int next(int k) {
         if (!ListConf<D>::ROW) {
             const int j = q.x;
-            if (k + 1 < cnt) q.x = base[(size_t)(k + 1) * cap];
+            if (k + 1 < cnt) {   // column-major: the next entry one column on
+                base += cap;
+                q.x = *base;
+            }
             return j;
         }
         const int s = k & 3;
