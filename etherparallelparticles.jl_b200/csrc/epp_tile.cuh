@@ -491,26 +491,38 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                     return;
                 }
                 // 3D: software pipeline, neighbour k + 1's loads in flight while k's term runs
-                int en = cnt > 0 ? lr.next(0) : list_entry(0, 1);
+                // the row is read four entries (16 bytes) at a time, two groups ahead; inside a
+                // group the entry is picked at compile time
+                const int4* row = reinterpret_cast<const int4*>(lr.base);
+                int4 q = lr.q, qn = lr.qn;
+                int en = cnt > 0 ? q.x : list_entry(0, 1);
                 int jn = entry_index(en);
                 EPP_CHECK(jn < A.n_max, 16, jn);
                 float4 xn = cnt > 0 ? A.s.xh[jn] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 typename Act::Nb nn = act.fetch(jn, ti, entry_tag(en));
-                for (int k = 0; k < cnt; ++k) {
-                    const int tj = entry_tag(en);
-                    const float4 xj = xn;
-                    const typename Act::Nb nb = nn;
-                    if (k + 1 < cnt) {
-                        en = lr.next(k + 1);
-                        jn = entry_index(en);
-                        EPP_CHECK(jn < A.n_max, 16, jn);
-                        xn = A.s.xh[jn];
-                        nn = act.fetch(jn, ti, entry_tag(en));
+                for (int k0 = 0; k0 < cnt; k0 += 4) {
+                    const int4 q2 = k0 + 8 < cnt ? row[(k0 >> 2) + 2] : make_int4(0, 0, 0, 0);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = k0 + u;
+                        if (k >= cnt) break;
+                        const int tj = entry_tag(en);
+                        const float4 xj = xn;
+                        const typename Act::Nb nb = nn;
+                        if (k + 1 < cnt) {
+                            en = u == 0 ? q.y : u == 1 ? q.z : u == 2 ? q.w : qn.x;
+                            jn = entry_index(en);
+                            EPP_CHECK(jn < A.n_max, 16, jn);
+                            xn = A.s.xh[jn];
+                            nn = act.fetch(jn, ti, entry_tag(en));
+                        }
+                        const float4 t = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc);
+                        sum.x += t.x;
+                        sum.y += t.y;
+                        sum.z += t.z;
                     }
-                    const float4 t = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc);
-                    sum.x += t.x;
-                    sum.y += t.y;
-                    sum.z += t.z;
+                    q = qn;
+                    qn = q2;
                 }
             } else {
                 sum = neighbours_by_stencil<D>(A, i, xi, ti, tc, act);
