@@ -492,8 +492,8 @@ def run_serve(args):
     rk.barrier()
     clocks = Clocks(rk.local)
     clocks.start()
-    if args.native:   # the C-ABI loop (epp_server_*), default launch configuration, no co-batching
-        st = serve.serve_native(mine, device=rk.local, budget_bytes=120 * 10**9)
+    if args.native:   # the C-ABI loop (epp_server_*), default launch configuration
+        st = serve.serve_native(mine, device=rk.local, budget_bytes=120 * 10**9, co_batch=args.co_batch)
         lat = st.pop("latencies")
     else:
         st = serve.Server(be, budget_bytes=120 * 10**9, co_batch=args.co_batch).run(runs)
@@ -545,7 +545,7 @@ def run_serve(args):
                       "requests_3d": sum(1 for s in specs if s.dim == 3),
                       "particles_total": int(sum(n_all)), "particles_range": [min(n_all), max(n_all)],
                       "hbm_budget_bytes_per_gpu": 120 * 10**9, "chunk_steps": 100,
-                      "co_batching": bool(args.co_batch) and not args.native,
+                      "co_batching": bool(args.co_batch),
                       "loop": "native C ABI (epp_server_*)" if args.native else "Python (epp.serve.Server)",
                       "parallelism": ("requests split over %d GPUs by expected work" % rk.world) if rk.world > 1
                       else "single GPU"},

@@ -21,7 +21,7 @@ EXPORTS = [
     "epp_set_instance_physics", "epp_get_instance_integrals", "epp_context_bytes", "epp_query",
     "epp_set_priority", "epp_set_block_threads", "epp_integrals_async", "epp_integrals_wait",
     "epp_server_create", "epp_server_destroy", "epp_server_submit", "epp_server_poll", "epp_server_drain",
-    "epp_server_result", "epp_server_download",
+    "epp_server_result", "epp_server_download", "epp_server_set_co_batch",
 ]
 
 
@@ -74,6 +74,7 @@ def load(path=LIB_PATH):
     srv = C.c_void_p
     lib.epp_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.c_int32, P(C.c_void_p)]
     lib.epp_server_destroy.argtypes = [srv]
+    lib.epp_server_set_co_batch.argtypes = [srv, C.c_int32, C.c_int32]
     lib.epp_server_submit.argtypes = [srv, P(abi.epp_config), C.c_int32, i32p, i32p, i32p, C.c_int64, f32p,
                                       C.c_int64, P(abi.epp_column_map), P(abi.epp_physics), C.c_int32, C.c_int32,
                                       P(C.c_int64)]
@@ -273,13 +274,16 @@ class NativeServer:
     """The native serving loop (epp_server_*): submit reference-layout states, poll or drain,
     read each request's integrals and (with keep_state) its final state."""
 
-    def __init__(self, device=0, budget_bytes=120 * 10**9, max_active=256, chunk_steps=100, ahead=2):
+    def __init__(self, device=0, budget_bytes=120 * 10**9, max_active=256, chunk_steps=100, ahead=2,
+                 co_batch=False, batch_max=256):
         self.lib = load()
         h = C.c_void_p()
         rc = self.lib.epp_server_create(device, int(budget_bytes), max_active, chunk_steps, ahead, C.byref(h))
         if rc != abi.EPP_OK:
             raise EppError(rc, "epp_server_create")
         self.h = h
+        if co_batch:
+            self._ck(self.lib.epp_server_set_co_batch(self.h, 1, batch_max), "epp_server_set_co_batch")
 
     def close(self):
         if getattr(self, "h", None):

@@ -365,7 +365,7 @@ def make_runs(specs, backend):
 
 
 def serve_native(specs, device=0, budget_bytes=120 * 10**9, max_active=256, chunk=100, ahead=2,
-                 clock=time.perf_counter, idle_wait=50e-6):
+                 clock=time.perf_counter, idle_wait=50e-6, co_batch=False):
     """The same request trace through the native serving loop (epp_server_*, the C ABI): each
     request is submitted when its arrival time passes (its case built beforehand), the loop is
     polled in between; returns the stats of Server.run (latency = completion - arrival)."""
@@ -376,7 +376,7 @@ def serve_native(specs, device=0, budget_bytes=120 * 10**9, max_active=256, chun
         c = s.case()
         prepared.append((s, c, be._config(c)[1], c.ps.column_map()))
     srv = NativeServer(device=device, budget_bytes=budget_bytes, max_active=max_active, chunk_steps=chunk,
-                       ahead=ahead)
+                       ahead=ahead, co_batch=co_batch)
     order = collections.deque(sorted(prepared, key=lambda p: p[0].arrival))
     ids = {}
     t0 = clock()

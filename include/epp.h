@@ -323,6 +323,12 @@ typedef struct epp_server_stats {
 int32_t epp_server_create(int32_t device, int64_t budget_bytes, int32_t max_active, int32_t chunk_steps,
                           int32_t ahead, epp_server** out);
 int32_t epp_server_destroy(epp_server* server);
+/* Co-batching (off by default): at admission the waiting requests that can share the head's cell
+ * grid (2D, the same domain, tags, column map, step count, keep_state and physics apart from dt
+ * and c0; no instance column of their own) join it, up to batch_max, as the instances of one
+ * batch context: one launch per pass for all of them.  Each keeps its own dt and c0; its state
+ * equals the request run alone, its FP64 integrals agree to rounding (another summation order). */
+int32_t epp_server_set_co_batch(epp_server* server, int32_t enabled, int32_t batch_max);
 int32_t epp_server_submit(epp_server* server, const epp_config* config, int32_t n_particles,
                           const int32_t* is_alive, const int32_t* cell_index, const int32_t* int_props,
                           int64_t ld_int, const float* float_props, int64_t ld_float,

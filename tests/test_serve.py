@@ -326,3 +326,32 @@ def test_native_server_budget():
         small.result(ids[0])
     assert e.value.code == abi.EPP_ERR_BUDGET
     small.close()
+
+
+@pytest.mark.gpu
+def test_native_server_co_batching_equals_alone():
+    """Co-batching in the C-ABI loop: requests of the 256-instance mix waiting together become one
+    batch context; each request's state is bit-identical to the request run alone, its FP64
+    integrals equal to the rounding of the per-instance reduction order (1e-12)."""
+    from epp.lib import NativeServer
+    steps = 60
+    specs = serve.batch_mix_requests(5, steps=steps)
+    srv = NativeServer(chunk_steps=20, co_batch=True)
+    cases, ids = _native_submit(srv, specs, steps)
+    st = srv.drain()
+    assert st["completed"] == len(specs) and st["failed"] == 0
+    assert st["max_concurrent"] == len(specs)   # all five resident together, as one batch
+    for spec, rid in zip(specs, ids):
+        res = srv.result(rid)
+        alone = serve.DeviceBackend(download=True)
+        h = alone.admit(spec.case())
+        alone.enqueue(h, steps)
+        ref = alone.finish(h)
+        assert res["integrals"]["n_pairs"] == ref["integrals"]["n_pairs"]
+        for k in ("mass_total", "kinetic", "potential", "internal"):
+            assert abs(res["integrals"][k] - ref["integrals"][k]) <= 1e-12 * abs(ref["integrals"][k]), (spec.rid, k)
+        out = spec.case()
+        srv.download(rid, out.ps)
+        for k, v in ref["state"].items():
+            assert np.array_equal(out.ps[k], v), (spec.rid, k)
+    srv.close()
