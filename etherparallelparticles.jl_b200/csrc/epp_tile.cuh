@@ -9,8 +9,8 @@
 // The search pass (k_build) stages each chunk of 32 candidates in shared memory with one
 // coalesced load per lane; every lane then tests all 32 staged candidates against its own
 // particle with broadcast shared-memory reads -- all lanes in lockstep -- using the reference's
-// IEEE criterion and the active-pair matrix, and appends its accepted neighbours (sorted
-// indices, candidate order) to its list.  The pair passes (k_list: continuity, momentum, the
+// IEEE criterion and the active-pair matrix, and appends its accepted neighbours (sorted index
+// and tag, candidate order) to its list.  The pair passes (k_list: continuity, momentum, the
 // count actions) then walk each particle's list, one thread per particle, so every lane runs
 // its own neighbour count without waiting for the others' candidates.
 //
@@ -150,7 +150,9 @@ __device__ __forceinline__ ListWriter<D> list_writer(const TileMask& M, int i) {
     return ListWriter<D>{ListConf<D>::ROW ? M.list + (size_t)i * ListConf<D>::LCAP : M.list + i, M.cap, 0, 0, 0};
 }
 
-// Reads a particle's list in order, the next entries already in flight.
+// Reads a particle's list in order, the next entries already in flight: 2D (column-major) one
+// entry at a time through next(); 3D (row-major) rows are read four entries at a time by k_list
+// from the two groups start() loads.
 template <int D>
 struct ListReader {
     const int* base;
@@ -169,21 +171,12 @@ struct ListReader {
             q.x = n > 0 ? base[0] : 0;
         }
     }
-    // entry k (called with k = 0, 1, 2, ... < cnt)
+    // entry k of a column-major list (called with k = 0, 1, 2, ... < cnt)
     __device__ __forceinline__ int next(int k) {
-        if (!ListConf<D>::ROW) {
-            const int j = q.x;
-            if (k + 1 < cnt) {   // column-major: the next entry one column on
-                base += cap;
-                q.x = *base;
-            }
-            return j;
-        }
-        const int s = k & 3;
-        const int j = s == 0 ? q.x : s == 1 ? q.y : s == 2 ? q.z : q.w;
-        if (s == 3) {   // next group of four, the one after it in flight
-            q = qn;
-            if (k + 5 < cnt) qn = reinterpret_cast<const int4*>(base)[(k + 5) >> 2];
+        const int j = q.x;
+        if (k + 1 < cnt) {   // the next entry one column on
+            base += cap;
+            q.x = *base;
         }
         return j;
     }
