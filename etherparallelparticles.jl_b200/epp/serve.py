@@ -154,7 +154,8 @@ class DeviceBackend:
         self.tuner = tuner        # autotune.Autotuner: launch configuration per dimension and size
         self.tune_concurrent = tune_concurrent   # tune for throughput with several runs resident
 
-    def _config(self, case):
+    def config_of(self, case):
+        """(NeighbourSystem, epp_config) of a request's case on this backend's device."""
         from .classes import NeighbourSystem
         ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
         adj = ns.active_pair.adjacency_matrix.tolist()
@@ -168,11 +169,11 @@ class DeviceBackend:
 
     def bytes_needed(self, case):
         from .lib import context_bytes
-        return context_bytes(self._config(case)[1])
+        return context_bytes(self.config_of(case)[1])
 
     def admit(self, case):
         from .algorithm import DeviceParticleSystem
-        ns, _ = self._config(case)
+        ns, _ = self.config_of(case)
         dps = DeviceParticleSystem(case.ps, ns, device=self.device)
         dps.physics = case.physics
         if self.priorities:
@@ -190,7 +191,7 @@ class DeviceBackend:
         """One batch context holding `cases` as instances 0..K-1 (casegen.merge_cases)."""
         from .algorithm import DeviceParticleSystem
         b = casegen.merge_cases(cases)
-        ns, _ = self._config(b)
+        ns, _ = self.config_of(b)
         dps = DeviceParticleSystem(b.ps, ns, device=self.device, n_instances=b.n_instances)
         dps.physics = b.physics
         dps.batch = b
@@ -374,7 +375,7 @@ def serve_native(specs, device=0, budget_bytes=120 * 10**9, max_active=256, chun
     prepared = []
     for s in specs:
         c = s.case()
-        prepared.append((s, c, be._config(c)[1], c.ps.column_map()))
+        prepared.append((s, c, be.config_of(c)[1], c.ps.column_map()))
     srv = NativeServer(device=device, budget_bytes=budget_bytes, max_active=max_active, chunk_steps=chunk,
                        ahead=ahead, co_batch=co_batch)
     order = collections.deque(sorted(prepared, key=lambda p: p[0].arrival))

@@ -264,7 +264,7 @@ def _native_submit(srv, specs, steps, keep_state=True):
     cases, ids = [], []
     for s in specs:
         c = s.case()
-        _, cfg = be._config(c)
+        _, cfg = be.config_of(c)
         cases.append(c)
         ids.append(srv.submit(cfg, c.ps, c.ps.column_map(), c.physics, steps, keep_state=keep_state))
     return cases, ids
@@ -311,7 +311,7 @@ def test_native_server_budget():
     steps = 40
     specs = _small_stream(n=4, steps=steps, seed=5)
     be = serve.DeviceBackend()
-    sizes = [context_bytes(be._config(s.case())[1]) for s in specs]
+    sizes = [context_bytes(be.config_of(s.case())[1]) for s in specs]
     budget = max(sizes) + min(sizes) // 2
     srv = NativeServer(budget_bytes=budget, chunk_steps=20)
     cases, ids = _native_submit(srv, specs, steps, keep_state=False)
