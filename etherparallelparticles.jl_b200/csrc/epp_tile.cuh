@@ -132,16 +132,23 @@ struct ListWriter {
             base += cap;
             return;
         }
-        const int s = cnt & 3;
-        if (s == 0) b0 = j;
-        else if (s == 1) b1 = j;
-        else if (s == 2) b2 = j;
-        else *reinterpret_cast<int4*>(base + (cnt - 3)) = make_int4(b0, b1, b2, j);
+        // row-major: the last three entries wait in b0..b2 (oldest first); every fourth entry
+        // stores the group and the row pointer moves on
+        if ((cnt & 3) == 3) {
+            *reinterpret_cast<int4*>(base) = make_int4(b0, b1, b2, j);
+            base += 4;
+        }
+        b0 = b1;
+        b1 = b2;
+        b2 = j;
     }
     // the last partial group of a row (its unused slots are never read)
     __device__ __forceinline__ void flush(int cnt) {
-        if (ListConf<D>::ROW && cnt < ListConf<D>::LCAP && (cnt & 3))
-            *reinterpret_cast<int4*>(base + (cnt & ~3)) = make_int4(b0, b1, b2, 0);
+        if (!ListConf<D>::ROW || cnt >= ListConf<D>::LCAP) return;
+        const int r = cnt & 3;   // entries waiting: the newest r of b0..b2
+        if (r == 1) *reinterpret_cast<int4*>(base) = make_int4(b2, 0, 0, 0);
+        else if (r == 2) *reinterpret_cast<int4*>(base) = make_int4(b1, b2, 0, 0);
+        else if (r == 3) *reinterpret_cast<int4*>(base) = make_int4(b0, b1, b2, 0);
     }
 };
 
