@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                     // dr2 <= R2 as integers: non-negative floats order like their bit patterns, so
                     // bits(dr2) - bits(R2) - 1 is negative exactly for the accepted candidates, and
                     // a funnel shift moves that sign bit into the chunk's word (candidate 0 ends in
-                    // the top bit; one bit reversal per chunk restores candidate order)
+                    // the top bit, where the append loop below starts)
                     const int nR2 = -__float_as_int(hc_r2) - 1;
                     // two candidates per packed sub / mul; dr2 = (dx dx + dy dy) + dz dz, IEEE
                     const f32x2 XI = f2_pack(xi.x, xi.x), YI = f2_pack(xi.y, xi.y), ZI = f2_pack(xi.z, xi.z);
@@ -379,7 +379,6 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                         word = __funnelshift_l((unsigned)(__float_as_int(d0) + nR2), word, 1);
                         word = __funnelshift_l((unsigned)(__float_as_int(d1) + nR2), word, 1);
                     }
-                    word = __brev(word);
                 } else {
 #pragma unroll 8
                     for (int b = 0; b < 32; ++b) {
@@ -395,15 +394,16 @@ __global__ void __launch_bounds__(128, D == 2 ? 8 : 6)
                             hc_h = xj.w;
                             hc_r2 = dflt ? A.dom.gap_square : xj.w == xi.w ? tc.h2sq : pair_r2(xi.w, xj.w);
                         }
-                        word |= (unsigned)(dr2 <= hc_r2) << b;
+                        word |= (unsigned)(dr2 <= hc_r2) << (31 - b);
                     }
                 }
-                word &= allowed;
-                if ((k_self >> 5) == ch) word &= ~(1u << (k_self & 31));   // not its own neighbour
+                // candidate b at bit 31 - b: walked from the top with count-leading-zeros
+                word &= __brev(allowed);
+                if ((k_self >> 5) == ch) word &= ~(0x80000000u >> (k_self & 31));   // not its own neighbour
                 // this lane's neighbours among the chunk, in candidate order
                 while (word) {
-                    const int b = __ffs(word) - 1;
-                    word &= word - 1u;
+                    const int b = __clz(word);
+                    word ^= 0x80000000u >> b;
                     L.put(cnt++, s_j[wib][b]);
                 }
                 __syncwarp();
