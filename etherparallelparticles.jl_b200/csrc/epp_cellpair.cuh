@@ -114,11 +114,12 @@ struct CPCont {
         float vol;
     };
     __device__ __forceinline__ Self self(int i) const { return Self{s.vm[i], s.rho[i]}; }
+    // Neighbour records go through the read-only path: no pass writes what it gathers.
     // V_j enters only the balanced (fluid-wall, wall-fluid) term: in 3D fluid-fluid pairs skip its
     // load (5% off the pass); in 2D, without the 3D software pipeline, the branch costs more than
     // the 4-byte gather saves
     __device__ __forceinline__ Nb fetch(int j, int ti, int tj) const {
-        return Nb{s.vm[j], D == 3 && ti == P.fluid && tj == P.fluid ? 0.0f : s.vol[j]};
+        return Nb{__ldg(&s.vm[j]), D == 3 && ti == P.fluid && tj == P.fluid ? 0.0f : __ldg(&s.vol[j])};
     }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
                                            const PairGeo& g, const TargetConst& tc) const {
@@ -240,7 +241,9 @@ struct CPMom {
     __device__ __forceinline__ Self self(int i) const {
         return Self{m.s.vm[i], m.s.rp4[i], m.P.c0_of(inst_of(m.s.tagm[i])), gap_of(i)};
     }
-    __device__ __forceinline__ Nb fetch(int j, int, int) const { return Nb{m.s.vm[j], m.s.rp4[j], gap_of(j)}; }
+    __device__ __forceinline__ Nb fetch(int j, int, int) const {
+        return Nb{__ldg(&m.s.vm[j]), __ldg(&m.s.rp4[j]), gap_of(j)};
+    }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
                                            const PairGeo& g, const TargetConst& tc) const {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);

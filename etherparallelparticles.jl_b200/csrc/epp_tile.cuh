@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                         const int j = entry_index(e);
                         EPP_CHECK(j < A.n_max, 16, j);
                         const int tj = entry_tag(e);
-                        const float4 xj = A.s.xh[j];
+                        const float4 xj = __ldg(&A.s.xh[j]);
                         const float4 t =
                             act.term(me, act.fetch(j, ti, tj), ti, tj, xj, geometry<D>(xi, xj), tc);
                         sum.x += t.x;
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                 int en = cnt > 0 ? q.x : list_entry(0, 1);
                 int jn = entry_index(en);
                 EPP_CHECK(jn < A.n_max, 16, jn);
-                float4 xn = cnt > 0 ? A.s.xh[jn] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float4 xn = cnt > 0 ? __ldg(&A.s.xh[jn]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 typename Act::Nb nn = act.fetch(jn, ti, entry_tag(en));
                 for (int k0 = 0; k0 < cnt; k0 += 4) {
                     const int4 q2 = k0 + 8 < cnt ? row[(k0 >> 2) + 2] : make_int4(0, 0, 0, 0);
@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(128, D == 2 ? 9 : 4)   // 2D: 9 blocks (56 reg
                             en = u == 0 ? q.y : u == 1 ? q.z : u == 2 ? q.w : qn.x;
                             jn = entry_index(en);
                             EPP_CHECK(jn < A.n_max, 16, jn);
-                            xn = A.s.xh[jn];
+                            xn = __ldg(&A.s.xh[jn]);
                             nn = act.fetch(jn, ti, entry_tag(en));
                         }
                         const float4 t = act.term(me, nb, ti, tj, xj, geometry<D>(xi, xj), tc);
