@@ -68,7 +68,7 @@ __device__ __forceinline__ float kern_dwr(int kind, float q, float hinv) {
     switch (kind) {
         case EPP_KERNEL_CUBIC_SPLINE:
             if (q < 1.0f) return s * (3.0f * q - 4.0f) * 0.75f;
-            if (q < 2.0f) return -s * (2.0f - q) * (2.0f - q) * 0.75f / q;
+            if (q < 2.0f) return __fdividef(-s * (2.0f - q) * (2.0f - q) * 0.75f, q);   // a scale, no cancellation
             return 0.0f;
         case EPP_KERNEL_GAUSSIAN:
             return q < 3.0f ? -2.0f * s * expf(-q * q) : 0.0f;
