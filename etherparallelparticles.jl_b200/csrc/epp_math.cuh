@@ -212,6 +212,51 @@ __device__ __forceinline__ float4 make_rp4(float rho, float p) {
     return make_float4(rho, p, __fdiv_rn(p, __fmul_rn(rho, rho)), __fdiv_rn(1.0f, rho));
 }
 
+// The cell grid of a domain, on the host, in FP32 as the Domain2D constructor computes it
+// (Domain2D.jl:28-67): n_a = floor(span_a / gap) cells per axis, gap_a = span_a / n_a and
+// gap_inv_a = 1 / gap_a.  `n_inst` copies of the grid are stacked as independent layers (batches).
+// Returns EPP_ERR_INVALID_ARGUMENT for a non-positive or non-finite gap or extent (fewer than one
+// cell on an axis) or more than 2^22 layers, and EPP_ERR_CAPACITY when all layers together hold
+// more than `max_cells` (at most 2^30) cells; the count is checked after every axis, so the
+// product cannot overflow, and a per-axis count is checked against 2^31 before the conversion
+// to int.
+inline int plan_domain(const epp_domain& in, int n_inst, long long max_cells, DevDomain& d) {
+    const int D = in.dim;
+    if (D != 2 && D != 3) return EPP_ERR_INVALID_ARGUMENT;
+    if (n_inst < 1) n_inst = 1;
+    if (n_inst > (1 << 22) || max_cells > (1ll << 30)) return EPP_ERR_INVALID_ARGUMENT;
+    const float gap = in.gap;
+    if (!(gap > 0.0f) || !(gap < 3.0e38f)) return EPP_ERR_INVALID_ARGUMENT;
+    d.dim = D;
+    d.gap_square = gap * gap;
+    long long ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        d.n[a] = 1;
+        d.first[a] = d.last[a] = 0.0f;
+        d.gap_inv[a] = 1.0f;
+    }
+    for (int a = 0; a < D; ++a) {
+        d.first[a] = in.first[a];
+        d.last[a] = in.last[a];
+        volatile float span = d.last[a] - d.first[a];
+        volatile float q = span / gap;
+        const float fq = floorf(q);
+        if (!(fq >= 1.0f)) return EPP_ERR_INVALID_ARGUMENT;   // also NaN
+        if (!(fq < 2147483648.0f)) return EPP_ERR_CAPACITY;
+        const int na = (int)fq;
+        d.n[a] = na;
+        volatile float ga = span / (float)na;
+        d.gap_inv[a] = 1.0f / ga;
+        ncell *= na;   // <= 2^30 * 2^31 before the check below: no overflow
+        if (ncell > max_cells) return EPP_ERR_CAPACITY;
+    }
+    if (ncell * n_inst > max_cells) return EPP_ERR_CAPACITY;   // <= 2^30 * 2^22
+    d.cells_per_inst = (int)ncell;
+    d.n_inst = n_inst;
+    d.n_cells = (int)(ncell * n_inst);
+    return EPP_OK;
+}
+
 // Cell of a position: indexCartesianFromPosition + indexCartesianToLinear (Domain2D.jl:92-137),
 // 0-based.  Returns -1 when the position is outside the domain (the particle is then killed,
 // NeighbourSearch.jl:41-43).

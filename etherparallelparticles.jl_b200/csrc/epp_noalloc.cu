@@ -9,7 +9,9 @@
 // every GPU that loads libepp.so holds it until the process exits.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "epp_cells.cuh"
 
@@ -42,7 +44,11 @@ constexpr size_t kScratchBytes = kOffMeta + align256(sizeof(int) * 64);
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-unsigned char* g_scratch_addr[kMaxDevices] = {};   // device address of the scratch, per device
+// Device address of the scratch, per device, looked up on the first call on that device.  The
+// look-up is guarded, so first calls from several host threads at once are safe (the calls
+// themselves still share the scratch and must not overlap on the GPU).
+std::atomic<unsigned char*> g_scratch_addr[kMaxDevices];
+std::mutex g_scratch_mu;
 
 // Bin particle i (positions column-major: x at pos[i], y at pos[n + i], z at pos[2n + i]); outside
 // the domain -> dead bin (n_cells), as NeighbourSearch.jl:41-43 kills it.
@@ -58,20 +64,28 @@ __global__ void k_na_bin(int n, DevDomain dom, const float* pos, int* count, int
 }
 
 // Rank inside the cell by particle id; writes the 1-based id to its sorted position.
+// A permutation entry or destination outside 0..n-1 is skipped and reported (EPP_STATUS_QUEUE).
 __global__ void k_na_rank(int n, int n_cells, const int2* perm, const int2* cs, const int* start,
-                          int* sorted_ids) {
+                          int* sorted_ids, unsigned* status) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const int2 e = perm[p];
     const int src = e.y;
-    if (src < 0 || src >= n) return;
+    if (src < 0 || src >= n) {
+        atomicOr(status, EPP_STATUS_QUEUE);
+        return;
+    }
     const int c = cs[src].x;
     if (c >= n_cells) return;   // dead particles are not part of the cell list
     const int s = start[c], en = min(start[c + 1], n);
     int rank = 0;
     for (int q = max(s, 0); q < en; ++q) rank += perm[q].x < e.x;
     const int dst = s + rank;
-    if (dst >= 0 && dst < n) sorted_ids[dst] = e.x + 1;
+    if (dst < 0 || dst >= n) {
+        atomicOr(status, EPP_STATUS_QUEUE);
+        return;
+    }
+    sorted_ids[dst] = e.x + 1;
 }
 
 // Scatter in arrival order: perm[start[c] + slot] = (particle id, particle id).
@@ -93,36 +107,6 @@ __global__ void k_na_counts(int n_cells, const int* start, int* counts, int* off
     if (c <= n_cells && offsets) offsets[c] = start[c];
 }
 
-int device_domain(const epp_domain& d, DevDomain& o) {
-    if (d.dim != 2 && d.dim != 3) return EPP_ERR_INVALID_ARGUMENT;
-    if (!(d.gap > 0.0f)) return EPP_ERR_INVALID_ARGUMENT;
-    std::memset(&o, 0, sizeof o);
-    o.dim = d.dim;
-    o.gap_square = d.gap * d.gap;
-    long long nc = 1;
-    for (int a = 0; a < 3; ++a) {
-        o.n[a] = 1;
-        o.gap_inv[a] = 1.0f;
-    }
-    for (int a = 0; a < d.dim; ++a) {
-        o.first[a] = d.first[a];
-        o.last[a] = d.last[a];
-        const float span = d.last[a] - d.first[a];
-        volatile float q = span / d.gap;
-        const int na = (int)floorf(q);
-        if (na < 1) return EPP_ERR_INVALID_ARGUMENT;
-        o.n[a] = na;
-        volatile float ga = span / (float)na;
-        o.gap_inv[a] = 1.0f / ga;
-        nc *= na;
-    }
-    if (nc > kNaMaxCells) return EPP_ERR_CAPACITY;
-    o.n_cells = (int)nc;
-    o.cells_per_inst = (int)nc;
-    o.n_inst = 1;
-    return EPP_OK;
-}
-
 }  // namespace
 
 extern "C" {
@@ -139,17 +123,22 @@ int32_t epp_cell_sort_noalloc(const epp_domain* domain, int32_t n, const float* 
     if (!domain || n < 0 || (n > 0 && !pos) || !sorted_ids || !n_alive) return EPP_ERR_INVALID_ARGUMENT;
     if (n > kNaMaxParticles) return EPP_ERR_CAPACITY;
     DevDomain dom;
-    int rc = device_domain(*domain, dom);
-    if (rc) return rc;
+    std::memset(&dom, 0, sizeof dom);
+    if (const int rc = plan_domain(*domain, 1, kNaMaxCells, dom)) return rc;   // the context's cell grid
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EPP_ERR_CUDA;
     // set-up, once per device, with that device current: the scratch's device address
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return EPP_ERR_CUDA;
-        g_scratch_addr[dev] = static_cast<unsigned char*>(p);
+    unsigned char* base = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!base) {
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        base = g_scratch_addr[dev].load(std::memory_order_acquire);
+        if (!base) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return EPP_ERR_CUDA;
+            base = static_cast<unsigned char*>(p);
+            g_scratch_addr[dev].store(base, std::memory_order_release);
+        }
     }
-    unsigned char* base = g_scratch_addr[dev];
     int* count = reinterpret_cast<int*>(base + kOffCounts);
     unsigned long long* scan = reinterpret_cast<unsigned long long*>(base + kOffScan);
     int2* cs = reinterpret_cast<int2*>(base + kOffCs);
@@ -176,7 +165,7 @@ int32_t epp_cell_sort_noalloc(const epp_domain* domain, int32_t n, const float* 
     unsigned* status = reinterpret_cast<unsigned*>(meta + 1);
     if (n > 0) {
         k_na_scatter<<<gb, T, 0, s>>>(n, cs, start, perm, status);
-        k_na_rank<<<gb, T, 0, s>>>(n, nc, perm, cs, start, sorted_ids);
+        k_na_rank<<<gb, T, 0, s>>>(n, nc, perm, cs, start, sorted_ids, status);
     }
     k_na_counts<<<(nc + 1 + T - 1) / T, T, 0, s>>>(nc, start, counts, offsets);
     if (cudaGetLastError() != cudaSuccess) return EPP_ERR_CUDA;

@@ -2,9 +2,9 @@
 
 The reference is Julia and cannot run here, so its known-answer tests are read as text: every
 value below is parsed out of the cited test file, and the script fails if a file no longer
-contains the expression it expects.  Run it in a checkout that has the reference mounted:
+contains the expression it expects.  Run it with the path of a checkout of the reference:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to EtherParallelParticles.jl>
 
 The generated JSON is committed; the tests read only the JSON.
 """
@@ -164,7 +164,9 @@ def columns(root):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: make_golden.py <path to a checkout of EtherParallelParticles.jl>")
+    root = sys.argv[1]
     kat = {
         "generated_by": "tests/golden/make_golden.py",
         "neighbour_search": neighbour_search(root),

@@ -82,3 +82,28 @@ def test_context_bytes_capacity_limit():
     with pytest.raises(epplib.EppError) as e:
         epplib.context_bytes(abi.make_config(d, (1 << 28) + 1, [[1, 1], [1, 0]]))
     assert e.value.code == abi.EPP_ERR_CAPACITY
+
+
+@pytest.mark.parametrize("gap,first,last,code", [
+    # 2^22 x 2^21 x 2^21 cells: the product is 2^64, which wraps to 0 in 64-bit arithmetic
+    (1.0, [0, 0, 0], [4194304.0, 2097152.0, 2097152.0], abi.EPP_ERR_CAPACITY),
+    # more than 2^31 cells on one axis: rejected before the conversion to int
+    (1e-30, [0, 0, 0], [1.0, 1.0, 1.0], abi.EPP_ERR_CAPACITY),
+    (float("nan"), [0, 0, 0], [1.0, 1.0, 1.0], abi.EPP_ERR_INVALID_ARGUMENT),
+    (0.1, [0, 0, 0], [float("inf"), 1.0, 1.0], abi.EPP_ERR_CAPACITY),
+    (0.1, [0, 0, 0], [0.05, 1.0, 1.0], abi.EPP_ERR_INVALID_ARGUMENT),   # no cell on the x axis
+])
+def test_domains_that_overflow_the_cell_count_are_refused(gap, first, last, code):
+    """Both domain set-ups (the context's and the allocation-free cell sort's) check the cell
+    count after every axis: a 3D domain whose cell count overflows 64 bits, or an axis beyond
+    2^31 cells, is refused on the host, before anything is launched."""
+    d = abi.make_domain(3, gap, first, last)
+    with pytest.raises(epplib.EppError) as e:
+        epplib.context_bytes(abi.make_config(d, 1000, [[1, 1], [1, 0]]))
+    assert e.value.code == code
+    lib = epplib.load()
+    n_alive = C.c_int32(-1)
+    rc = lib.epp_cell_sort_noalloc(C.byref(d), 10, C.c_void_p(16), None, None, C.c_void_p(16),
+                                   C.byref(n_alive), None)
+    assert rc == code
+    assert n_alive.value == -1

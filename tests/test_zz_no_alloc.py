@@ -4,7 +4,8 @@ Some hosts drive the library from code that must not call cudaMalloc -- an appli
 fixed device pool, or a loop in the middle of a step where an allocation would synchronise the
 device.  This entry point keeps its intermediate arrays in a static device array of the library
 and works on buffers the caller passes in.  The test checks it against the context path
-(epp_search + epp_cell_stats) on two calls in a row, since every call reuses that same array.
+(epp_search + epp_cell_stats) and against the oracle's cell list on two calls in a row, since
+every call reuses that same array.
 The buffers below are the caller's (the test allocates them with torch); the entry point itself
 allocates nothing.  This file is collected last on purpose.
 """
@@ -33,6 +34,20 @@ def _context_cells(case, pos):
     out = d.ctx.cell_stats()
     d.close()
     return out
+
+
+def _oracle_cells(case, pos):
+    """Counts, offsets and sorted ids of the oracle's bucket insert (NeighbourSearch.jl:12-47)."""
+    from helpers import config_for
+    from oracle_lib import Oracle
+    ps = case.ps
+    ps["PositionVec"] = pos
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    o = Oracle(config_for(ps, ns, max_cell_particles=64 if case.meta["dim"] == 2 else 128), 32)
+    o.upload(ps.n_particles, ps.is_alive, ps.cell_index, ps.int_properties, ps.float_properties, ps.column_map())
+    o.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_NONE, case.physics)
+    oc, oo, oi = o.cell_stats(ps.n_particles)   # ids buffer sized for every particle
+    return oc, oo, oi[: int(oo[-1])]
 
 
 def _noalloc(domain, pos):
@@ -74,6 +89,10 @@ def test_noalloc_matches_context_path_twice(dim):
         assert np.array_equal(c, rc), "counts differ on call %d" % call
         assert np.array_equal(o, ro), "offsets differ on call %d" % call
         assert np.array_equal(ids, ri), "sorted ids differ on call %d" % call
+        # and the oracle's cell list of the same positions
+        oc, oo, oi = _oracle_cells(case, pos)
+        assert np.array_equal(c, oc) and np.array_equal(o, oo) and np.array_equal(ids, oi), \
+            "the oracle's cell list differs on call %d" % call
 
 
 def test_noalloc_rejects_oversize():
