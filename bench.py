@@ -28,18 +28,28 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import numpy as np  # noqa: E402
 
-# Algorithmic bytes per particle (FP32 components actually used, Int32 ids; neighbour data served
-# on chip, so each particle's record is read once and written once):
-#   whole step             2D 189 B, 3D 245 B
-#   momentum+integrate+bin reads x, v, rho, p, Kahan c, tag; writes x, v, c, cell   2D 64, 3D 88
-#   search                 reads x, h, tag; writes nCount                          2D 20, 3D 24
-#   continuity             reads x, h, v, m, rho, vol, tag; writes drho, (rho, p)', nCount
-#                                                                                    2D 52, 3D 60
+# Algorithmic bytes per particle per step: the compulsory traffic of a step in which each
+# particle's record is read and written once and neighbour data is served on chip (stage table):
+#   momentum pass      read x, v, rho, drho, id, Kahan c; write x, c, v, rho       2D 64,  3D 88
+#   hash + count       read x; write cell key; histogram atomic                    2D 16,  3D 20
+#   scan               8 B per cell, per particle                                  2D 5,   3D 0.5
+#   scatter / reorder  read key + rank; gather state; write sorted state           2D 80,  3D 104
+#   continuity         read x, v, id; write drho                                   2D 24,  3D 32
+#   whole step                                                                     2D 189, 3D 245
+# The six kernels of a step re-split those stages: the momentum pass also bins (momentum + hash
+# and count), the reorder is the scatter (key + rank, 8 B) and the rank-by-id gather (the rest),
+# and the continuity stage is split between the search pass (reads x and id) and the continuity
+# pass (reads v, writes drho).  The per-kernel figures add up to the whole step.
 B_ALG_STEP = {2: 189.0, 3: 245.0}
 STAGES = ["momentum_integrate_bin", "scan", "scatter", "rank_gather", "search", "continuity"]
-B_ALG_STAGE = {"momentum_integrate_bin": {2: 64.0, 3: 88.0}, "search": {2: 20.0, 3: 24.0},
-               "continuity": {2: 52.0, 3: 60.0}}
+B_ALG_STAGE = {"momentum_integrate_bin": {2: 80.0, 3: 108.0}, "scan": {2: 5.0, 3: 0.5},
+               "scatter": {2: 8.0, 3: 8.0}, "rank_gather": {2: 72.0, 3: 96.0},
+               "search": {2: 12.0, 3: 16.0}, "continuity": {2: 12.0, 3: 16.0}}
+PAIR_STAGES = ("momentum_integrate_bin", "search", "continuity")
 KERNEL_OF_STAGE = {"momentum_integrate_bin": "k_list<CPMom> (momentum + integrate + bin, fused)",
+                   "scan": "k_scan (decoupled look-back exclusive scan)",
+                   "scatter": "k_scatter (arrival-order scatter)",
+                   "rank_gather": "k_rank_gather (rank by id + state gather + density update)",
                    "search": "k_build (neighbour lists + nCount)",
                    "continuity": "k_list<CPCont> (continuity + density preview, fused)"}
 
@@ -47,7 +57,7 @@ KERNEL_OF_STAGE = {"momentum_integrate_bin": "k_list<CPMom> (momentum + integrat
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="epp", choices=["epp", "reference"])
     ap.add_argument("--case", default="2d", choices=["2d", "3d", "2d-small", "3d-small", "batch", "serve"])
@@ -67,7 +77,22 @@ def parse():
                     help="2D cases: the benchmark physics, or the reference example's own (CubicSpline, "
                          "linear EOS, classic viscosity, sAccelerateMove!, kernel filter every 20 steps)")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per particle (0 = tuned default)")
+    ap.add_argument("--no-served", dest="served", action="store_false",
+                    help="2D line: skip the batch and serve legs (batched and served sims/s)")
+    ap.add_argument("--no-parity", dest="parity", action="store_false",
+                    help="skip the untimed parity check of the workload against the oracle")
+    ap.add_argument("--leg-requests", type=int, default=16,
+                    help="2D line's serve leg: requests of the Poisson stream served (the first ones)")
     return ap.parse_args()
+
+
+def plain_config(case, label, world, flush=True):
+    """The workload keys of the plain-path line (the same in both arms)."""
+    m = case.meta
+    return {"workload": label, "particles": case.n, "fluid": m["n_fluid"], "walls": m["n_wall"],
+            "cells": m["n_cells"], "resort": "every step",
+            "l2": "flushed (256 MB write) before every timed step" if flush else "not flushed",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
 
 
 def make_case(name, physics="benchmark"):
@@ -175,6 +200,7 @@ def cpu_reference(case, steps_budget_s=20.0, max_steps=3, warmup=0):
         pairs += int(o.field(9, 0, ps.n_particles).sum())
         steps += 1
     return {"value": pairs / t_total, "unit": "pair-interactions/s", "cores": threads, "kind": "port",
+            "pairs_per_step": pairs / steps,
             "sample": "%d full steps of %s (%d particles), %.2f s" % (steps, case.meta.get("label", ""), ps.n_particles, t_total),
             "seconds_per_step": t_total / steps}
 
@@ -197,9 +223,10 @@ def run_reference(args):
     val = res["value"]
     out = {"metric": "SPH pair-interactions/s", "value": val, "unit": "pair-interactions/s",
            "impl": "reference", "n_gpus": args.gpus, "steps": k, "warmup": w,
-           "ms_per_step": res["seconds_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
+           "ms_per_step": res["seconds_per_step"] * 1e3, "pairs_per_step": res["pairs_per_step"],
+           "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (dam-break lattice generated in-process)",
-           "config": {"workload": label, "particles": case.n},
+           "config": plain_config(case, label, args.gpus, not args.no_flush),
            "cpu_baseline": {"value": val, "unit": "pair-interactions/s", "cores": res["cores"],
                             "kind": "port", "sample": res["sample"]},
            "e2e": {"value": val, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0,
@@ -566,6 +593,9 @@ def run_serve(args):
 
 def main():
     args = parse()
+    # more hardware queues than the default 8 for the serve leg's concurrent streams (set before
+    # the first CUDA call of the process)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if args.impl == "reference":
         return run_reference(args)
     if args.case == "batch":
@@ -599,8 +629,9 @@ def main():
     ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
     ctx.synchronize()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    W = max(args.warmup, 3)
     with torch.cuda.stream(stream):
-        ctx.step(max(args.warmup, 3), phys)
+        ctx.step(W, phys)
     ctx.synchronize()
     clocks = Clocks(local)
     # ---- timed region: K steps, L2 flushed before each, device time by CUDA events ----
@@ -642,8 +673,8 @@ def main():
                 flush.fill_(1.0)
             stage += np.array(ctx.profile_step(phys))
         stage /= nprof
-    # roofline of the dominant pair kernel (the larger of the two pair stages)
-    dom_stage = max(B_ALG_STAGE, key=lambda k: stage[STAGES.index(k)])
+    # roofline of the dominant kernel: the longest of the step's kernels
+    dom_stage = max(STAGES, key=lambda k: stage[STAGES.index(k)])
     dom_ms = float(stage[STAGES.index(dom_stage)])
     n = case.n
     achieved = B_ALG_STAGE[dom_stage][dim] * n / (dom_ms * 1e-3) / 1e9
@@ -666,7 +697,7 @@ def main():
     fp32_peak = fp32_peak_tflops(stream)
 
     # ---- end to end through the C ABI with host buffers (pinned) ----
-    e2e = run_e2e(dps, case, args, stream)
+    e2e = run_e2e(dps, case, args.steps, stream)
     if world > 1:   # whole job: every rank's pairs over the slowest rank's host time
         t = torch.tensor([e2e["value"] * e2e["seconds"], e2e["seconds"]], dtype=torch.float64, device="cuda")
         tmax = t.clone()
@@ -677,27 +708,29 @@ def main():
         e2e["note"] += "; pairs summed over %d ranks, time of the slowest" % world
 
     integ = ctx.integrals(phys)
+    dps.close()
+    del flush
+    torch.cuda.empty_cache()
     if rank == 0:
         step_bytes = B_ALG_STEP[dim] * n
+        step_ms = ms_max / args.steps
         out = {
             "metric": "SPH pair-interactions/s",
             "value": value,
             "unit": "pair-interactions/s",
             "n_gpus": world,
             "steps": args.steps,
-            "warmup": max(args.warmup, 3),
-            "ms_per_step": ms_max / args.steps,
+            "warmup": W,
+            "ms_per_step": step_ms,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (dam-break lattice generated in-process, hydrostatic density)",
-            "config": {"workload": label, "particles": n, "fluid": case.meta["n_fluid"],
-                       "walls": case.meta["n_wall"], "cells": case.meta["n_cells"],
-                       "pairs_per_step": pairs_all / args.steps / world, "resort": "every step",
-                       "l2": "flushed (256 MB write) before every timed step" if not args.no_flush else "not flushed",
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "step_hbm_gbs_algorithmic": step_bytes / (ms_max / args.steps * 1e-3) / 1e9},
+            "config": plain_config(case, label, world, not args.no_flush),
+            "pairs_per_step": pairs_all / args.steps / world,
+            "step_hbm_gbs_algorithmic": step_bytes / (step_ms * 1e-3) / 1e9,
+            "step_roofline_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak,
             # per fused step: momentum+integrate+bin, scan, scatter, rank+gather, search, continuity
             # (families other than 0 fuse search and continuity into one kernel)
             "gpu_launches": (6 if args.lanes == 0 else 5) * args.steps
@@ -709,9 +742,12 @@ def main():
                          "algorithmic_bytes_per_particle": B_ALG_STAGE[dom_stage][dim],
                          "kernel_ms": round(dom_ms, 5),
                          "stage_ms": dict(zip(STAGES, [round(x, 5) for x in stage])),
+                         "stage_frac": {k: round(B_ALG_STAGE[k][dim] * n / (stage[STAGES.index(k)] * 1e-3) / 1e9
+                                                 / peak, 4) for k in STAGES if stage[STAGES.index(k)] > 0},
                          "frac_of_nominal_8tbs": achieved / 8000.0,
-                         "compute": compute_roof(tr_case, stage, fp32_peak, clk),
-                         "note": "pair kernels are issue/latency bound, not HBM bound (ncu summaries in profiles/)"},
+                         "limiter": "instruction issue and neighbour-gather latency, not DRAM bandwidth (ncu: "
+                                    "DRAM 4-18% busy in the pair kernels; profiles/)",
+                         "compute": compute_roof(tr_case, stage, fp32_peak, clk)},
             "clocks": clk,
             "e2e": e2e,
             "device_status": st,
@@ -732,11 +768,242 @@ def main():
                 out["energy_drift"] = energy_drift_fp64(dcase, 20 if dim == 2 else 10, device=local)
             except Exception as exc:
                 out["energy_drift"] = {"error": str(exc)}
+            if args.parity:
+                try:
+                    out["parity"] = parity_block(args, dim, local)
+                except Exception as exc:
+                    out["parity"] = {"error": repr(exc)}
+            if args.served and args.case == "2d" and args.physics == "benchmark":
+                try:
+                    out["batch"] = measure_batch(local, steps=50, warmup=3, instances=256)
+                except Exception as exc:
+                    out["batch"] = {"error": repr(exc)}
+                try:
+                    out["serve"] = serve_legs(local, args, out["batch"])
+                except Exception as exc:
+                    out["serve"] = {"error": repr(exc)}
         print(json.dumps(out))
-    dps.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def parity_block(args, dim, device):
+    """Untimed: the workload's state after 10 fused steps checked against the oracle (cell list,
+    neighbour sets, dρ/dt and dv/dt against FP32 and FP64); 3D uses the dx = 0.02 tank."""
+    from epp import casegen
+    from scale_parity import scale_parity
+    t0 = time.perf_counter()
+    if dim == 2:
+        pcase = casegen.dam_break_2d(dx=0.002 if args.case == "2d" else 0.02, max_neighbour_number=40,
+                                     physics=args.physics)
+        r = scale_parity(pcase, 40, warm_steps=10, device=device)
+    else:
+        pcase = casegen.dam_break_3d(dx=0.02, max_neighbour_number=100)
+        r = scale_parity(pcase, 100, warm_steps=10, device=device)
+    out = {"case": "2D dam break dx=%g" % pcase.meta["dx"] if dim == 2 else "3D dam break dx=0.02 (3.2x1x1 tank)",
+           "particles": r["particles"], "scan_tiles": r["scan_tiles"], "cells": r["cells"], "ncount": r["ncount"],
+           "sets": r["sets"], "sets_rows_compared": r["sets_rows_compared"],
+           "drho_term_vs_fp32": r["drho"]["term_vs_fp32"], "dv_term_vs_fp32": r["dv"]["term_vs_fp32"],
+           "drho_rel": r["drho"]["rel_vs_fp32"], "dv_rel": r["dv"]["rel_vs_fp32"],
+           "vs_fp64": {"drho_term": r["drho"]["term_vs_fp64"], "dv_term": r["dv"]["term_vs_fp64"],
+                       "drho_rel": r["drho"]["rel_vs_fp64"], "dv_rel": r["dv"]["rel_vs_fp64"],
+                       "reference_fp32_drho_rel": r["drho"]["oracle_fp32_rel_vs_fp64"],
+                       "reference_fp32_dv_rel": r["dv"]["oracle_fp32_rel_vs_fp64"]},
+           "floors": {"drho": r["drho"]["floor"], "dv": r["dv"]["floor"]},
+           "bar": "bit-exact cells/sets; term-scale error < 1e-5",
+           "warm_steps": r["warm_steps"], "seconds": time.perf_counter() - t0}
+    out["within_bar"] = bool(r["cells"] and r["sets"] and r["drho"]["term_vs_fp32"] < 1e-5
+                             and r["dv"]["term_vs_fp32"] < 1e-5)
+    return out
+
+
+def plain_instance_ms(cases, device, stream, k=20):
+    """Device ms per step of each case alone on the plain path: one context sized for the largest
+    case, every case uploaded, searched, stepped 3 times untimed and `k` times timed (epp_step
+    graph, CUDA events on the context's stream)."""
+    import torch
+    from epp import abi, casegen
+    from epp.algorithm import DeviceParticleSystem
+    from epp.classes import NeighbourSystem
+    big = max(cases, key=lambda c: c.n)
+    ns1 = NeighbourSystem(big.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    plain = DeviceParticleSystem(big.ps, ns1, device=device)
+    pctx = plain.ctx
+    pctx.set_stream(stream.cuda_stream)
+    per_step = []
+    for c in cases:
+        q = c.ps
+        pctx.upload(q.n_particles, q.is_alive, q.cell_index, q.int_properties, q.float_properties, plain.cmap)
+        pctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, c.physics, 0)
+        with torch.cuda.stream(stream):
+            pctx.step(3, c.physics)
+        torch.cuda.synchronize()
+        a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a_.record(stream)
+            pctx.step(k, c.physics)
+            b_.record(stream)
+        torch.cuda.synchronize()
+        per_step.append(a_.elapsed_time(b_) / k)
+    plain.close()
+    return per_step
+
+
+def measure_batch(device, steps=50, warmup=3, instances=256, sim_steps=2000):
+    """Batch leg of the 2D line: the seeded mix of `instances` uneven 2D dam breaks (width
+    U[0.5, 1.5] m, height U[1.0, 2.5] m, dx = 0.01 m, each with its own c0 and dt) stepped as one
+    batch, every pass one launch over all instances; sims/s at `sim_steps` steps per simulation
+    from `steps` timed steps (L2 flushed before each), against the plain path running the same
+    instances one at a time (device time per instance step, 20 steps each)."""
+    import torch
+    from epp import abi, autotune, casegen
+    from epp.algorithm import DeviceParticleSystem
+    from epp.classes import NeighbourSystem
+    import oracle_lib
+    from helpers import config_for
+    SYM, CONT = abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY
+    t_leg = time.perf_counter()
+    b = casegen.dam_break_batch(instances, seed=0, dx=0.01)
+    phys = b.physics
+    ns = NeighbourSystem(b.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    tuned, tune_ms = autotune.tune_case(b, n_instances=b.n_instances, inst=(b.inst_dt, b.inst_c0), steps=5,
+                                        device=device)
+    dps = DeviceParticleSystem(b.ps, ns, device=device, n_instances=b.n_instances)
+    ctx = dps.ctx
+    ctx.set_instance_physics(b.inst_dt, b.inst_c0)
+    ctx.set_block_threads(tuned[1])
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    dps.syncto()
+    ctx.search(SYM, CONT, phys, 0)
+    e0 = [energy(x) for x in ctx.instance_integrals(phys, b.n_instances)]
+    with torch.cuda.stream(stream):
+        ctx.step(warmup, phys)
+    ctx.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    clocks = Clocks(device)
+    torch.cuda.synchronize()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            ctx.step(1, phys)
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    st = ctx.synchronize(raise_on_status=False)
+    ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
+    e1 = [energy(x) for x in ctx.instance_integrals(phys, b.n_instances)]
+    dps.close()
+    del flush
+    step_ms = ms / steps
+    sims_s = b.n_instances / (sim_steps * step_ms * 1e-3)
+    cases = [casegen.dam_break_2d(dx=0.01, column=col, max_neighbour_number=1) for col in b.meta["columns"]]
+    per_step = plain_instance_ms(cases, device, stream)
+    plain_sims_s = len(cases) / (sim_steps * sum(per_step) * 1e-3)
+    # energy drift against the FP64 oracle: the smallest and the largest instance, same steps
+    S = warmup + steps
+    order = sorted(range(len(cases)), key=lambda k: cases[k].n)
+    drift = {}
+    oracle_lib.set_threads(os.cpu_count() or 1)
+    for k in (order[0], order[-1]):
+        c = casegen.dam_break_2d(dx=0.01, column=b.meta["columns"][k], max_neighbour_number=60)
+        nso = NeighbourSystem(c.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=60)
+        o = oracle_lib.Oracle(config_for(c.ps, nso, max_cell_particles=64), 64)
+        q = c.ps
+        o.upload(q.n_particles, q.is_alive, q.cell_index, q.int_properties, q.float_properties, q.column_map())
+        o.search(SYM, CONT, c.physics)
+        o0 = energy(o.integrals(c.physics))
+        o.step(S, c.physics)
+        o1 = energy(o.integrals(c.physics))
+        dg, do = (e1[k] - e0[k]) / abs(e0[k]), (o1 - o0) / abs(o0)
+        drift[str(k)] = {"particles": c.n, "gpu_fp32": dg, "oracle_fp64": do, "abs_diff": abs(dg - do)}
+    return {"metric": "batched sims/s (%d-instance 2D dam-break mix, %d steps per simulation)"
+                      % (b.n_instances, sim_steps),
+            "value": sims_s, "unit": "sims/s", "steps": steps, "warmup": warmup, "ms_per_step": step_ms,
+            "config": {"workload": "%d uneven 2D dam breaks, width U[0.5,1.5] m, height U[1.0,2.5] m, dx=0.01 m, "
+                                   "seed 0" % b.n_instances, "particles": b.n,
+                       "fluid_per_instance": [min(b.meta["inst_n_fluid"]), max(b.meta["inst_n_fluid"])],
+                       "cells": b.meta["n_cells"], "dt": "per instance (0.1 h / c0_k)",
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "plain_path": {"sims_per_s": plain_sims_s, "ms_per_instance_step_mean": float(np.mean(per_step)),
+                           "ms_per_instance_step": [round(x, 5) for x in per_step],
+                           "method": "each instance alone on the plain path (epp_step graph), 20 steps timed by "
+                                     "CUDA events per instance, summed over the instances"},
+            "speedup_vs_plain": sims_s / plain_sims_s,
+            "autotune": {"family": tuned[0], "block_threads": tuned[1], "resort_every": 1},
+            "energy_drift": {"steps": S, "bar": 1e-4, "instances": drift,
+                             "max_abs_diff": max(v["abs_diff"] for v in drift.values())},
+            "gpu_launches": 6 * steps, "clocks": clk, "device_status": st,
+            "leg_seconds": time.perf_counter() - t_leg}
+
+
+def serve_legs(device, args, batch):
+    """Serve leg of the 2D line.  (a) The batch leg's instance mix as requests arriving at once,
+    co-batched by the Python serving loop (2000 steps each): sims/s and p50/p99 completion latency;
+    its one-at-a-time baseline is the batch leg's per-instance plain-path device time, run in FIFO
+    order (completion of request k = sum of the first k runs; host work not counted, which favours
+    the baseline).  (b) The first `args.leg_requests` requests of the seeded Poisson stream (mean
+    50 req/s, 70% 2D / 30% 3D, 1e3-1e6 fluid particles, 2000 steps each) served with continuous
+    batching under a 120 GB budget and, for the baseline, the same requests one at a time
+    (max_active = 1); default launch configuration (no autotuner), both measured on the host clock."""
+    from epp import serve
+    t_leg = time.perf_counter()
+    be = serve.DeviceBackend(device=device)
+    out = {}
+    # warm-up: one small request of each dimension (module load, first graph builds)
+    warm = [s for s in serve.request_stream(16, seed=99, n_range=(1e3, 3e3), steps=10)]
+    warm = [next(s for s in warm if s.dim == 2), next(s for s in warm if s.dim == 3)]
+    for s in warm:
+        s.arrival = 0.0
+    serve.Server(be).run(serve.make_runs(warm, be))
+    # (a) the instance mix, co-batched
+    specs = serve.batch_mix_requests(256, steps=2000)
+    runs = serve.make_runs(specs, be)
+    clocks = Clocks(device)
+    clocks.start()
+    st = serve.Server(be, budget_bytes=120 * 10**9, co_batch=True).run(runs)
+    clk = clocks.stop()
+    per = batch["plain_path"]["ms_per_instance_step"] if isinstance(batch, dict) and "plain_path" in batch else None
+    mix = {"workload": "the batch leg's 256-instance mix as requests arriving at once, 2000 steps each, co-batched",
+           "sims_per_s": st["sims_per_s"], "latency_p50_s": st["latency_p50_s"], "latency_p99_s": st["latency_p99_s"],
+           "makespan_s": st["makespan_s"], "completed": st["completed"], "clocks": clk}
+    if per:
+        done = np.cumsum(np.array(per) * 2000 * 1e-3)
+        mix["plain_path"] = {"sims_per_s": len(per) / float(done[-1]), "latency_p50_s": float(np.percentile(done, 50)),
+                             "latency_p99_s": float(np.percentile(done, 99)),
+                             "method": "per-instance plain-path device time x 2000 steps, FIFO one at a time"}
+        mix["speedup_vs_plain"] = mix["sims_per_s"] / mix["plain_path"]["sims_per_s"]
+    out["mix"] = mix
+    # (b) the Poisson stream
+    specs = serve.request_stream(32, seed=0, steps=2000)[: args.leg_requests]
+    runs = serve.make_runs(specs, be)
+    clocks = Clocks(device)
+    clocks.start()
+    st = serve.Server(be, budget_bytes=120 * 10**9, co_batch=True).run(runs)
+    clk = clocks.stop()
+    plain_runs = serve.make_runs(specs, be)
+    pl = serve.Server(be, budget_bytes=120 * 10**9, max_active=1).run(plain_runs)
+    n_p = [r.case.n for r in runs]
+    out["stream"] = {"workload": "first %d requests of the seeded Poisson stream (mean 50 req/s, 70%% 2D / 30%% 3D, "
+                                 "fluid log-uniform 1e3-1e6, 2000 steps each)" % len(specs),
+                     "requests_2d": sum(1 for s in specs if s.dim == 2),
+                     "requests_3d": sum(1 for s in specs if s.dim == 3),
+                     "particles_range": [min(n_p), max(n_p)],
+                     "sims_per_s": st["sims_per_s"], "latency_p50_s": st["latency_p50_s"],
+                     "latency_p99_s": st["latency_p99_s"], "makespan_s": st["makespan_s"],
+                     "max_concurrent": st["max_concurrent"], "clocks": clk,
+                     "plain_path": {"sims_per_s": pl["sims_per_s"], "latency_p50_s": pl["latency_p50_s"],
+                                    "latency_p99_s": pl["latency_p99_s"],
+                                    "method": "same requests one at a time (max_active = 1), same kernels"},
+                     "speedup_vs_plain": st["sims_per_s"] / pl["sims_per_s"] if pl["sims_per_s"] else None}
+    out["budget_bytes"] = 120 * 10**9
+    out["leg_seconds"] = time.perf_counter() - t_leg
+    return out
 
 
 def fp32_peak_tflops(stream):
@@ -823,51 +1090,84 @@ def energy_drift_fp64(case, steps, device=0):
             "bar": 1e-4, "within_bar": abs(dg - do) <= 1e-4}
 
 
-def run_e2e(dps, case, args, stream):
-    """Same metric through the public C ABI with host (pinned) buffers: upload of the reference-
-    layout matrices, K x (epp_step + FP64 integrals read back), download; host wall clock."""
+def pinned_copy(a, order="F"):
+    """A copy of numpy array `a` in page-locked host memory with the given element order; returns
+    (torch tensor that owns the memory, numpy view of it)."""
     import torch
+    tt = {np.dtype(np.float32): torch.float32, np.dtype(np.int32): torch.int32}[a.dtype]
+    t = torch.empty(max(a.size, 1), dtype=tt, pin_memory=True)
+    v = t.numpy()[: a.size].reshape(a.shape, order=order)
+    v[...] = a
+    assert t.is_pinned() and np.shares_memory(v, t.numpy())
+    assert v.flags.f_contiguous if order == "F" else v.flags.c_contiguous
+    return t, v
+
+
+def run_e2e(dps, case, K, stream, reps=5):
+    """Same metric through the public C ABI with host buffers in page-locked memory (allocated once,
+    column-major like the reference's matrices): upload, initial search, K x (epp_step + that
+    step's FP64 integrals read back, one step in flight), download.  Host clock; the region is
+    repeated `reps` times (each continuing from the last state) and the median is reported, with
+    its phases (each phase ends with the device idle).  Pairs: the K steps' searches only."""
     ps = dps.host
     ctx = dps.ctx
     phys = case.physics
-    ip = torch.from_numpy(np.asfortranarray(ps.int_properties)).pin_memory().numpy()
-    fp = torch.from_numpy(np.asfortranarray(ps.float_properties)).pin_memory().numpy()
-    ip = np.asfortranarray(ip)
-    fp = np.asfortranarray(fp)
-    alive = torch.from_numpy(ps.is_alive.copy()).pin_memory().numpy()
-    cell = torch.from_numpy(ps.cell_index.copy()).pin_memory().numpy()
-    # download once so the host matrices hold the current state, then time a full run
-    ctx.download(alive, cell, ip, fp, dps.cmap)
-    K = args.steps
-    p0 = ctx.pairs_total()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ctx.upload(ps.n_particles, alive, cell, ip, fp, dps.cmap)
-    ctx.search(1, 1, phys, 0)
-    # every step's FP64 integrals are read back; step k + 1 is queued before step k's are waited
-    # for, so the host turnaround of the read-back overlaps the next step
-    pending = None
-    for _ in range(K):
-        ctx.step(1, phys)
-        t = ctx.integrals_async(phys)
-        if pending is not None:
-            ctx.integrals_wait(pending)
-        pending = t
-    ctx.integrals_wait(pending)
-    ctx.download(alive, cell, ip, fp, dps.cmap)
-    t1 = time.perf_counter()
-    pairs = ctx.pairs_total() - p0
+    keep = []
+    bufs = {}
+    for name, arr, order in (("ip", ps.int_properties, "F"), ("fp", ps.float_properties, "F"),
+                             ("alive", ps.is_alive, "C"), ("cell", ps.cell_index, "C")):
+        t, v = pinned_copy(np.asarray(arr), order)
+        keep.append(t)
+        bufs[name] = v
+    ip, fp, alive, cell = bufs["ip"], bufs["fp"], bufs["alive"], bufs["cell"]
+    ctx.download(alive, cell, ip, fp, dps.cmap)   # the host matrices hold the current state
+    runs = []
+    for _ in range(reps):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        ctx.upload(ps.n_particles, alive, cell, ip, fp, dps.cmap)
+        ctx.synchronize()
+        t1 = time.perf_counter()
+        ctx.search(1, 1, phys, 0)
+        ctx.synchronize()
+        t2 = time.perf_counter()
+        p0 = ctx.pairs_total()
+        t2b = time.perf_counter()
+        pending = None
+        for _ in range(K):
+            ctx.step(1, phys)
+            t = ctx.integrals_async(phys)
+            if pending is not None:
+                ctx.integrals_wait(pending)
+            pending = t
+        ctx.integrals_wait(pending)
+        t3 = time.perf_counter()
+        p1 = ctx.pairs_total()
+        t3b = time.perf_counter()
+        ctx.download(alive, cell, ip, fp, dps.cmap)
+        t4 = time.perf_counter()
+        total = (t4 - t0) - (t2b - t2) - (t3b - t3)   # the pair-count reads are bookkeeping
+        runs.append({"seconds": total, "pairs": p1 - p0, "upload_s": t1 - t0, "search_s": t2 - t1,
+                     "steps_with_readback_s": t3 - t2b, "download_s": t4 - t3b})
+    runs.sort(key=lambda r: r["seconds"])
+    med = runs[len(runs) // 2]
     cm = dps.cmap
-    ncols_f = sum(w for c, w in [(cm.position, case.meta["dim"]), (cm.velocity, case.meta["dim"]),
-                                 (cm.dvelocity, case.meta["dim"]), (cm.mass, 1), (cm.volume, 1), (cm.density, 1),
-                                 (cm.ddensity, 1), (cm.pressure, 1), (cm.h, 1)] if c >= 0)
-    ncols_i = 2 + sum(1 for c in (cm.tag, cm.is_movable, cm.n_count) if c >= 0)
+    d = case.meta["dim"]
+    ncols_f = sum(w for c, w in [(cm.position, d), (cm.velocity, d), (cm.dvelocity, d), (cm.mass, 1), (cm.volume, 1),
+                                 (cm.density, 1), (cm.ddensity, 1), (cm.pressure, 1), (cm.h, 1), (cm.gap, 1)]
+                  if c >= 0)
+    ncols_i = 2 + sum(1 for c in (cm.tag, cm.is_movable, cm.n_count, cm.instance) if c >= 0)
     n = ps.n_particles
-    h2d = (n * 4 * (ncols_f + ncols_i)) / K + 64
-    d2h = (n * 4 * (ncols_f + ncols_i)) / K + 72
-    return {"value": pairs / (t1 - t0), "unit": "pair-interactions/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "seconds": t1 - t0,
-            "note": "upload + initial search + K x (step + integrals read back, one step in flight) + download, host clock"}
+    h2d = n * 4 * (ncols_f + ncols_i)
+    d2h = n * 4 * (ncols_f + ncols_i - (1 if cm.instance >= 0 else 0)) + 72 * K
+    return {"value": med["pairs"] / med["seconds"], "unit": "pair-interactions/s",
+            "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K), "seconds": med["seconds"],
+            "steps": K, "repeats": reps, "phases_s": {k: med[k] for k in ("upload_s", "search_s",
+                                                                          "steps_with_readback_s", "download_s")},
+            "seconds_all": [round(r["seconds"], 6) for r in runs],
+            "host_buffers": "page-locked, column-major, allocated once",
+            "note": "upload + initial search + K x (step + integrals read back, one step in flight) + download, "
+                    "host clock, median of %d; pairs of the K steps' searches" % reps}
 
 
 if __name__ == "__main__":

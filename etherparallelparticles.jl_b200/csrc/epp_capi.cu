@@ -3,6 +3,7 @@
 // graph-captured dam-break step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -133,6 +134,20 @@ struct epp_ctx {
     float inst_rho0 = 0.0f;
     int inst_gamma = 0;
     double* inst_out = nullptr;         // device [n_inst * 9] integrals
+    // CFL time stepping (epp_physics.cfl > 0): tbl[set][k] holds instance k's dt (and c0, B) for the
+    // step that starts from the state in buffer set `set`; the fused step of parity c reads tbl[c]
+    // and its k_cfl writes tbl[1 - c] for the state it produces
+    InstPhys* tbl[2]{};
+    double2* cfl_partial = nullptr;     // [n_inst * cfl_chunks]
+    unsigned* cfl_ticket = nullptr;
+    double* sim_time = nullptr;         // [n_inst] simulated time of steps taken with a CFL dt
+    int cfl_chunks = 1;
+    int graph_fluid = 1;                // fluid tag k_cfl reduces over
+    bool cfl_tables_ok = false;         // c0 and B of both tables match tbl_c0 / tbl_key
+    bool cfl_valid = false;             // tbl[cur].dt is the CFL dt of the current state
+    float tbl_rho0 = 0.0f, tbl_c0 = 0.0f;
+    int tbl_gamma = 0;
+    std::vector<double> time_fixed;     // simulated time of steps taken with a fixed dt, per instance
     // fused step graphs, one per ping-pong parity
     cudaGraphExec_t graph[2]{};
     cudaGraphExec_t graph_f[2]{};   // the same step followed by the kernel filter
@@ -145,6 +160,7 @@ struct epp_ctx {
     long long iticket_next = 0;
     long long islot_ticket[EPP_INTEGRALS_SLOTS]{-1, -1, -1, -1};
     float islot_c0[EPP_INTEGRALS_SLOTS]{};
+    float islot_cfl[EPP_INTEGRALS_SLOTS]{};
     bool timed = false;
     std::string err;
 };
@@ -209,36 +225,11 @@ void dev_free(epp_ctx* ctx, T*& p) {
     p = nullptr;
 }
 
-// Cells of the grid (all instances) and scan tiles of a configuration; false if it is invalid.
-bool plan_cells(const epp_config* cfg, DevDomain& d, long long& ncell) {
-    const int D = cfg->domain.dim;
-    d.dim = D;
-    const float gap = cfg->domain.gap;
-    d.gap_square = gap * gap;
-    ncell = 1;
-    for (int a = 0; a < 3; ++a) {
-        d.n[a] = 1;
-        d.first[a] = d.last[a] = 0.0f;
-        d.gap_inv[a] = 1.0f;
-    }
-    for (int a = 0; a < D; ++a) {
-        d.first[a] = cfg->domain.first[a];
-        d.last[a] = cfg->domain.last[a];
-        const float span = d.last[a] - d.first[a];
-        volatile float q = span / gap;
-        const int na = (int)floorf(q);
-        if (na < 1) return false;
-        d.n[a] = na;
-        volatile float ga = span / (float)na;
-        d.gap_inv[a] = 1.0f / ga;
-        ncell *= na;
-    }
+// Cells of the grid (all instances) of a configuration: EPP_OK, or the status that rejects it.
+int plan_cells(const epp_config* cfg, DevDomain& d) {
     const int n_inst = cfg->n_instances > 1 ? cfg->n_instances : 1;
-    if ((D == 3 && n_inst > 1) || ncell * n_inst > (1ll << 30) || n_inst > (1 << 22)) return false;
-    d.cells_per_inst = (int)ncell;
-    d.n_inst = n_inst;
-    d.n_cells = (int)(ncell * n_inst);
-    return true;
+    if (cfg->domain.dim == 3 && n_inst > 1) return EPP_ERR_INVALID_ARGUMENT;   // batches are 2D
+    return plan_domain(cfg->domain, n_inst, 1ll << 30, d);
 }
 
 size_t nlist_bytes(int D, int cap) {
@@ -263,9 +254,41 @@ void fill_state(Arena& a, State& s, int cap) {
     s.rp4 = a.take<float4>(cap);
 }
 
-// Device physics of a call: the per-instance table (uploaded when it changed) overrides dt, c0, B.
+// The CFL tables (epp_physics.cfl > 0): c0 and B of every instance (its own c0 in a batch with
+// instance physics, phys.c0 otherwise) in both buffer sets; their dt fields are written on the
+// device by k_cfl.  Re-uploading them invalidates the current CFL dt.
+void ensure_cfl_tables(epp_ctx* ctx, const epp_physics& p) {
+    if (ctx->cfl_tables_ok && ctx->tbl_rho0 == p.rho0 && ctx->tbl_gamma == p.gamma &&
+        (!ctx->inst_c0.empty() || ctx->tbl_c0 == p.c0))
+        return;
+    std::vector<InstPhys> t(ctx->n_inst);
+    for (int k = 0; k < ctx->n_inst; ++k) {
+        const float c0 = ctx->inst_c0.empty() ? p.c0 : ctx->inst_c0[k];
+        t[k].dt = ctx->inst_dt.empty() ? p.dt : ctx->inst_dt[k];
+        t[k].c0 = c0;
+        t[k].B = (float)((double)p.rho0 * (double)c0 * (double)c0 / (double)p.gamma);
+        t[k].pad = 0.0f;
+    }
+    for (int b = 0; b < 2; ++b)
+        cudaMemcpyAsync(ctx->tbl[b], t.data(), sizeof(InstPhys) * ctx->n_inst, cudaMemcpyHostToDevice, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->cfl_tables_ok = true;
+    ctx->tbl_rho0 = p.rho0;
+    ctx->tbl_gamma = p.gamma;
+    ctx->tbl_c0 = p.c0;
+    ctx->cfl_valid = false;
+}
+
+// Device physics of a call: the per-instance table (uploaded when it changed) overrides dt, c0, B;
+// with a CFL physics, the CFL table of the current buffer set does.
 DevPhys dev_phys(epp_ctx* ctx, const epp_physics& p) {
     DevPhys d = to_dev(p);
+    if (p.cfl > 0.0f) {
+        ensure_cfl_tables(ctx, p);
+        d.ip = ctx->tbl[ctx->cur];
+        d.gap = ctx->gap;
+        return d;
+    }
     if (!ctx->inst_dt.empty()) {
         if (ctx->inst_dirty || ctx->inst_rho0 != p.rho0 || ctx->inst_gamma != p.gamma) {
             std::vector<InstPhys> t(ctx->n_inst);
@@ -302,6 +325,43 @@ PairArgs pair_args(epp_ctx* ctx, int set, int crit) {
 }
 
 int lanes_of(const epp_ctx* ctx) { return ctx->lanes; }
+
+// k_cfl over the state in buffer set `set` (FUSED: the momentum pass's output of a step from set
+// `set`), writing `next`; `used` (or null) is the table of the step just taken, added to the time.
+template <int D, bool FUSED>
+int launch_cfl(epp_ctx* ctx, int set, float cfl, const InstPhys* used, InstPhys* next) {
+    CflArgs a;
+    a.start = ctx->start[set];
+    a.cells_per_inst = ctx->dom.cells_per_inst;
+    a.n_inst = ctx->n_inst;
+    a.n_cells = ctx->n_cells;
+    a.n_max = ctx->n;
+    a.chunks = ctx->cfl_chunks;
+    a.vm = FUSED ? ctx->tmp.vm : ctx->S[set].vm;
+    a.xh = FUSED ? ctx->tmp.xh : ctx->S[set].xh;
+    a.tagm = ctx->S[set].tagm;
+    a.cs = ctx->cs;
+    a.fluid = ctx->graph_fluid;
+    a.cfl = cfl;
+    a.used = used;
+    a.next = next;
+    a.partial = ctx->cfl_partial;
+    a.time = ctx->sim_time;
+    a.ticket = ctx->cfl_ticket;
+    k_cfl<D, FUSED><<<ctx->n_inst * ctx->cfl_chunks, 256, 0, ctx->stream>>>(a);
+    CK_LAUNCH();
+    return EPP_OK;
+}
+
+// The CFL dt of the current state into its table (tbl[cur]).
+template <int D>
+int cfl_update(epp_ctx* ctx, const epp_physics& p) {
+    ensure_cfl_tables(ctx, p);
+    ctx->graph_fluid = p.fluid_tag;
+    const int rc = launch_cfl<D, false>(ctx, ctx->cur, p.cfl, nullptr, ctx->tbl[ctx->cur]);
+    if (rc == EPP_OK) ctx->cfl_valid = true;
+    return rc;
+}
 
 // Physics that needs the generic pair terms (any kernel, classic viscosity); the benchmark physics
 // (Wendland C2, artificial viscosity) runs the specialised ones.
@@ -525,6 +585,11 @@ int run_search(epp_ctx* ctx, int crit, int action, const epp_physics* phys, bool
     }
     int rc = sort_cells<D>(ctx);
     if (rc) return rc;
+    ctx->cfl_valid = false;   // a new buffer set
+    if (phys && phys->cfl > 0.0f && action == EPP_ACTION_DAMBREAK_CONTINUITY) {
+        rc = cfl_update<D>(ctx, *phys);   // the continuity pass previews the next step's density
+        if (rc) return rc;
+    }
     rc = launch_search_pass<D>(ctx, ctx->cur, crit, action, phys, emit, false);
     if (rc) return rc;
     ctx->searched = true;
@@ -559,6 +624,13 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     mom.F.accel = ctx->graph_accel ? ctx->accel : nullptr;
     mom.status = ctx->status;
     const bool gen = generic_physics(&phys);
+    const bool cfl = phys.cfl > 0.0f;
+    // passes after the momentum pass preview the next step's density: the next step's dt
+    DevPhys Pn = mom.P;
+    if (cfl) {   // this step takes tbl[c]; its k_cfl writes tbl[1 - c] for the state it produces
+        mom.P.ip = ctx->tbl[c];
+        Pn.ip = ctx->tbl[to];
+    }
     {
         auto mom_pass = [&](auto G) {
             constexpr bool GG = decltype(G)::value;
@@ -569,6 +641,11 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
         };
         const int rc0 = gen ? mom_pass(std::true_type{}) : mom_pass(std::false_type{});
         if (rc0) return rc0;
+        if (cfl) {
+            ctx->graph_fluid = phys.fluid_tag;
+            const int rc1 = launch_cfl<D, true>(ctx, c, phys.cfl, ctx->tbl[c], ctx->tbl[to]);
+            if (rc1) return rc1;
+        }
     }
     EPP_MARK(1);
     k_scan<<<ctx->n_tiles, kScanThreads, 0, ctx->stream>>>(ctx->n_cells + 1, ctx->count, ctx->start[to],
@@ -590,8 +667,8 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
         rc = launch_build<D>(ctx, to, EPP_CRITERION_SYMMETRY, ctx->pairs);
         if (rc) return rc;
         EPP_MARK(5);
-        rc = gen ? launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], mom.P, ctx->ncount})
-                 : launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], mom.P, ctx->ncount});
+        rc = gen ? launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], Pn, ctx->ncount})
+                 : launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], Pn, ctx->ncount});
         if (rc) return rc;
     } else {
         rc = launch_search_pass<D>(ctx, to, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false,
@@ -601,14 +678,14 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     }
     EPP_MARK(6);
     if (filter) {   // the kernel filter after this step's search (main.jl:180-183), family 0
-        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPFilter<D>{ctx->S[to], mom.P, ctx->fwv, ctx->fwr});
+        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPFilter<D>{ctx->S[to], Pn, ctx->fwv, ctx->fwr});
         if (rc) return rc;
         k_filter_finish<D><<<blocks_for(n), kThreads, 0, ctx->stream>>>(ctx->start[to], ctx->n_cells, n, ctx->S[to],
-                                                                        mom.P, ctx->fwv, ctx->fwr, 1);
+                                                                        Pn, ctx->fwv, ctx->fwr, 1);
         CK_LAUNCH();
     }
     if (phys.wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE) {   // wall pressure of the previewed density
-        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPExtrap<D, true>{ctx->S[to], mom.P, nullptr, nullptr});
+        rc = launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPExtrap<D, true>{ctx->S[to], Pn, nullptr, nullptr});
         if (rc) return rc;
     }
 #undef EPP_MARK
@@ -660,6 +737,11 @@ int build_graphs(epp_ctx* ctx, const epp_physics& phys) {
 
 template <int D>
 int run_selfaction(epp_ctx* ctx, int action, const epp_physics* phys) {
+    if (phys && phys->cfl > 0.0f && !ctx->cfl_valid &&
+        (action == EPP_ACTION_DAMBREAK_DENSITY || action == EPP_ACTION_DAMBREAK_INTEGRATE)) {
+        const int rc = cfl_update<D>(ctx, *phys);   // the dt of the step that starts from this state
+        if (rc) return rc;
+    }
     DevPhys P = phys ? dev_phys(ctx, *phys) : DevPhys{};
     if (action == EPP_ACTION_KERNEL_FILTER_SELF) {
         k_filter_finish<D><<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
@@ -737,10 +819,18 @@ int run_interaction(epp_ctx* ctx, int action, const epp_physics* phys) {
     return launch_interaction_pass<D>(ctx, CPCountDv<D>{ctx->S[ctx->cur]});
 }
 
+// Simulated time of `n` steps with a fixed dt (host bookkeeping; CFL steps add on the device).
+void advance_fixed_time(epp_ctx* ctx, const epp_physics& phys, long long n) {
+    for (int k = 0; k < ctx->n_inst; ++k)
+        ctx->time_fixed[k] += (double)n * (double)(ctx->inst_dt.empty() ? phys.dt : ctx->inst_dt[k]);
+}
+
 template <int D>
 int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     int rc;
+    const bool cfl = phys.cfl > 0.0f;
     if (ctx->inst_dirty) dev_phys(ctx, phys);   // upload the per-instance table the graphs read
+    if (cfl) ensure_cfl_tables(ctx, phys);
     if (ctx->dv_dirty) {
         // the first step goes through the per-call kernels, which honour a non-zero dVelocity
         rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_DENSITY, &phys);
@@ -750,6 +840,15 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         }
         if (!rc) rc = run_interaction<D>(ctx, EPP_ACTION_DAMBREAK_MOMENTUM, &phys);
         if (!rc) rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_INTEGRATE, &phys);
+        if (!rc) {
+            ctx->cfl_valid = false;   // the velocities moved on
+            if (cfl) {
+                k_advance_time<<<1, 256, 0, ctx->stream>>>(ctx->n_inst, ctx->tbl[ctx->cur], ctx->sim_time);
+                CK_LAUNCH();
+            } else {
+                advance_fixed_time(ctx, phys, 1);
+            }
+        }
         if (!rc) rc = run_search<D>(ctx, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false);
         if (rc) return rc;
         ++ctx->step_count;
@@ -767,6 +866,11 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         if (n_steps == 0) return EPP_OK;
     }
     const bool extrap = phys.wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE;
+    if (cfl && !ctx->cfl_valid) {   // the graph's first step takes the CFL dt of this state
+        rc = cfl_update<D>(ctx, phys);
+        if (rc) return rc;
+        ctx->rpn_valid = false;
+    }
     if (!ctx->rpn_valid || !same_phys(ctx->rpn_phys, phys)) {
         k_density_preview<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
             ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], dev_phys(ctx, phys));
@@ -792,6 +896,8 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         CK(cudaGraphLaunch(f ? ctx->graph_f[ctx->cur] : ctx->graph[ctx->cur], ctx->stream));
         ctx->cur = 1 - ctx->cur;
     }
+    if (!cfl) advance_fixed_time(ctx, phys, n_steps);
+    ctx->cfl_valid = cfl;   // each step's k_cfl left the dt of the state it produced
     ctx->rpn_valid = true;
     ctx->rpn_walls = extrap;
     ctx->rpn_phys = phys;
@@ -828,6 +934,10 @@ int check_physics(epp_ctx* ctx, const epp_physics* p) {
                     "the lane-group pair passes run the dam break's pressure terms; use family 0 or 1");
     if (ctx->lanes != 0 && p->wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE)
         return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the pressure extrapolation runs on pair-pass family 0");
+    if (!(p->cfl >= 0.0f && p->cfl < 1e30f))
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "cfl %g out of range", (double)p->cfl);
+    if (ctx->lanes != 0 && p->cfl > 0.0f)
+        return fail(ctx, EPP_ERR_UNSUPPORTED_ACTION, "the CFL time step runs on pair-pass family 0");
     return EPP_OK;
 }
 
@@ -868,10 +978,9 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->cap = cfg->n_capacity;
     // domain in FP32 exactly as Domain2D (Domain2D.jl:34-66)
     DevDomain& d = ctx->dom;
-    long long ncell = 1;
-    if (!plan_cells(cfg, d, ncell)) {
+    if (const int prc = plan_cells(cfg, d)) {
         delete ctx;
-        return EPP_ERR_INVALID_ARGUMENT;
+        return prc;
     }
     const int n_inst = d.n_inst;
     ctx->n_inst = n_inst;
@@ -898,6 +1007,7 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
         return EPP_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->dev);
     if (dev_alloc(ctx, &ctx->arena.base, need) != cudaSuccess) {
         cudaGetLastError();
         epp_destroy(ctx);
@@ -945,9 +1055,16 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
         epp_destroy(ctx);
         return EPP_ERR_BUDGET;
     }
+    ctx->cfl_chunks = std::max(1, (4 * ctx->sms) / n_inst);
+    ctx->time_fixed.assign(n_inst, 0.0);
     if (dev_alloc(ctx, &ctx->nlist, nlist_bytes(D, ctx->cap)) != cudaSuccess ||
         dev_alloc(ctx, &ctx->inst_table, sizeof(InstPhys) * n_inst) != cudaSuccess ||
-        dev_alloc(ctx, &ctx->inst_out, sizeof(double) * 9 * n_inst) != cudaSuccess) {
+        dev_alloc(ctx, &ctx->inst_out, sizeof(double) * 9 * n_inst) != cudaSuccess ||
+        dev_alloc(ctx, &ctx->tbl[0], sizeof(InstPhys) * n_inst) != cudaSuccess ||
+        dev_alloc(ctx, &ctx->tbl[1], sizeof(InstPhys) * n_inst) != cudaSuccess ||
+        dev_alloc(ctx, &ctx->cfl_partial, sizeof(double2) * n_inst * ctx->cfl_chunks) != cudaSuccess ||
+        dev_alloc(ctx, &ctx->cfl_ticket, sizeof(unsigned)) != cudaSuccess ||
+        dev_alloc(ctx, &ctx->sim_time, sizeof(double) * n_inst) != cudaSuccess) {
         cudaGetLastError();
         epp_destroy(ctx);
         return EPP_ERR_OUT_OF_MEMORY;
@@ -955,12 +1072,13 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     // zeroed lists: a list slot read before any search wrote it holds index 0, in bounds
     if (cudaMemsetAsync(ctx->arena.base, 0, need, ctx->stream) != cudaSuccess ||
         cudaMemsetAsync(ctx->nlist, 0, nlist_bytes(D, ctx->cap), ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(ctx->cfl_ticket, 0, sizeof(unsigned), ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(ctx->sim_time, 0, sizeof(double) * n_inst, ctx->stream) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         epp_destroy(ctx);
         return EPP_ERR_CUDA;
     }
-    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->dev);
     if ((D == 2 ? prepare_kernels<2>(ctx) : prepare_kernels<3>(ctx)) != EPP_OK) {
         epp_destroy(ctx);
         return EPP_ERR_CUDA;
@@ -979,6 +1097,11 @@ int32_t epp_destroy(epp_ctx* ctx) {
     dev_free(ctx, ctx->inst_table);
     dev_free(ctx, ctx->nlist);
     dev_free(ctx, ctx->inst_out);
+    dev_free(ctx, ctx->tbl[0]);
+    dev_free(ctx, ctx->tbl[1]);
+    dev_free(ctx, ctx->cfl_partial);
+    dev_free(ctx, ctx->cfl_ticket);
+    dev_free(ctx, ctx->sim_time);
     dev_free(ctx, ctx->list_mem);
     dev_free(ctx, ctx->list_stage);
     dev_free(ctx, ctx->arena.base);
@@ -1003,6 +1126,7 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     if (ldi < n || ldf < n) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "leading dimension < n");
     cudaSetDevice(ctx->dev);
     const int D = ctx->D;
+    const bool same_n = n == ctx->n;
     ctx->n = n;
     if (n == 0) {
         drop_graphs(ctx);
@@ -1078,7 +1202,9 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     if (D == 2) launch(std::integral_constant<int, 2>{});
     else launch(std::integral_constant<int, 3>{});
     CK_LAUNCH();
-    drop_graphs(ctx);   // the captured launches hold the old particle count
+    // the captured step graphs hold the particle count (grid sizes, bounds) and otherwise only the
+    // context's own buffers: they stay valid for an upload of the same count
+    if (!same_n) drop_graphs(ctx);
     CK(cudaMemsetAsync(ctx->fwv, 0, sizeof(float) * ctx->cap, ctx->stream));
     CK(cudaMemsetAsync(ctx->fwr, 0, sizeof(float) * ctx->cap, ctx->stream));
     CK(cudaMemsetAsync(ctx->fwp, 0, sizeof(float) * ctx->cap, ctx->stream));
@@ -1091,6 +1217,9 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     ctx->extrap_pending = false;
     ctx->rpn_walls = false;
     ctx->step_count = 0;
+    ctx->cfl_valid = false;
+    ctx->time_fixed.assign(ctx->n_inst, 0.0);
+    CK(cudaMemsetAsync(ctx->sim_time, 0, sizeof(double) * ctx->n_inst, ctx->stream));
     ctx->searched = false;
     ctx->sorted_once = false;
     ctx->nlist_valid = false;
@@ -1241,6 +1370,7 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
         ctx->nlist_valid = false;
         ctx->searched = false;   // positions moved: the next pass needs a search!
         ctx->rpn_valid = false;
+        ctx->cfl_valid = false;
     }
     if (action == EPP_ACTION_DAMBREAK_DENSITY || action == EPP_ACTION_KERNEL_FILTER_SELF ||
         action == EPP_ACTION_EXTRAPOLATE_PRESSURE_SELF)
@@ -1290,14 +1420,14 @@ int launch_integrals(epp_ctx* ctx, const epp_physics* phys) {
     return EPP_OK;
 }
 
-void fill_integrals(epp_integrals* out, const double* r, int n_alive, float c0) {
+void fill_integrals(epp_integrals* out, const double* r, int n_alive, float c0, float cfl) {
     out->mass_total = r[0];
     out->mass_fluid = r[1];
     out->kinetic = r[2];
     out->potential = r[3];
     out->internal = r[4];
     out->max_speed = r[5];
-    out->cfl_dt = r[6] < 1e300 ? 0.1 * r[6] / ((double)c0 + r[5]) : 0.0;
+    out->cfl_dt = r[6] < 1e300 ? (cfl > 0.0f ? (double)cfl : 0.1) * r[6] / ((double)c0 + r[5]) : 0.0;
     out->n_alive = n_alive;
     out->n_pairs = (int64_t)r[7];   // directed pairs of the last search = sum of nCount over alive particles
 }
@@ -1317,7 +1447,7 @@ int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* 
     CK(cudaMemcpyAsync(&n_alive, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    fill_integrals(out, r, n_alive, phys->c0);
+    fill_integrals(out, r, n_alive, phys->c0, phys->cfl);
     return EPP_OK;
 }
 
@@ -1346,6 +1476,7 @@ int32_t epp_integrals_async(epp_ctx* ctx, const epp_physics* phys, int64_t* tick
     CK(cudaEventRecord(ctx->iev[slot], ctx->stream));
     ctx->islot_ticket[slot] = t;
     ctx->islot_c0[slot] = phys->c0;
+    ctx->islot_cfl[slot] = phys->cfl;
     ctx->iticket_next = t + 1;
     *ticket = t;
     return EPP_OK;
@@ -1362,7 +1493,7 @@ int32_t epp_integrals_wait(epp_ctx* ctx, int64_t ticket, epp_integrals* out) {
     int n_alive = 0;
     std::memcpy(&n_alive, h + 8, sizeof n_alive);
     std::memset(out, 0, sizeof *out);
-    fill_integrals(out, h, n_alive, ctx->islot_c0[slot]);
+    fill_integrals(out, h, n_alive, ctx->islot_c0[slot], ctx->islot_cfl[slot]);
     ctx->islot_ticket[slot] = -1;
     return EPP_OK;
 }
@@ -1389,6 +1520,46 @@ int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t*
     return EPP_OK;
 }
 
+int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t ld, int32_t max_nb) {
+    if (!ctx || !counts) return EPP_ERR_INVALID_ARGUMENT;
+    if (ids && (max_nb < 0 || ld < ctx->n)) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "ld < n or max_nb < 0");
+    if (ctx->lanes != 0 || !ctx->nlist_valid)
+        return fail(ctx, EPP_ERR_STATE, "no neighbour lists of the search pass (family 0, after a search or step)");
+    cudaSetDevice(ctx->dev);
+    const int n = ctx->n;
+    if (n == 0) return EPP_OK;
+    const int lcap = ctx->D == 2 ? ListConf<2>::LCAP : ListConf<3>::LCAP;
+    const bool row_major = ctx->D == 2 ? ListConf<2>::ROW : ListConf<3>::ROW;
+    int n_alive = 0;
+    CK(cudaMemcpyAsync(&n_alive, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    n_alive = n_alive < 0 ? 0 : n_alive > n ? n : n_alive;
+    std::vector<int> id(n_alive > 0 ? n_alive : 1), cnt(n_alive > 0 ? n_alive : 1);
+    std::vector<int> list((size_t)lcap * ctx->cap);
+    if (n_alive > 0) {
+        CK(cudaMemcpyAsync(id.data(), ctx->S[ctx->cur].id, sizeof(int) * n_alive, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(cnt.data(), ctx->ncount, sizeof(int) * n_alive, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(list.data(), ctx->nlist, sizeof(int) * list.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    for (int r = 0; r < n; ++r) counts[r] = 0;   // particles not alive have no list
+    for (int i = 0; i < n_alive; ++i) {
+        const int row = id[i];
+        if (row < 0 || row >= n) return fail(ctx, EPP_ERR_DEVICE_STATUS, "sorted particle %d has id %d", i, row);
+        counts[row] = cnt[i];
+        if (!ids) continue;
+        const int kept = std::min(std::min(cnt[i], lcap), (int)max_nb);
+        for (int k = 0; k < kept; ++k) {
+            const int e = row_major ? list[(size_t)i * lcap + k] : list[(size_t)k * ctx->cap + i];
+            const int j = e & ((1 << kEntryBits) - 1);
+            if (j >= n_alive) return fail(ctx, EPP_ERR_DEVICE_STATUS, "list entry %d of particle %d: index %d", k, i, j);
+            ids[(size_t)k * ld + row] = id[j] + 1;
+        }
+    }
+    return EPP_OK;
+}
+
 int32_t epp_synchronize(epp_ctx* ctx, uint32_t* device_status) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
@@ -1399,6 +1570,36 @@ int32_t epp_synchronize(epp_ctx* ctx, uint32_t* device_status) {
     if (device_status) *device_status = st;
     if (st & ~(unsigned)EPP_STATUS_KILLED)
         return fail(ctx, EPP_ERR_DEVICE_STATUS, "device status 0x%x", st);
+    return EPP_OK;
+}
+
+int32_t epp_step_dt(epp_ctx* ctx, const epp_physics* phys, int32_t n, float* next_dt, double* sim_time) {
+    if (!ctx || !phys) return EPP_ERR_INVALID_ARGUMENT;
+    if (n != ctx->n_inst) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "n = %d, context has %d instances", n, ctx->n_inst);
+    if (const int prc = check_physics(ctx, phys)) return prc;
+    cudaSetDevice(ctx->dev);
+    if (next_dt) {
+        if (phys->cfl > 0.0f && ctx->n > 0) {
+            if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "the CFL time step needs a search! first");
+            ensure_cfl_tables(ctx, *phys);
+            if (!ctx->cfl_valid) {
+                const int rc = ctx->D == 2 ? cfl_update<2>(ctx, *phys) : cfl_update<3>(ctx, *phys);
+                if (rc) return rc;
+            }
+            std::vector<InstPhys> t(n);
+            CK(cudaMemcpyAsync(t.data(), ctx->tbl[ctx->cur], sizeof(InstPhys) * n, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            for (int k = 0; k < n; ++k) next_dt[k] = t[k].dt;
+        } else {
+            for (int k = 0; k < n; ++k) next_dt[k] = ctx->inst_dt.empty() ? phys->dt : ctx->inst_dt[k];
+        }
+    }
+    if (sim_time) {
+        std::vector<double> t(n);
+        CK(cudaMemcpyAsync(t.data(), ctx->sim_time, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int k = 0; k < n; ++k) sim_time[k] = t[k] + ctx->time_fixed[k];
+    }
     return EPP_OK;
 }
 
@@ -1427,6 +1628,7 @@ int32_t epp_set_instance_physics(epp_ctx* ctx, int32_t n, const float* dt, const
     ctx->inst_dt.assign(dt, dt + n);
     ctx->inst_c0.assign(c0, c0 + n);
     ctx->inst_dirty = true;
+    ctx->cfl_tables_ok = false;
     ctx->rpn_valid = false;   // the density preview used the previous time steps
     return EPP_OK;
 }
@@ -1458,7 +1660,7 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
         out[k].potential = v[3];
         out[k].internal = v[4];
         out[k].max_speed = v[5];
-        out[k].cfl_dt = v[6] < 1e300 ? 0.1 * v[6] / (c0 + v[5]) : 0.0;
+        out[k].cfl_dt = v[6] < 1e300 ? (phys->cfl > 0.0f ? (double)phys->cfl : 0.1) * v[6] / (c0 + v[5]) : 0.0;
         out[k].n_alive = (int64_t)v[7];
         out[k].n_pairs = (int64_t)v[8];
     }
@@ -1503,11 +1705,13 @@ int32_t epp_context_bytes(const epp_config* cfg, int64_t* bytes) {
     if ((D != 2 && D != 3) || cfg->n_capacity < 1 || !(cfg->domain.gap > 0.0f)) return EPP_ERR_INVALID_ARGUMENT;
     if (cfg->n_capacity > (1 << kEntryBits)) return EPP_ERR_CAPACITY;
     DevDomain d;
-    long long ncell = 1;
-    if (!plan_cells(cfg, d, ncell)) return EPP_ERR_INVALID_ARGUMENT;
+    if (const int prc = plan_cells(cfg, d)) return prc;
     const int n_tiles = (d.n_cells + 1 + kScanTile - 1) / kScanTile;
+    // + per instance: instance table, integrals, two CFL tables, CFL partials (at most 4 x 148 chunks
+    // per instance), simulated time
     const size_t b = arena_bytes(cfg->n_capacity, d.n_cells, D, n_tiles) + nlist_bytes(D, cfg->n_capacity) +
-                     (sizeof(InstPhys) + sizeof(double) * 9) * (size_t)d.n_inst + 3 * 256;
+                     (3 * sizeof(InstPhys) + sizeof(double) * 10) * (size_t)d.n_inst +
+                     sizeof(double2) * (size_t)std::max(d.n_inst, 4 * 148) + 8 * 256;
     *bytes = (int64_t)b;
     return EPP_OK;
 }
@@ -1558,6 +1762,11 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
         int rc = epp_step(ctx, 1, phys);   // settles dVelocity through the per-call path
         if (rc) return rc;
     }
+    if (phys->cfl > 0.0f && !ctx->cfl_valid) {
+        const int rc = ctx->D == 2 ? cfl_update<2>(ctx, *phys) : cfl_update<3>(ctx, *phys);
+        if (rc) return rc;
+        ctx->rpn_valid = false;
+    }
     if (!ctx->rpn_valid || !same_phys(ctx->rpn_phys, *phys)) {
         k_density_preview<<<blocks_for(ctx->n), kThreads, 0, ctx->stream>>>(
             ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], dev_phys(ctx, *phys));
@@ -1574,6 +1783,8 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
                          : enqueue_fused_step<3>(ctx, ctx->cur, *phys, ev);
     if (!rc) {
         ctx->cur = 1 - ctx->cur;
+        ctx->cfl_valid = phys->cfl > 0.0f;
+        if (phys->cfl <= 0.0f) advance_fixed_time(ctx, *phys, 1);
         ctx->rpn_valid = true;
         ctx->rpn_phys = *phys;
         ctx->lists_valid = false;

@@ -285,6 +285,90 @@ __global__ void __launch_bounds__(256) k_integrals_inst(const int* start, DevDom
     }
 }
 
+// CFL time step of every instance (new; the reference's dt is fixed, main.jl:68):
+//   dt_k = (float)(cfl h_min / (c0_k + sqrt(max |v|^2)))
+// with |v|^2 in FP64 from the FP32 components, max and h_min over the alive fluid particles of
+// instance k.  Instance k's particles are the contiguous range [start[k cells], start[(k+1) cells])
+// of the sorted order; block b reduces chunk b % chunks of instance b / chunks into partial[b],
+// and the last block to finish combines the chunks of every instance (max and min do not depend
+// on the order: the result is deterministic), writes next[k].dt, adds used[k].dt (the dt of the
+// step just taken) to time[k] when `used` is set, and re-arms the ticket.  FUSED reads the
+// momentum pass's output (velocities and positions of the new state, in the order of `start`;
+// particles its bin killed are skipped); otherwise the sorted state itself.
+struct CflArgs {
+    const int* start;       // cell offsets of the order the arrays are in
+    int cells_per_inst, n_inst, n_cells, n_max, chunks;
+    const float4* vm;       // (vx, vy, vz, m)
+    const float4* xh;       // (x, y, z, h)
+    const int* tagm;
+    const int2* cs;         // FUSED: (cell, slot) of the bin; cell n_cells = killed
+    int fluid;
+    float cfl;
+    const InstPhys* used;   // dt of the step just taken (added to time), or null
+    InstPhys* next;         // dt written here; c0 read here
+    double2* partial;       // [n_inst * chunks]: (max |v|^2, min h)
+    double* time;           // [n_inst]
+    unsigned* ticket;
+};
+
+template <int D, bool FUSED>
+__global__ void __launch_bounds__(256) k_cfl(const __grid_constant__ CflArgs A) {
+    __shared__ double sh_v[256 / 32], sh_h[256 / 32];
+    __shared__ bool last;
+    const int k = blockIdx.x / A.chunks, chunk = blockIdx.x % A.chunks;
+    const int lo = max(A.start[k * A.cells_per_inst], 0);
+    const int hi = min(A.start[(k + 1) * A.cells_per_inst], A.n_max);
+    double v2 = 0.0, hm = 1e300;
+    for (int i = lo + chunk * blockDim.x + threadIdx.x; i < hi; i += A.chunks * blockDim.x) {
+        if (tag_of(A.tagm[i]) != A.fluid) continue;
+        if (FUSED && A.cs[i].x >= A.n_cells) continue;   // left the domain in this step
+        const float4 v = A.vm[i];
+        const double u2 = (double)v.x * v.x + (double)v.y * v.y + (D == 3 ? (double)v.z * v.z : 0.0);
+        v2 = fmax(v2, u2);
+        hm = fmin(hm, (double)A.xh[i].w);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v2 = fmax(v2, __shfl_down_sync(0xffffffffu, v2, o));
+        hm = fmin(hm, __shfl_down_sync(0xffffffffu, hm, o));
+    }
+    if (lane == 0) {
+        sh_v[warp] = v2;
+        sh_h[warp] = hm;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 256 / 32; ++w) {
+            v2 = fmax(v2, sh_v[w]);
+            hm = fmin(hm, sh_h[w]);
+        }
+        A.partial[blockIdx.x] = make_double2(v2, hm);
+        __threadfence();
+        last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int q = threadIdx.x; q < A.n_inst; q += blockDim.x) {
+        double vq = 0.0, hq = 1e300;
+        for (int c = 0; c < A.chunks; ++c) {
+            const double2 p = __ldcg(&A.partial[q * A.chunks + c]);
+            vq = fmax(vq, p.x);
+            hq = fmin(hq, p.y);
+        }
+        if (A.used) A.time[q] += (double)A.used[q].dt;
+        if (hq < 1e300) A.next[q].dt = (float)((double)A.cfl * hq / ((double)A.next[q].c0 + sqrt(vq)));
+    }
+    if (threadIdx.x == 0) *A.ticket = 0;
+}
+
+// time[k] += table[k].dt: the simulated time of a step taken through the per-call kernels.
+__global__ void k_advance_time(int n_inst, const InstPhys* table, double* time) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n_inst) time[k] += (double)table[k].dt;
+}
+
 // Staging columns (by particle row), used by upload and download:
 //   float: position[D], velocity[D], dvelocity[D], mass, volume, density, ddensity, pressure, h
 //   int:   tag, movable, ncount, alive, cell

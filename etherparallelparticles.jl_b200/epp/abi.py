@@ -5,7 +5,7 @@ the header cites the reference interface each entry point replaces.
 """
 import ctypes as C
 
-EPP_ABI_VERSION = 3
+EPP_ABI_VERSION = 4
 EPP_MAX_TAGS = 16
 
 # epp_status
@@ -120,6 +120,7 @@ class epp_physics(C.Structure):
         ("pressure_fw", C.c_int32),
         ("tensile", C.c_int32),
         ("wall_pressure", C.c_int32),
+        ("cfl", C.c_float),
     ]
 
 
@@ -201,7 +202,7 @@ def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81
                  alpha=0.1, beta=0.1, viscosity=EPP_VISCOSITY_REFERENCE, fluid_tag=1,
                  wall_tag=2, kahan=1, kernel=EPP_KERNEL_WENDLAND_C2, eos=EPP_EOS_TAIT, mu=0.0,
                  motion=EPP_MOTION_SYMPLECTIC, filter_interval=0, pressure_ff=EPP_PRESSURE_DEFAULT,
-                 pressure_fw=EPP_PRESSURE_DEFAULT, tensile=0, wall_pressure=EPP_WALL_PRESSURE_EOS):
+                 pressure_fw=EPP_PRESSURE_DEFAULT, tensile=0, wall_pressure=EPP_WALL_PRESSURE_EOS, cfl=0.0):
     p = epp_physics()
     p.dt = dt
     p.rho0 = rho0
@@ -225,6 +226,7 @@ def make_physics(dt, rho0=1000.0, c0=62.64, p0=0.0, gamma=7, gravity=(0.0, -9.81
     p.pressure_fw = pressure_fw
     p.tensile = tensile
     p.wall_pressure = wall_pressure
+    p.cfl = cfl
     return p
 
 

@@ -21,7 +21,8 @@ EXPORTS = [
     "epp_set_instance_physics", "epp_get_instance_integrals", "epp_context_bytes", "epp_query",
     "epp_set_priority", "epp_set_block_threads", "epp_integrals_async", "epp_integrals_wait",
     "epp_server_create", "epp_server_destroy", "epp_server_submit", "epp_server_poll", "epp_server_drain",
-    "epp_server_result", "epp_server_download", "epp_server_set_co_batch",
+    "epp_server_result", "epp_server_download", "epp_server_set_co_batch", "epp_neighbour_lists",
+    "epp_step_dt",
 ]
 
 
@@ -85,6 +86,8 @@ def load(path=LIB_PATH):
     lib.epp_server_download.argtypes = [srv, C.c_int64, i32p, i32p, i32p, C.c_int64, f32p, C.c_int64]
     lib.epp_integrals_wait.argtypes = [ctx, C.c_int64, P(abi.epp_integrals)]
     lib.epp_cell_stats.argtypes = [ctx, i32p, i32p, i32p, i32p]
+    lib.epp_neighbour_lists.argtypes = [ctx, i32p, i32p, C.c_int64, C.c_int32]
+    lib.epp_step_dt.argtypes = [ctx, P(abi.epp_physics), C.c_int32, f32p, P(C.c_double)]
     lib.epp_synchronize.argtypes = [ctx, P(C.c_uint32)]
     lib.epp_last_step_timing.argtypes = [ctx, f32p]
     lib.epp_pairs_total.argtypes = [ctx, P(C.c_int64)]
@@ -200,6 +203,26 @@ class Context:
         self._ck(self.lib.epp_cell_stats(self.h, None, None, _ptr(ids, C.c_int32), C.byref(nc)),
                  "epp_cell_stats")
         return counts, offsets, ids[: int(offsets[-1])]
+
+    def step_dt(self, phys, n=1):
+        """(next_dt[n], sim_time[n]): the dt of the next step per instance and the simulated time
+        advanced by epp_step since the last upload (epp_step_dt)."""
+        import numpy as np
+        dt = np.zeros(n, np.float32)
+        t = np.zeros(n, np.float64)
+        self._ck(self.lib.epp_step_dt(self.h, C.byref(phys), n, _ptr(dt, C.c_float), _ptr(t, C.c_double)),
+                 "epp_step_dt")
+        return dt, t
+
+    def neighbour_lists(self, n, max_nb):
+        """(counts[n], ids[n, max_nb]): nCount per caller row and the 1-based neighbour ids of the
+        search pass's lists (epp_neighbour_lists), in list order; unused slots are 0."""
+        import numpy as np
+        counts = np.zeros(n, np.int32)
+        ids = np.zeros((max_nb, max(n, 1)), np.int32)   # ids[k, row]: column-major with ld = n
+        self._ck(self.lib.epp_neighbour_lists(self.h, _ptr(counts, C.c_int32), _ptr(ids, C.c_int32), max(n, 1),
+                                              max_nb), "epp_neighbour_lists")
+        return counts, ids[:, :n].T.copy()
 
     def synchronize(self, raise_on_status=True):
         st = C.c_uint32(0)

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define EPP_ABI_VERSION 3
+#define EPP_ABI_VERSION 4
 #define EPP_MAX_TAGS 16
 
 typedef enum epp_status {
@@ -148,6 +148,14 @@ typedef struct epp_physics {
     int32_t tensile;          /* 1: iPressureCorrection (Pressure.jl:10-22) on both: the pressure term
                                * grows by |term| 0.01 W(r) / W((gap_i + gap_j) / 2); needs the gap column */
     int32_t wall_pressure;    /* EPP_WALL_PRESSURE_* */
+    float cfl;                /* 0: every step takes dt (the reference's fixed step, main.jl:68).
+                               * > 0: each epp_step step takes dt = cfl h_min / (c0 + max|v|) of the
+                               * state it starts from: max|v| and h_min (smallest H) over the alive
+                               * fluid particles, per instance in a batch with the instance's c0,
+                               * reduced in FP64 on the device inside the step (no host round trip)
+                               * and rounded once to FP32.  At rest, cfl = 0.1 gives the reference's
+                               * dt = 0.1 h / c0.  The per-call selfaction!(DAMBREAK_DENSITY) takes
+                               * the same dt of the current state; INTEGRATE reuses it. */
 } epp_physics;
 
 typedef struct epp_config {
@@ -182,7 +190,8 @@ typedef struct epp_integrals {
     double potential;       /* sum -m g.x (fluid) */
     double internal;        /* sum m e(rho), Tait internal energy (fluid) */
     double max_speed;       /* max |v| (fluid) */
-    double cfl_dt;          /* 0.1 h_min / (c0 + max|v|) -- the CFL bound of the step */
+    double cfl_dt;          /* cfl h_min / (c0 + max|v|) (cfl of the physics, 0.1 when it is 0): the
+                             * CFL time step of this state, in FP64 (epp_step rounds it to FP32) */
     int64_t n_alive;
     int64_t n_pairs;        /* directed active neighbour pairs of the last search */
 } epp_integrals;
@@ -242,9 +251,26 @@ int32_t epp_integrals_wait(epp_ctx* ctx, int64_t ticket, epp_integrals* out);
 int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t* sorted_ids,
                        int32_t* n_cells);
 
+/* Parity access to the neighbour lists of the default pair passes (family 0), as the search pass
+ * built them at the last epp_search or epp_step (the lists every pair pass of a step reads):
+ * counts[row] = nCount of the particle in caller row `row` (0 for particles not alive), and
+ * ids[k * ld + row] for k < min(counts[row], max_nb, list capacity) = the 1-based id of its k-th
+ * neighbour in list order (stencil rows, then cell order, then id order inside a cell).  A list
+ * keeps at most 64 (2D) / 160 (3D) entries; a particle with more neighbours has only those stored
+ * (its pair passes read its stencil instead).  ids may be NULL.  Replaces reading the nCount /
+ * nIndex columns of the reference's particle system after search! (NeighbourSearch.jl:166-227). */
+int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t ld, int32_t max_nb);
+
 /* Waits for the context stream; returns EPP_ERR_DEVICE_STATUS when a device check failed
  * (bits in *device_status, which is then cleared). device_status may be NULL. */
 int32_t epp_synchronize(epp_ctx* ctx, uint32_t* device_status);
+
+/* Time stepping: next_dt[k] = the dt the next step of instance k takes under `phys` (phys->dt, the
+ * instance's dt, or with phys->cfl > 0 the CFL dt of the current state, computed on the device);
+ * sim_time[k] = simulated time advanced by epp_step since the last epp_upload (the sum of the dt
+ * of every step taken).  n = the context's instances (1 without a batch); either array may be
+ * NULL.  No reference counterpart: main.jl:165-206 keeps t on the host with its fixed dt. */
+int32_t epp_step_dt(epp_ctx* ctx, const epp_physics* phys, int32_t n, float* next_dt, double* sim_time);
 
 /* Device time of the last epp_step call (ms, CUDA events on the context stream). */
 int32_t epp_last_step_timing(epp_ctx* ctx, float* ms_total);
@@ -350,9 +376,9 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
 
 /* Cell-list build that allocates nothing, for callers that must not call cudaMalloc while they
  * drive the library (a host application that owns a fixed device pool, or one that is in the
- * middle of a step where a device allocation would synchronise or is not allowed).  No
- * counterpart in the reference: it is the bin + count + scan + counting sort of search!
- * (NeighbourSearch.jl:12-47) as one call on caller-owned device buffers.
+ * middle of a step where a device allocation would synchronise or is not allowed).  It has no
+ * counterpart in the reference.  It runs the bin + count + scan + counting sort of epp_search's
+ * cell-list build as one call on caller-owned device buffers.
  *   pos         device, column-major positions: x at pos[i], y at pos[n + i], z at pos[2n + i]
  *   counts      device [n_cells] or NULL;  offsets  device [n_cells + 1] or NULL
  *   sorted_ids  device [n]: 1-based particle ids in cell order, by id inside a cell (the first
@@ -364,8 +390,11 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
  * loads the library until the process exits).  Larger inputs return EPP_ERR_CAPACITY.  Every call
  * shares that array, so calls that overlap on the GPU (other streams, other host threads) race;
  * serialise them.  The first call on a device looks up the array's device address for that
- * device (cudaGetSymbolAddress), so make it before any stream capture.  It calls no cudaMalloc,
- * cudaFree or other allocating routine. */
+ * device (cudaGetSymbolAddress), so make it before any stream capture; that look-up is guarded,
+ * so first calls from several host threads are safe.  It calls no cudaMalloc, cudaFree or other
+ * allocating routine.  A domain of more than 2^20 cells (checked axis by axis, before anything
+ * runs on the GPU) returns EPP_ERR_CAPACITY; a device-side inconsistency returns
+ * EPP_ERR_DEVICE_STATUS. */
 int32_t epp_cell_sort_noalloc(const epp_domain* domain, int32_t n, const float* pos, int32_t* counts,
                               int32_t* offsets, int32_t* sorted_ids, int32_t* n_alive, void* stream);
 int32_t epp_noalloc_limits(int32_t* max_particles, int32_t* max_cells, int64_t* scratch_bytes);

@@ -221,6 +221,7 @@ inline T kern_value0(int kind, T hinv, int dim) { return kern_sigma<T>(kind, dim
 template <typename T>
 struct Phys {
     T dt, rho0, c0, p0, B, g[3], alpha, beta, coef, mu, c02;
+    double cfl;   // 0: fixed dt; > 0: the CFL time step of each step's starting state
     int gamma, visc, fluid, wall, kahan, kernel, eos, motion, filter_interval;
     int pff, pfw, tensile, wallp;   // resolved EPP_PRESSURE_* per pair type, tensile flag, EPP_WALL_PRESSURE_*
 };
@@ -228,6 +229,7 @@ template <typename T>
 Phys<T> make_phys(const epp_physics& p) {
     Phys<T> o;
     o.dt = T(p.dt);
+    o.cfl = (double)p.cfl;
     o.rho0 = T(p.rho0);
     o.c0 = T(p.c0);
     o.p0 = T(p.p0);
@@ -290,6 +292,7 @@ struct System : SysBase {
     std::vector<T> wv, wv_rho;   // kernel-filter sums (Filter.jl: SumWeight, SumWeightedDensity)
     std::vector<T> wv_p;         // SumWeightedPressure of the wall-pressure extrapolation (Pressure.jl:85-131)
     long long step_count = 0;    // steps since upload (main.jl:165 step += 1)
+    double sim_time = 0.0;       // sum of the dt of the steps since upload
     std::vector<T> nw, ndw, nhinv, nr, nrvec;
     /* neighbour system */
     std::vector<int32_t> ccount, clist, nccount, nclist;
@@ -674,10 +677,32 @@ struct System : SysBase {
         return EPP_OK;
     }
 
-    /* main.jl:166-182 */
-    int step(int nsteps, const Phys<T>& P) {
+    /* CFL time step of the current state (new; the reference's dt is fixed, main.jl:68):
+     * cfl h_min / (c0 + max|v|) over the alive fluid particles, |v|^2 summed in FP64 from the
+     * stored components, h_min the smallest H, rounded once to FT.  Without fluid: P.dt. */
+    T cfl_dt(const Phys<T>& P) const {
+        double v2max = 0.0, hmin = 1e300;
+        for (int I = 0; I < n; ++I) {
+            if (alive[I] != 1 || tag[I] != P.fluid) continue;
+            double v2 = 0.0;
+            for (int a = 0; a < D; ++a) {
+                const double u = (double)vel[(size_t)a * n_cap + I];
+                v2 += u * u;
+            }
+            v2max = std::max(v2max, v2);
+            hmin = std::min(hmin, (double)h[I]);
+        }
+        if (!(hmin < 1e300)) return P.dt;
+        return T(P.cfl * hmin / ((double)P.c0 + std::sqrt(v2max)));
+    }
+
+    /* main.jl:166-182; with P.cfl > 0 each step takes the CFL dt of the state it starts from */
+    int step(int nsteps, const Phys<T>& P0) {
         if (!searched) return EPP_ERR_STATE;
         for (int s = 0; s < nsteps; ++s) {
+            Phys<T> P = P0;
+            if (P0.cfl > 0.0) P.dt = cfl_dt(P0);
+            sim_time += (double)P.dt;
             ++step_count;
             selfaction(EPP_ACTION_DAMBREAK_DENSITY, P);
             if (P.wallp == EPP_WALL_PRESSURE_EXTRAPOLATE) {   // wall pressure from the fluid around it
@@ -747,6 +772,7 @@ int upload(System<T>* s, int32_t n, const int32_t* alive, const int32_t* cell, c
     for (int I = n; I < s->n_cap; ++I) s->alive[I] = 0;
     s->searched = false;
     s->step_count = 0;
+    s->sim_time = 0.0;
     std::fill(s->wv.begin(), s->wv.end(), T(0));       // filter sums start at zero (not uploaded)
     std::fill(s->wv_rho.begin(), s->wv_rho.end(), T(0));
     std::fill(s->wv_p.begin(), s->wv_p.end(), T(0));
@@ -825,7 +851,7 @@ int integrals(System<T>* s, const epp_physics* ph, epp_integrals* out) {
     }
     out->mass_total = mt; out->mass_fluid = mf; out->kinetic = ke; out->potential = pe;
     out->internal = ie; out->max_speed = vmax;
-    out->cfl_dt = hmin < 1e300 ? 0.1 * hmin / (c0 + vmax) : 0.0;
+    out->cfl_dt = hmin < 1e300 ? (ph->cfl > 0.0f ? (double)ph->cfl : 0.1) * hmin / (c0 + vmax) : 0.0;
     out->n_alive = na; out->n_pairs = np;
     return EPP_OK;
 }
@@ -1060,6 +1086,20 @@ int32_t orc_cell_stats(orc_sys* s0, int32_t* counts, int32_t* offsets, int32_t* 
     SysBase* s = reinterpret_cast<SysBase*>(s0);
     const epp_physics* phys = nullptr;
     DISPATCH(s, cell_stats(S, counts, offsets, ids, n_cells));
+}
+
+int32_t orc_step_dt(orc_sys* s0, const epp_physics* phys, double* next_dt, double* sim_time) {
+    SysBase* s = reinterpret_cast<SysBase*>(s0);
+    if (!phys) return EPP_ERR_INVALID_ARGUMENT;
+    auto go = [&](auto* S) -> int32_t {
+        using T = typename std::remove_reference<decltype(S->rho[0])>::type;
+        const Phys<T> P = make_phys<T>(*phys);
+        if (next_dt) *next_dt = (double)(P.cfl > 0.0 ? S->cfl_dt(P) : P.dt);
+        if (sim_time) *sim_time = S->sim_time;
+        return EPP_OK;
+    };
+    if (s->precision == 64) return go(static_cast<System<double>*>(s));
+    return go(static_cast<System<float>*>(s));
 }
 
 uint32_t orc_status(orc_sys* s0) {

@@ -78,6 +78,9 @@ int32_t orc_integrals(orc_sys* s, const epp_physics* phys, epp_integrals* out);
 int32_t orc_cell_stats(orc_sys* s, int32_t* counts, int32_t* offsets, int32_t* sorted_ids,
                        int32_t* n_cells);
 /* returns and clears the accumulated EPP_STATUS_* bits */
+/* dt of the next step under phys (the CFL dt of the current state when phys->cfl > 0) and the
+ * simulated time of the steps since upload. */
+int32_t orc_step_dt(orc_sys* s, const epp_physics* phys, double* next_dt, double* sim_time);
 uint32_t orc_status(orc_sys* s);
 
 #ifdef __cplusplus

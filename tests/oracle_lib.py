@@ -62,6 +62,7 @@ def load():
     lib.orc_step.argtypes = [C.c_void_p, C.c_int32, P(abi.epp_physics)]
     lib.orc_integrals.argtypes = [C.c_void_p, P(abi.epp_physics), P(abi.epp_integrals)]
     lib.orc_cell_stats.argtypes = [C.c_void_p, i32p, i32p, i32p, i32p]
+    lib.orc_step_dt.argtypes = [C.c_void_p, P(abi.epp_physics), f64p, f64p]
     lib.orc_status.restype = C.c_uint32
     lib.orc_status.argtypes = [C.c_void_p]
     _lib = lib
@@ -143,6 +144,12 @@ class Oracle:
         self._ck(self.lib.orc_cell_stats(self.h, _p(counts, C.c_int32), _p(offsets, C.c_int32),
                                          _p(ids, C.c_int32), C.byref(nc)), "orc_cell_stats")
         return counts, offsets, ids[:n_alive]
+
+    def step_dt(self, phys):
+        """(dt of the next step, simulated time since upload)."""
+        dt, t = C.c_double(0), C.c_double(0)
+        self._ck(self.lib.orc_step_dt(self.h, C.byref(phys), C.byref(dt), C.byref(t)), "orc_step_dt")
+        return dt.value, t.value
 
     def status(self):
         return self.lib.orc_status(self.h)
