@@ -456,7 +456,7 @@ def run_batch(args):
             "pairs_per_s": pairs / (ms * 1e-3) if world == 1 else None,
             "energy_drift": {"steps": S, "bar": 1e-4, "instances": drift,
                              "max_abs_diff": max(v["abs_diff"] for v in drift.values())},
-            "gpu_launches": 6 * args.steps,
+            "gpu_launches": 5 * args.steps,
             "roofline": {"bound": "hbm", "stage_ms": dict(zip(STAGES, [round(float(x), 4) for x in stage])),
                          "achieved": B_ALG_STEP[2] * b.n / (step_ms * 1e-3) / 1e9,
                          "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
@@ -673,11 +673,20 @@ def main():
                 flush.fill_(1.0)
             stage += np.array(ctx.profile_step(phys))
         stage /= nprof
+    # 2D family 0 runs the continuity action inside the search pass (stencil-row masks): that
+    # kernel carries both stages' bytes and the continuity stage is empty
+    b_alg = {k: dict(v) for k, v in B_ALG_STAGE.items()}
+    kernel_of = dict(KERNEL_OF_STAGE)
+    if stage[STAGES.index("continuity")] == 0.0:
+        b_alg["search"][dim] += b_alg["continuity"][dim]
+        if dim == 2 and not args.lanes:
+            kernel_of["search"] = "k_mask_build<CPCont> (stencil-row masks + continuity + density preview)"
+            kernel_of["momentum_integrate_bin"] = "k_mask_walk<CPMom> (momentum + integrate + bin over the masks)"
     # roofline of the dominant kernel: the longest of the step's kernels
     dom_stage = max(STAGES, key=lambda k: stage[STAGES.index(k)])
     dom_ms = float(stage[STAGES.index(dom_stage)])
     n = case.n
-    achieved = B_ALG_STAGE[dom_stage][dim] * n / (dom_ms * 1e-3) / 1e9
+    achieved = b_alg[dom_stage][dim] * n / (dom_ms * 1e-3) / 1e9
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -689,7 +698,10 @@ def main():
     tr_case = {}
     try:   # DRAM bytes of one launch of that kernel from an ncu capture of the same workload
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            tr_case = json.load(f).get(args.case, {})
+            base = lambda name: name.split(" ")[0].split("<")[0]  # noqa: E731
+            # only captures of the kernels this run launches
+            tr_case = {k: v for k, v in json.load(f).get(args.case, {}).items()
+                       if k in kernel_of and base(v.get("kernel", "")) == base(kernel_of[k])}
             if tr_case.get(dom_stage):
                 traffic = tr_case[dom_stage]["bytes_per_launch"]
     except Exception:
@@ -732,22 +744,22 @@ def main():
             "step_hbm_gbs_algorithmic": step_bytes / (step_ms * 1e-3) / 1e9,
             "step_roofline_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak,
             # per fused step: momentum+integrate+bin, scan, scatter, rank+gather, search, continuity
-            # (families other than 0 fuse search and continuity into one kernel)
-            "gpu_launches": (6 if args.lanes == 0 else 5) * args.steps
+            # (2D family 0 and the other families run the continuity action inside the search pass)
+            "gpu_launches": (6 if (args.lanes == 0 and dim == 3) or args.lanes == 64 else 5) * args.steps
                             + (2 * (args.steps // phys.filter_interval) if phys.filter_interval else 0),
-            "roofline": {"bound": "hbm", "kernel": KERNEL_OF_STAGE[dom_stage], "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": kernel_of[dom_stage], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
                          else "fallback 6650 GB/s (of fallback)",
-                         "algorithmic_bytes_per_particle": B_ALG_STAGE[dom_stage][dim],
+                         "algorithmic_bytes_per_particle": b_alg[dom_stage][dim],
                          "kernel_ms": round(dom_ms, 5),
                          "stage_ms": dict(zip(STAGES, [round(x, 5) for x in stage])),
-                         "stage_frac": {k: round(B_ALG_STAGE[k][dim] * n / (stage[STAGES.index(k)] * 1e-3) / 1e9
+                         "stage_frac": {k: round(b_alg[k][dim] * n / (stage[STAGES.index(k)] * 1e-3) / 1e9
                                                  / peak, 4) for k in STAGES if stage[STAGES.index(k)] > 0},
                          "frac_of_nominal_8tbs": achieved / 8000.0,
                          "limiter": "instruction issue and neighbour-gather latency, not DRAM bandwidth (ncu: "
                                     "DRAM 4-18% busy in the pair kernels; profiles/)",
-                         "compute": compute_roof(tr_case, stage, fp32_peak, clk)},
+                         "compute": compute_roof(tr_case, stage, fp32_peak, clk, kernel_of)},
             "clocks": clk,
             "e2e": e2e,
             "device_status": st,
@@ -938,7 +950,7 @@ def measure_batch(device, steps=50, warmup=3, instances=256, sim_steps=2000):
             "autotune": {"family": tuned[0], "block_threads": tuned[1], "resort_every": 1},
             "energy_drift": {"steps": S, "bar": 1e-4, "instances": drift,
                              "max_abs_diff": max(v["abs_diff"] for v in drift.values())},
-            "gpu_launches": 6 * steps, "clocks": clk, "device_status": st,
+            "gpu_launches": 5 * steps, "clocks": clk, "device_status": st,
             "leg_seconds": time.perf_counter() - t_leg}
 
 
@@ -1034,7 +1046,7 @@ def fp32_peak_tflops(stream):
         torch.set_float32_matmul_precision(prev)
 
 
-def compute_roof(tr_case, stage, fp32_peak, clk):
+def compute_roof(tr_case, stage, fp32_peak, clk, kernel_of=None):
     """Second roof of the three pair kernels: FP32 flops and warp instructions per launch (ncu
     instruction-mix capture of the same workload) over this run's kernel times, against the
     measured SGEMM FP32 rate and the issue rate 148 SMs x 4 schedulers x the sampled SM clock."""
@@ -1048,7 +1060,7 @@ def compute_roof(tr_case, stage, fp32_peak, clk):
         if "flops_per_launch" not in e or ms <= 0:
             continue
         tf = e["flops_per_launch"] / (ms * 1e-3) / 1e12
-        out["stages"][st] = {"kernel": KERNEL_OF_STAGE[st], "kernel_ms": round(ms, 5),
+        out["stages"][st] = {"kernel": (kernel_of or KERNEL_OF_STAGE)[st], "kernel_ms": round(ms, 5),
                              "flops_per_launch": e["flops_per_launch"], "achieved_tflops": tf,
                              "fp32_frac": tf / fp32_peak,
                              "warp_inst_per_launch": e["warp_inst_per_launch"],

@@ -251,14 +251,15 @@ int32_t epp_integrals_wait(epp_ctx* ctx, int64_t ticket, epp_integrals* out);
 int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t* sorted_ids,
                        int32_t* n_cells);
 
-/* Parity access to the neighbour lists of the default pair passes (family 0), as the search pass
- * built them at the last epp_search or epp_step (the lists every pair pass of a step reads):
- * counts[row] = nCount of the particle in caller row `row` (0 for particles not alive), and
- * ids[k * ld + row] for k < min(counts[row], max_nb, list capacity) = the 1-based id of its k-th
- * neighbour in list order (stencil rows, then cell order, then id order inside a cell).  A list
- * keeps at most 64 (2D) / 160 (3D) entries; a particle with more neighbours has only those stored
- * (its pair passes read its stencil instead).  ids may be NULL.  Replaces reading the nCount /
- * nIndex columns of the reference's particle system after search! (NeighbourSearch.jl:166-227). */
+/* Parity access to the neighbours the default pair passes (family 0) read, as the search pass
+ * recorded them at the last epp_search or epp_step (2D stencil-row masks, 3D or EPP_TUNING_LISTS
+ * neighbour lists): counts[row] = nCount of the particle in caller row `row` (0 for particles not
+ * alive), and ids[k * ld + row] for k < min(counts[row], max_nb) = the 1-based id of its k-th
+ * neighbour in list order (stencil rows, then cell order, then id order inside a cell).  A
+ * particle whose neighbours are not stored -- more than 32 candidates in a 2D stencil row, more
+ * than 160 neighbours in a 3D list; its pair passes read its stencil instead -- has its ids left
+ * as they were.  ids may be NULL.  Replaces reading the nCount / nIndex columns of the reference's
+ * particle system after search! (NeighbourSearch.jl:166-227). */
 int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t ld, int32_t max_nb);
 
 /* Waits for the context stream; returns EPP_ERR_DEVICE_STATUS when a device check failed
@@ -294,7 +295,11 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
  * warp tile of 32 particles per warp, neighbours filtered once per step into a per-particle
  * neighbour list that the momentum pass reuses; 1 = one warp per occupied cell with a compacted
  * pair queue; 2, 4, 8, 16 or 32 = that many lanes of a warp per particle.  Chosen by the
- * autotuner; results change only at the FP32 rounding level (neighbour sets are identical). */
+ * autotuner; results change only at the FP32 rounding level (neighbour sets are identical).
+ * In 2D, family 0 keeps per-particle stencil-row masks (three 32-bit words: which candidates of
+ * each stencil row are neighbours) in place of lists, and its search pass runs the search action;
+ * EPP_TUNING_LISTS selects family 0 with neighbour lists instead (the same sums, bit for bit). */
+#define EPP_TUNING_LISTS 64
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
 /* Threads per block of the family-0 search and list passes: 128 (default), 64 or 32.  Smaller
  * blocks spread a small system over more SMs; results do not change (the per-particle order is

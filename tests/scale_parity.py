@@ -116,8 +116,8 @@ class ScaleParity:
         self.o32.download(ops.is_alive, ops.cell_index, ops.int_properties, ops.float_properties, self.dps.cmap)
         bi = ops.basic_index
         o_ids = ops.int_properties[:n, bi["nIndex"] - 1: bi["nIndex"] - 1 + self.max_nb]
-        lcap = 64 if dim == 2 else 160
-        full = (g_cnt <= min(lcap, self.max_nb)) & (o_cnt <= self.max_nb)
+        # rows whose neighbours the device stores (the others read their stencil in every pass)
+        full = ((g_ids[:, 0] != 0) | (g_cnt == 0)) & (g_cnt <= self.max_nb) & (o_cnt <= self.max_nb)
         out["ncount"] = bool(np.array_equal(g_cnt, o_cnt))
         out["sets"] = bool(out["ncount"] and np.array_equal(
             neighbour_pairs(np.where(full, g_cnt, 0), g_ids), neighbour_pairs(np.where(full, o_cnt, 0), o_ids)))
