@@ -777,7 +777,7 @@ def main():
                 out["cpu_baseline"] = {"value": None, "error": str(exc)}
             try:   # 2D: this workload; 3D: the dx = 0.01 block (the FP64 oracle at 6.2M particles is slow)
                 dcase = make_case(args.case, args.physics)[0] if dim == 2 else casegen.dam_break_3d(dx=0.01, max_neighbour_number=1)
-                out["energy_drift"] = energy_drift_fp64(dcase, 20 if dim == 2 else 10, device=local)
+                out["energy_drift"] = energy_drift_fp64(dcase, 100 if dim == 2 else 10, device=local)
             except Exception as exc:
                 out["energy_drift"] = {"error": str(exc)}
             if args.parity:
@@ -786,6 +786,10 @@ def main():
                 except Exception as exc:
                     out["parity"] = {"error": repr(exc)}
             if args.served and args.case == "2d" and args.physics == "benchmark":
+                try:
+                    out["3d"] = measure_3d(local)
+                except Exception as exc:
+                    out["3d"] = {"error": repr(exc)}
                 try:
                     out["batch"] = measure_batch(local, steps=50, warmup=3, instances=256)
                 except Exception as exc:
@@ -860,6 +864,70 @@ def plain_instance_ms(cases, device, stream, k=20):
         per_step.append(a_.elapsed_time(b_) / k)
     plain.close()
     return per_step
+
+
+def measure_3d(device, steps=20, warmup=3):
+    """3D leg of the 2D line: the 3D dam break at dx = 0.005 m (4.8M fluid particles, 3-layer
+    walls: 6.2M), the plain path, `steps` timed steps with the L2 flushed before each."""
+    import torch
+    from epp import abi, casegen
+    from epp.algorithm import DeviceParticleSystem
+    from epp.classes import NeighbourSystem
+    t_leg = time.perf_counter()
+    case = casegen.dam_break_3d(dx=0.005, max_neighbour_number=1)
+    phys = case.physics
+    ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
+    dps = DeviceParticleSystem(case.ps, ns, device=device)
+    ctx = dps.ctx
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    dps.syncto()
+    ctx.search(abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY, phys, 0)
+    with torch.cuda.stream(stream):
+        ctx.step(warmup, phys)
+    ctx.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    p0 = ctx.pairs_total()
+    clocks = Clocks(device)
+    torch.cuda.synchronize()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            ctx.step(1, phys)
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    st = ctx.synchronize(raise_on_status=False)
+    ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
+    pairs = ctx.pairs_total() - p0
+    with torch.cuda.stream(stream):
+        stage = np.mean([ctx.profile_step(phys) for _ in range(3)], axis=0)
+    dps.close()
+    del flush
+    torch.cuda.empty_cache()
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    step_ms = ms / steps
+    gbs = B_ALG_STEP[3] * case.n / (step_ms * 1e-3) / 1e9
+    return {"metric": "SPH pair-interactions/s", "value": pairs / (ms * 1e-3), "unit": "pair-interactions/s",
+            "steps": steps, "warmup": warmup, "ms_per_step": step_ms,
+            "config": {"workload": "3D dam break dx=0.005 (4.8M fluid)", "particles": case.n,
+                       "fluid": case.meta["n_fluid"], "walls": case.meta["n_wall"], "cells": case.meta["n_cells"],
+                       "resort": "every step", "l2": "flushed (256 MB write) before every timed step"},
+            "pairs_per_step": pairs / steps,
+            "step_hbm_gbs_algorithmic": gbs, "step_roofline_frac": gbs / peak,
+            "stage_ms": dict(zip(STAGES, [round(float(x), 5) for x in stage])),
+            "gpu_launches": 6 * steps, "clocks": clk, "device_status": st,
+            "leg_seconds": time.perf_counter() - t_leg}
 
 
 def measure_batch(device, steps=50, warmup=3, instances=256, sim_steps=2000):
