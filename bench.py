@@ -677,9 +677,11 @@ def main():
     # kernel carries both stages' bytes and the continuity stage is empty
     b_alg = {k: dict(v) for k, v in B_ALG_STAGE.items()}
     kernel_of = dict(KERNEL_OF_STAGE)
-    if stage[STAGES.index("continuity")] == 0.0:
+    masks = (dim == 2 and args.lanes == 0) or args.lanes == 65
+    if masks or args.lanes not in (0, 64):   # no continuity kernel: its time is in the search pass
         b_alg["search"][dim] += b_alg["continuity"][dim]
-        if dim == 2 and not args.lanes:
+        b_alg["continuity"][dim] = 0.0
+        if masks:
             kernel_of["search"] = "k_mask_build<CPCont> (stencil-row masks + continuity + density preview)"
             kernel_of["momentum_integrate_bin"] = "k_mask_walk<CPMom> (momentum + integrate + bin over the masks)"
     # roofline of the dominant kernel: the longest of the step's kernels
@@ -755,7 +757,7 @@ def main():
                          "kernel_ms": round(dom_ms, 5),
                          "stage_ms": dict(zip(STAGES, [round(x, 5) for x in stage])),
                          "stage_frac": {k: round(b_alg[k][dim] * n / (stage[STAGES.index(k)] * 1e-3) / 1e9
-                                                 / peak, 4) for k in STAGES if stage[STAGES.index(k)] > 0},
+                                                 / peak, 4) for k in STAGES if b_alg[k][dim] > 0},
                          "frac_of_nominal_8tbs": achieved / 8000.0,
                          "limiter": "instruction issue and neighbour-gather latency, not DRAM bandwidth (ncu: "
                                     "DRAM 4-18% busy in the pair kernels; profiles/)",

@@ -125,7 +125,7 @@ struct epp_ctx {
     int last_crit = EPP_CRITERION_SYMMETRY;
     unsigned adj[kMaxTags]{};
     int lanes = 0;             // pair-pass family: 0 warp tiles + lists, 1 cell-centric, 2..32 lane groups
-    bool list_mode = false;    // family 0 in 2D with neighbour lists instead of stencil-row masks
+    int store = 0;             // family 0: 0 = default (2D masks, 3D lists), EPP_TUNING_LISTS, EPP_TUNING_MASKS
     int pass_threads = 128;    // threads per block of the family-0 search and list passes (32, 64, 128)
     int* nlist = nullptr;      // neighbour lists of the last search ([LCAP * cap])
     bool nlist_valid = false;   // the lists match the current order, positions and criterion
@@ -374,26 +374,30 @@ bool generic_physics(const epp_physics* p) {
                  p->tensile != 0);
 }
 
-// Family 0 in 2D keeps stencil-row masks (epp_mask.cuh) unless the context was set to neighbour
-// lists (epp_set_tuning 64); 3D always keeps lists.
-bool uses_masks(const epp_ctx* ctx) { return ctx->D == 2 && !ctx->list_mode; }
+// Family 0 keeps stencil-row masks (epp_mask.cuh) in 2D and neighbour lists in 3D, unless the
+// context was set otherwise (epp_set_tuning EPP_TUNING_LISTS / EPP_TUNING_MASKS).
+bool uses_masks(const epp_ctx* ctx) {
+    return ctx->store == EPP_TUNING_MASKS || (ctx->D == 2 && ctx->store != EPP_TUNING_LISTS);
+}
 
-// The 2D mask search pass with search action `act` (CPCount: masks and nCount only).
-template <class Act>
+// The mask search pass with search action `act` (CPCount: masks and nCount only).
+template <int D, class Act>
 int launch_mask_build(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs) {
     PairArgs A = pair_args(ctx, set, crit);
-    k_mask_build<Act><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
-        A, reinterpret_cast<unsigned*>(ctx->nlist), ctx->cap, act, pairs);
+    if constexpr (D == 2)
+        k_mask2_build<Act><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
+            A, reinterpret_cast<unsigned*>(ctx->nlist), ctx->cap, act, pairs);
+    else
+        k_mask_build<D, Act><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
+            A, reinterpret_cast<unsigned*>(ctx->nlist), ctx->cap, act, pairs);
     CK_LAUNCH();
     return EPP_OK;
 }
 
-// Family 0, the search pass: neighbour lists (masks in 2D) and nCount of set `set` under `crit`.
+// Family 0, the search pass: neighbour lists or masks, and nCount, of set `set` under `crit`.
 template <int D>
 int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
-    if constexpr (D == 2) {
-        if (uses_masks(ctx)) return launch_mask_build(ctx, set, crit, CPCount<2>{ctx->ncount}, pairs);
-    }
+    if (uses_masks(ctx)) return launch_mask_build<D>(ctx, set, crit, CPCount<D>{ctx->ncount}, pairs);
     PairArgs A = pair_args(ctx, set, crit);
     TileMask M{ctx->cap, ctx->nlist};
     k_build<D><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(A, M, ctx->ncount, pairs);
@@ -405,22 +409,25 @@ int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
 // continuity passes do; the filter and extrapolation passes read a subset of the records (and the
 // fused extrapolation writes the wall records others would stage), so they read global memory.
 template <class Act> struct StagesRows { static constexpr bool value = false; };
-template <bool F, bool G> struct StagesRows<CPMom<2, F, G>> { static constexpr bool value = true; };
-template <bool F, bool G> struct StagesRows<CPCont<2, F, G>> { static constexpr bool value = true; };
+template <int D, bool F, bool G> struct StagesRows<CPMom<D, F, G>> { static constexpr bool value = true; };
+template <int D, bool F, bool G> struct StagesRows<CPCont<D, F, G>> { static constexpr bool value = true; };
 
-// Family 0, a pair action over the lists (masks in 2D) of the last search pass (same order and
+// Family 0, a pair action over the lists or masks of the last search pass (same order and
 // positions).
 template <int D, class Act, bool EPI = false>
 int launch_list(epp_ctx* ctx, int set, int crit, const Act& act) {
     PairArgs A = pair_args(ctx, set, crit);
-    if constexpr (D == 2) {
-        if (uses_masks(ctx)) {
-            k_mask_walk<Act, EPI, StagesRows<Act>::value><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0,
-                                                           ctx->stream>>>(
+    if (uses_masks(ctx)) {
+        if constexpr (D == 2)
+            k_mask2_walk<Act, EPI, StagesRows<Act>::value><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads,
+                                                             0, ctx->stream>>>(
                 A, reinterpret_cast<const unsigned*>(ctx->nlist), ctx->cap, act, ctx->scan_state, ctx->n_tiles + 1);
-            CK_LAUNCH();
-            return EPP_OK;
-        }
+        else
+            k_mask_walk<D, Act, EPI, StagesRows<Act>::value><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads,
+                                                              0, ctx->stream>>>(
+                A, reinterpret_cast<const unsigned*>(ctx->nlist), ctx->cap, act, ctx->scan_state, ctx->n_tiles + 1);
+        CK_LAUNCH();
+        return EPP_OK;
     }
     TileMask M{ctx->cap, ctx->nlist};
     k_list<D, Act, EPI><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
@@ -434,8 +441,8 @@ int launch_list(epp_ctx* ctx, int set, int crit, const Act& act) {
 // 2D with masks the search pass runs the search action itself (one kernel).
 template <int D, bool BUILD, class Act, bool EPI = false>
 int launch_pass(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs) {
-    if constexpr (D == 2 && BUILD && !EPI) {
-        if (uses_masks(ctx)) return launch_mask_build(ctx, set, crit, act, pairs);
+    if constexpr (BUILD && !EPI) {
+        if (uses_masks(ctx)) return launch_mask_build<D>(ctx, set, crit, act, pairs);
     }
     if (BUILD) {
         int rc = launch_build<D>(ctx, set, crit, pairs);
@@ -702,7 +709,7 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     CK_LAUNCH();
     EPP_MARK(4);
     int rc;
-    if (ctx->lanes == 0 && uses_masks(ctx)) {   // 2D: one search pass with the continuity action
+    if (ctx->lanes == 0 && uses_masks(ctx)) {   // masks: one search pass with the continuity action
         rc = gen ? launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], Pn, ctx->ncount},
                                         ctx->pairs)
                  : launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], Pn, ctx->ncount},
@@ -1607,23 +1614,32 @@ int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t
         counts[row] = cnt[i];
         if (!ids) continue;
         if (masks) {
-            if (words[(size_t)ctx->cap + i] == kMaskOverflow) continue;   // read from its stencil: not stored
-            const int n0 = ctx->dom.n[0], n1 = ctx->dom.n[1];
+            const int D = ctx->D;
+            const int rows = D == 2 ? MaskConf<2>::ROWS : MaskConf<3>::ROWS;
+            const int W = D == 2 ? MaskConf<2>::W : MaskConf<3>::W;
+            const int own = rows / 2;
+            bool over = true;
+            for (int q = 0; q < W; ++q) over = over && words[(size_t)(own * W + q) * ctx->cap + i] == kMaskOverflow;
+            if (over) continue;   // read from its stencil: not stored
+            const int n0 = ctx->dom.n[0], n1 = ctx->dom.n[1], n2 = ctx->dom.n[2];
             const int rid = cell[i] / n0, cx = cell[i] % n0;
+            const int y = rid % n1, z = rid / n1;
             int k_out = 0;
-            for (int r = 0; r < 3; ++r) {
-                const int yy = rid % n1 + r - 1;
-                if (yy < 0 || yy >= n1) continue;
-                const int crow = rid + r - 1;
-                const int xa = std::max(cx - 1, 0), xb = std::min(cx + 1, n0 - 1);
-                const int lo = std::max(start[(size_t)crow * n0 + xa], 0);
-                unsigned w = words[(size_t)r * ctx->cap + i];
-                for (int k = 0; w; ++k, w >>= 1) {
-                    if (!(w & 1u)) continue;
-                    const int j = lo + k;
-                    if (j >= n_alive) return fail(ctx, EPP_ERR_DEVICE_STATUS, "mask bit %d of particle %d: index %d", k, i, j);
-                    if (k_out < max_nb) ids[(size_t)k_out * ld + row] = id[j] + 1;
-                    ++k_out;
+            for (int r = 0; r < rows; ++r) {
+                const int yy = y + (D == 2 ? r : r % 3) - 1, zz = D == 2 ? z : z + r / 3 - 1;
+                if (yy < 0 || yy >= n1 || (D == 3 && (zz < 0 || zz >= n2))) continue;
+                const int crow = yy + n1 * zz;
+                const int lo = std::max(start[(size_t)crow * n0 + std::max(cx - 1, 0)], 0);
+                for (int q = 0; q < W; ++q) {
+                    unsigned w = words[(size_t)(r * W + q) * ctx->cap + i];
+                    for (int k = 32 * q; w; ++k, w >>= 1) {
+                        if (!(w & 1u)) continue;
+                        const int j = lo + k;
+                        if (j >= n_alive)
+                            return fail(ctx, EPP_ERR_DEVICE_STATUS, "mask bit %d of particle %d: index %d", k, i, j);
+                        if (k_out < max_nb) ids[(size_t)k_out * ld + row] = id[j] + 1;
+                        ++k_out;
+                    }
                 }
             }
             continue;
@@ -1750,15 +1766,17 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     const int g0 = lanes_per_particle;
-    if (g0 != 0 && g0 != 1 && g0 != 2 && g0 != 4 && g0 != 8 && g0 != 16 && g0 != 32 && g0 != EPP_TUNING_LISTS)
-        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pair-pass family %d not in {0,1,2,4,8,16,32,64}", g0);
-    const int g = g0 == EPP_TUNING_LISTS ? 0 : g0;
-    const bool lists = g0 == EPP_TUNING_LISTS;
+    if (g0 != 0 && g0 != 1 && g0 != 2 && g0 != 4 && g0 != 8 && g0 != 16 && g0 != 32 && g0 != EPP_TUNING_LISTS &&
+        g0 != EPP_TUNING_MASKS)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pair-pass family %d not in {0,1,2,4,8,16,32,64,65}", g0);
+    const bool fam0 = g0 == EPP_TUNING_LISTS || g0 == EPP_TUNING_MASKS;
+    const int g = fam0 ? 0 : g0;
+    const int store = fam0 ? g0 : 0;
     if (g != 0 && ctx->n_inst > 1)
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "batches of %d instances use pair-pass family 0", ctx->n_inst);
-    if (g != ctx->lanes || lists != ctx->list_mode) {
+    if (g != ctx->lanes || store != ctx->store) {
         ctx->lanes = g;
-        ctx->list_mode = lists;
+        ctx->store = store;
         ctx->nlist_valid = false;
         drop_graphs(ctx);
     }

@@ -9,6 +9,8 @@
 // of the same target -- a fixed order, so results are deterministic.  This replaces the
 // thread-per-particle loop in which only about a third of the lanes had a neighbour at any time.
 #pragma once
+#include <type_traits>
+
 #include "epp_pair_g.cuh"
 
 namespace epp {
@@ -109,17 +111,31 @@ struct CPCont {
         float4 v;
         float rho;
     };
-    struct Nb {
+    // what the term reads of a neighbour: (vx, vy, vz, m) and V_j; in 2D V_j rides in the unused z
+    // lane, so a record is 16 bytes (staged rows of the mask passes stay small)
+    struct Nb3 {
         float4 v;
         float vol;
     };
+    struct Nb2 {
+        float4 v;   // (vx, vy, V, m)
+    };
+    using Nb = typename std::conditional<D == 2, Nb2, Nb3>::type;
+    __device__ __forceinline__ static float vol_of(const Nb2& n) { return n.v.z; }
+    __device__ __forceinline__ static float vol_of(const Nb3& n) { return n.vol; }
     __device__ __forceinline__ Self self(int i) const { return Self{s.vm[i], s.rho[i]}; }
     // Neighbour records go through the read-only path: no pass writes what it gathers.
     // V_j enters only the balanced (fluid-wall, wall-fluid) term: in 3D fluid-fluid pairs skip its
     // load (5% off the pass); in 2D, without the 3D software pipeline, the branch costs more than
     // the 4-byte gather saves
     __device__ __forceinline__ Nb fetch(int j, int ti, int tj) const {
-        return Nb{__ldg(&s.vm[j]), D == 3 && ti == P.fluid && tj == P.fluid ? 0.0f : __ldg(&s.vol[j])};
+        if constexpr (D == 2) {
+            float4 v = __ldg(&s.vm[j]);
+            v.z = __ldg(&s.vol[j]);
+            return Nb{v};
+        } else {
+            return Nb{__ldg(&s.vm[j]), ti == P.fluid && tj == P.fluid ? 0.0f : __ldg(&s.vol[j])};
+        }
     }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
                                            const PairGeo& g, const TargetConst& tc) const {
@@ -137,7 +153,7 @@ struct CPCont {
         vdx += g.dy * (me.v.y - nb.v.y);
         if (D == 3) vdx += g.dz * (me.v.z - nb.v.z);
         if (ff) out.x = nb.v.w * vdx * dwr;                     // iClassicContinuity!
-        else out.x = me.rho * nb.vol * vdx * dwr;               // iBalancedContinuity!
+        else out.x = me.rho * vol_of(nb) * vdx * dwr;           // iBalancedContinuity!
         return out;
     }
     __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,
@@ -231,10 +247,14 @@ struct CPMom {
         float c0;
         float gap;   // GEN with the tensile correction only
     };
-    struct Nb {
+    struct NbG {
         float4 v, rp;
         float gap;
     };
+    struct NbP {   // the benchmark physics reads no gap
+        float4 v, rp;
+    };
+    using Nb = typename std::conditional<GEN, NbG, NbP>::type;
     __device__ __forceinline__ float gap_of(int i) const {
         return GEN && m.P.tensile ? m.P.gap[m.s.id[i]] : 0.0f;
     }
@@ -242,7 +262,8 @@ struct CPMom {
         return Self{m.s.vm[i], m.s.rp4[i], m.P.c0_of(inst_of(m.s.tagm[i])), gap_of(i)};
     }
     __device__ __forceinline__ Nb fetch(int j, int, int) const {
-        return Nb{__ldg(&m.s.vm[j]), __ldg(&m.s.rp4[j]), gap_of(j)};
+        if constexpr (GEN) return Nb{__ldg(&m.s.vm[j]), __ldg(&m.s.rp4[j]), gap_of(j)};
+        else return Nb{__ldg(&m.s.vm[j]), __ldg(&m.s.rp4[j])};
     }
     __device__ __forceinline__ float4 term(const Self& me, const Nb& nb, int ti, int tj, float4 xj,
                                            const PairGeo& g, const TargetConst& tc) const {
@@ -258,7 +279,7 @@ struct CPMom {
         if (dwr == 0.0f) return out;
         const float4 rpi = me.rp, rpj = nb.rp, vi = me.v, vj = nb.v;
         float p_rho_2;
-        if (!GEN) {   // the dam break's pair: classic fluid-fluid, balanced fluid-wall
+        if constexpr (!GEN) {   // the dam break's pair: classic fluid-fluid, balanced fluid-wall
             p_rho_2 = ff ? rpi.z + rpj.z : (rpi.y + rpj.y) * rpi.w * rpj.w;
         } else {
             p_rho_2 = pressure_term(ff ? P.pff : P.pfw, rpi, rpj);

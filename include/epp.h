@@ -296,10 +296,13 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
  * neighbour list that the momentum pass reuses; 1 = one warp per occupied cell with a compacted
  * pair queue; 2, 4, 8, 16 or 32 = that many lanes of a warp per particle.  Chosen by the
  * autotuner; results change only at the FP32 rounding level (neighbour sets are identical).
- * In 2D, family 0 keeps per-particle stencil-row masks (three 32-bit words: which candidates of
- * each stencil row are neighbours) in place of lists, and its search pass runs the search action;
- * EPP_TUNING_LISTS selects family 0 with neighbour lists instead (the same sums, bit for bit). */
+ * In 2D, family 0 keeps per-particle stencil-row masks (one 32-bit word per stencil row: which
+ * candidates of the row are neighbours) in place of lists, and its search pass runs the search
+ * action; in 3D it keeps neighbour lists.  EPP_TUNING_LISTS and EPP_TUNING_MASKS select family 0
+ * with lists or masks (two words per row in 3D) in either dimension: the same neighbours in the
+ * same order, sums equal to FP32 rounding. */
 #define EPP_TUNING_LISTS 64
+#define EPP_TUNING_MASKS 65
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
 /* Threads per block of the family-0 search and list passes: 128 (default), 64 or 32.  Smaller
  * blocks spread a small system over more SMs; results do not change (the per-particle order is

@@ -1,10 +1,12 @@
-"""2D stencil-row masks (the default family-0 pair passes in 2D) against the neighbour-list passes.
+"""Stencil-row masks (the default family-0 pair passes in 2D, EPP_TUNING_MASKS in 3D) against the
+neighbour-list passes.
 
 Both forms visit every particle's neighbours in the same order (stencil rows, then cell order,
-then id order inside a cell), so every sum is the same: the state after fused steps, per-call
-actions and the neighbour sets must be bit-identical between a context on masks and one set to
-EPP_TUNING_LISTS, including multi-tile grids, warps that cross cell-row ends and particles whose
-stencil rows hold more than 32 candidates (read from their stencil)."""
+then id order inside a cell) with the same pair terms, so the neighbour counts and sets are
+identical and every sum agrees to FP32 rounding (the compiler may contract a multiply and an add
+into one fused operation differently in the two kernels).  Checked after fused steps and per-call
+actions, on multi-tile grids, warps that cross cell-row ends and particles whose stencil rows hold
+more candidates than a row's words (read from their stencil)."""
 import numpy as np
 import pytest
 
@@ -19,8 +21,9 @@ FIELDS = ("PositionVec", "VelocityVec", "Density", "dDensity", "Pressure", "Volu
 
 
 def pair_of_contexts(case):
+    """(masks, lists) contexts of the same case."""
     out = []
-    for tuning in (0, abi.EPP_TUNING_LISTS):
+    for tuning in (abi.EPP_TUNING_MASKS, abi.EPP_TUNING_LISTS):
         ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
         d = DeviceParticleSystem(case.ps, ns)
         d.ctx.set_tuning(tuning)
@@ -34,14 +37,33 @@ def host_fields(d):
     return {k: d.host[k].copy() for k in FIELDS}
 
 
+FLOORS = {"PositionVec": 1.0, "VelocityVec": 1e-2, "Density": 1.0, "dDensity": 1.0, "Pressure": 1.0,
+          "Volume": 1e-9, "dVelocityVec": 1.0}
+
+
 def assert_same(a, b, what):
+    """nCount exactly; the rest to FP32 rounding: |a - b| <= 1e-5 max(|b|, floor)."""
+    assert np.array_equal(a["nCount"], b["nCount"]), (what, "nCount")
     for k in FIELDS:
-        assert np.array_equal(a[k], b[k]), (what, k)
+        if k == "nCount":
+            continue
+        x, y = a[k].astype(np.float64), b[k].astype(np.float64)
+        assert np.all(np.isfinite(x)) and np.all(np.isfinite(y)), (what, k)
+        err = np.max(np.abs(x - y) / np.maximum(np.abs(y), FLOORS[k])) if x.size else 0.0
+        assert err <= 1e-5, (what, k, err, int(np.sum(x != y)))
 
 
-@pytest.mark.parametrize("dx,h_factor,steps", [(0.04, 1.5, 20), (0.02, 1.5, 10), (0.04, 3.0, 4)])
-def test_fused_steps_bit_identical(dx, h_factor, steps):
-    case = casegen.dam_break_2d(dx=dx, h_factor=h_factor, max_neighbour_number=1)
+def case_of(dim, dx, h_factor):
+    if dim == 2:
+        return casegen.dam_break_2d(dx=dx, h_factor=h_factor, max_neighbour_number=1)
+    return casegen.dam_break_3d(dx=dx, tank=(0.6, 0.3, 0.4), column=(0.2, 0.3, 0.24), h_factor=h_factor,
+                                max_neighbour_number=1)
+
+
+@pytest.mark.parametrize("dim,dx,h_factor,steps", [(2, 0.04, 1.5, 20), (2, 0.02, 1.5, 10), (2, 0.04, 3.0, 4),
+                                                   (3, 0.02, 1.3, 8), (3, 0.01, 1.3, 3), (3, 0.02, 2.0, 3)])
+def test_fused_steps_match(dim, dx, h_factor, steps):
+    case = case_of(dim, dx, h_factor)
     phys = case.physics
     m, l = pair_of_contexts(case)
     for d in (m, l):
@@ -55,7 +77,7 @@ def test_fused_steps_bit_identical(dx, h_factor, steps):
     cb, ib = l.ctx.neighbour_lists(n, 160)
     assert np.array_equal(ca, cb)
     stored = ia[:, 0] != 0
-    if h_factor > 2:   # stencil rows of more than 32 candidates: read from the stencil, not stored
+    if h_factor >= 2:   # stencil rows beyond a row's words: read from the stencil, not stored
         assert stored.sum() < n
     keep = stored & (ib[:, 0] != 0)
     assert np.array_equal(ia[keep], ib[keep])
@@ -63,10 +85,11 @@ def test_fused_steps_bit_identical(dx, h_factor, steps):
         d.close()
 
 
-def test_per_call_actions_bit_identical():
+@pytest.mark.parametrize("dim", [2, 3])
+def test_per_call_actions_match(dim):
     """search! (count only and continuity), interaction! (momentum, neighbour count, kernel filter,
     pressure extrapolation) and selfaction! on both forms."""
-    case = casegen.dam_break_2d(dx=0.04, max_neighbour_number=1)
+    case = case_of(dim, 0.04 if dim == 2 else 0.02, 1.5 if dim == 2 else 1.3)
     phys = case.physics
     m, l = pair_of_contexts(case)
     for d in (m, l):
@@ -89,7 +112,7 @@ def test_per_call_actions_bit_identical():
         d.close()
 
 
-def test_default_criterion_and_example_physics_bit_identical():
+def test_default_criterion_and_example_physics_match():
     """The default criterion (dr^2 <= gap^2) and the example's physics (CubicSpline, classic
     viscosity, kernel filter every 20 steps inside epp_step)."""
     case = casegen.dam_break_2d(dx=0.04, max_neighbour_number=1, physics="example")

@@ -14,10 +14,12 @@ h = 2 dx) lists overflow their capacity:
   passes' stencil fallback).
 
 Bars: cell counts, offsets, sorted membership, nCount and neighbour sets bit-exact; dρ/dt and
-dv/dt within 1e-5 of each particle's term scale against the FP32 oracle and against the FP64
-oracle.  The plain relative errors (floors g and 1e-6 rho0 c0 / h) are reported next to the FP32
-oracle's own error against FP64, and the device's may not exceed the FP32 oracle's by more than
-a factor of 4 (99.9th percentile): the CUDA path is as accurate as the reference's arithmetic.
+dv/dt within 1e-5 of each particle's term scale against the FP32 oracle.  Against the FP64 oracle
+the device's errors -- term scale, and plain relative error with floors g and 1e-6 rho0 c0 / h, as
+99.9th percentile and max -- may not exceed the FP32 oracle's own (the reference's FP32
+arithmetic) by more than half again: the CUDA path is as accurate as the reference's arithmetic.
+FP32 itself is far from FP64 in the plain relative measure near rest (dv/dt sums cancel terms
+about 10^3 times larger than g), which is why the per-particle bar is the term scale.
 """
 import json
 
@@ -49,13 +51,14 @@ def test_parity_at_scale(name):
     assert r["cells"], "cell counts / offsets / sorted ids differ"
     assert r["ncount"], "nCount differs"
     assert r["sets"], "neighbour sets differ"
-    if name == "3d_dx0.02_h2dx":   # the stencil fallback runs for most particles
-        assert r["sets_rows_compared"] < r["particles"] // 2
+    if name == "3d_dx0.02_h2dx":   # the stencil fallback runs for the particles beyond a list
+        assert r["sets_rows_compared"] < r["particles"]
     else:
         assert r["sets_rows_compared"] == r["particles"]
     for stage in ("drho", "dv"):
         e = r[stage]
         assert e["term_vs_fp32"] < TERM, (stage, e)
-        assert e["term_vs_fp64"] < TERM, (stage, e)
-        ref = max(e["oracle_fp32_rel_vs_fp64"]["p999"], 1e-6)
-        assert e["rel_vs_fp64"]["p999"] <= 4.0 * ref, (stage, e)
+        # against FP64: no further from it than the reference's own FP32 arithmetic (the FP32 oracle)
+        assert e["term_vs_fp64"] <= 1.5 * e["oracle_fp32_term_vs_fp64"] + TERM, (stage, e)
+        for q in ("p999", "max"):
+            assert e["rel_vs_fp64"][q] <= 1.5 * e["oracle_fp32_rel_vs_fp64"][q] + 1e-6, (stage, q, e)
