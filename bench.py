@@ -673,17 +673,16 @@ def main():
                 flush.fill_(1.0)
             stage += np.array(ctx.profile_step(phys))
         stage /= nprof
-    # 2D family 0 runs the continuity action inside the search pass (stencil-row masks): that
+    # 2D family 0 runs the continuity action inside the search pass (the window search): that
     # kernel carries both stages' bytes and the continuity stage is empty
     b_alg = {k: dict(v) for k, v in B_ALG_STAGE.items()}
     kernel_of = dict(KERNEL_OF_STAGE)
-    masks = (dim == 2 and args.lanes == 0) or args.lanes == 65
-    if masks or args.lanes not in (0, 64):   # no continuity kernel: its time is in the search pass
+    windows = dim == 2 and args.lanes == 0
+    if windows or args.lanes not in (0, 64):   # no continuity kernel: its time is in the search pass
         b_alg["search"][dim] += b_alg["continuity"][dim]
         b_alg["continuity"][dim] = 0.0
-        if masks:
-            kernel_of["search"] = "k_mask_build<CPCont> (stencil-row masks + continuity + density preview)"
-            kernel_of["momentum_integrate_bin"] = "k_mask_walk<CPMom> (momentum + integrate + bin over the masks)"
+        if windows:
+            kernel_of["search"] = "k_win_build<CPCont> (window search + lists + continuity + density preview)"
     # roofline of the dominant kernel: the longest of the step's kernels
     dom_stage = max(STAGES, key=lambda k: stage[STAGES.index(k)])
     dom_ms = float(stage[STAGES.index(dom_stage)])

@@ -12,7 +12,7 @@
 #include <type_traits>
 #include <vector>
 
-#include "epp_mask.cuh"
+#include "epp_window.cuh"
 #include "epp_self.cuh"
 
 using namespace epp;
@@ -125,7 +125,7 @@ struct epp_ctx {
     int last_crit = EPP_CRITERION_SYMMETRY;
     unsigned adj[kMaxTags]{};
     int lanes = 0;             // pair-pass family: 0 warp tiles + lists, 1 cell-centric, 2..32 lane groups
-    int store = 0;             // family 0: 0 = default (2D masks, 3D lists), EPP_TUNING_LISTS, EPP_TUNING_MASKS
+    int store = 0;             // family 0: 0 = default (2D window search), EPP_TUNING_LISTS (lockstep list search)
     int pass_threads = 128;    // threads per block of the family-0 search and list passes (32, 64, 128)
     int* nlist = nullptr;      // neighbour lists of the last search ([LCAP * cap])
     bool nlist_valid = false;   // the lists match the current order, positions and criterion
@@ -374,30 +374,27 @@ bool generic_physics(const epp_physics* p) {
                  p->tensile != 0);
 }
 
-// Family 0 keeps stencil-row masks (epp_mask.cuh) in 2D and neighbour lists in 3D, unless the
-// context was set otherwise (epp_set_tuning EPP_TUNING_LISTS / EPP_TUNING_MASKS).
-bool uses_masks(const epp_ctx* ctx) {
-    return ctx->store == EPP_TUNING_MASKS || (ctx->D == 2 && ctx->store != EPP_TUNING_LISTS);
-}
+// Family 0 in 2D searches each particle's own stencil-row windows with the search action folded in
+// (epp_window.cuh), unless the context was set to the lockstep list search and a separate
+// continuity pass (epp_set_tuning EPP_TUNING_LISTS); 3D always uses the latter.
+bool uses_windows(const epp_ctx* ctx) { return ctx->D == 2 && ctx->store != EPP_TUNING_LISTS; }
 
-// The mask search pass with search action `act` (CPCount: masks and nCount only).
-template <int D, class Act>
-int launch_mask_build(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs) {
+// The 2D window search pass with search action `act` (CPCount: lists and nCount only).
+template <class Act>
+int launch_win_build(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs) {
     PairArgs A = pair_args(ctx, set, crit);
-    if constexpr (D == 2)
-        k_mask2_build<Act><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
-            A, reinterpret_cast<unsigned*>(ctx->nlist), ctx->cap, act, pairs);
-    else
-        k_mask_build<D, Act><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
-            A, reinterpret_cast<unsigned*>(ctx->nlist), ctx->cap, act, pairs);
+    TileMask M{ctx->cap, ctx->nlist};
+    k_win_build<Act><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(A, M, act, pairs);
     CK_LAUNCH();
     return EPP_OK;
 }
 
-// Family 0, the search pass: neighbour lists or masks, and nCount, of set `set` under `crit`.
+// Family 0, the search pass: neighbour lists and nCount of set `set` under `crit`.
 template <int D>
 int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
-    if (uses_masks(ctx)) return launch_mask_build<D>(ctx, set, crit, CPCount<D>{ctx->ncount}, pairs);
+    if constexpr (D == 2) {
+        if (uses_windows(ctx)) return launch_win_build(ctx, set, crit, CPCount<2>{ctx->ncount}, pairs);
+    }
     PairArgs A = pair_args(ctx, set, crit);
     TileMask M{ctx->cap, ctx->nlist};
     k_build<D><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(A, M, ctx->ncount, pairs);
@@ -405,30 +402,10 @@ int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
     return EPP_OK;
 }
 
-// Whether the 2D mask walk of an action stages its neighbours in shared memory: the momentum and
-// continuity passes do; the filter and extrapolation passes read a subset of the records (and the
-// fused extrapolation writes the wall records others would stage), so they read global memory.
-template <class Act> struct StagesRows { static constexpr bool value = false; };
-template <int D, bool F, bool G> struct StagesRows<CPMom<D, F, G>> { static constexpr bool value = true; };
-template <int D, bool F, bool G> struct StagesRows<CPCont<D, F, G>> { static constexpr bool value = true; };
-
-// Family 0, a pair action over the lists or masks of the last search pass (same order and
-// positions).
+// Family 0, a pair action over the lists of the last search pass (same order and positions).
 template <int D, class Act, bool EPI = false>
 int launch_list(epp_ctx* ctx, int set, int crit, const Act& act) {
     PairArgs A = pair_args(ctx, set, crit);
-    if (uses_masks(ctx)) {
-        if constexpr (D == 2)
-            k_mask2_walk<Act, EPI, StagesRows<Act>::value><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads,
-                                                             0, ctx->stream>>>(
-                A, reinterpret_cast<const unsigned*>(ctx->nlist), ctx->cap, act, ctx->scan_state, ctx->n_tiles + 1);
-        else
-            k_mask_walk<D, Act, EPI, StagesRows<Act>::value><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads,
-                                                              0, ctx->stream>>>(
-                A, reinterpret_cast<const unsigned*>(ctx->nlist), ctx->cap, act, ctx->scan_state, ctx->n_tiles + 1);
-        CK_LAUNCH();
-        return EPP_OK;
-    }
     TileMask M{ctx->cap, ctx->nlist};
     k_list<D, Act, EPI><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
         A, M, ctx->ncount, act, ctx->scan_state, ctx->n_tiles + 1);
@@ -438,11 +415,11 @@ int launch_list(epp_ctx* ctx, int set, int crit, const Act& act) {
 
 // A pair pass of family 0.  BUILD: the search pass first (new lists at the current positions);
 // then the action over the lists (none for the count-only action: the search wrote nCount).  In
-// 2D with masks the search pass runs the search action itself (one kernel).
+// 2D with the window search, the search pass runs the search action itself (one kernel).
 template <int D, bool BUILD, class Act, bool EPI = false>
 int launch_pass(epp_ctx* ctx, int set, int crit, const Act& act, unsigned long long* pairs) {
-    if constexpr (BUILD && !EPI) {
-        if (uses_masks(ctx)) return launch_mask_build<D>(ctx, set, crit, act, pairs);
+    if constexpr (D == 2 && BUILD && !EPI) {
+        if (uses_windows(ctx)) return launch_win_build(ctx, set, crit, act, pairs);
     }
     if (BUILD) {
         int rc = launch_build<D>(ctx, set, crit, pairs);
@@ -709,7 +686,7 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     CK_LAUNCH();
     EPP_MARK(4);
     int rc;
-    if (ctx->lanes == 0 && uses_masks(ctx)) {   // masks: one search pass with the continuity action
+    if (ctx->lanes == 0 && uses_windows(ctx)) {   // 2D windows: one search pass with the continuity action
         rc = gen ? launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], Pn, ctx->ncount},
                                         ctx->pairs)
                  : launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], Pn, ctx->ncount},
@@ -1583,7 +1560,6 @@ int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t
     if (n == 0) return EPP_OK;
     const int lcap = ctx->D == 2 ? ListConf<2>::LCAP : ListConf<3>::LCAP;
     const bool row_major = ctx->D == 2 ? ListConf<2>::ROW : ListConf<3>::ROW;
-    const bool masks = uses_masks(ctx);
     int n_alive = 0;
     CK(cudaMemcpyAsync(&n_alive, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
                        ctx->stream));
@@ -1597,53 +1573,12 @@ int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t
         CK(cudaMemcpyAsync(list.data(), ctx->nlist, sizeof(int) * list.size(), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     }
-    std::vector<int> start, cell;
-    if (masks && n_alive > 0) {   // 2D masks: each row word indexes the particle's window in that stencil row
-        start.resize(ctx->n_cells + 2);
-        cell.resize(n_alive);
-        CK(cudaMemcpyAsync(start.data(), ctx->start[ctx->cur], sizeof(int) * (ctx->n_cells + 1), cudaMemcpyDeviceToHost,
-                           ctx->stream));
-        CK(cudaMemcpyAsync(cell.data(), ctx->S[ctx->cur].cell, sizeof(int) * n_alive, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-    }
-    const unsigned* words = reinterpret_cast<const unsigned*>(list.data());
     for (int r = 0; r < n; ++r) counts[r] = 0;   // particles not alive have no list
     for (int i = 0; i < n_alive; ++i) {
         const int row = id[i];
         if (row < 0 || row >= n) return fail(ctx, EPP_ERR_DEVICE_STATUS, "sorted particle %d has id %d", i, row);
         counts[row] = cnt[i];
         if (!ids) continue;
-        if (masks) {
-            const int D = ctx->D;
-            const int rows = D == 2 ? MaskConf<2>::ROWS : MaskConf<3>::ROWS;
-            const int W = D == 2 ? MaskConf<2>::W : MaskConf<3>::W;
-            const int own = rows / 2;
-            bool over = true;
-            for (int q = 0; q < W; ++q) over = over && words[(size_t)(own * W + q) * ctx->cap + i] == kMaskOverflow;
-            if (over) continue;   // read from its stencil: not stored
-            const int n0 = ctx->dom.n[0], n1 = ctx->dom.n[1], n2 = ctx->dom.n[2];
-            const int rid = cell[i] / n0, cx = cell[i] % n0;
-            const int y = rid % n1, z = rid / n1;
-            int k_out = 0;
-            for (int r = 0; r < rows; ++r) {
-                const int yy = y + (D == 2 ? r : r % 3) - 1, zz = D == 2 ? z : z + r / 3 - 1;
-                if (yy < 0 || yy >= n1 || (D == 3 && (zz < 0 || zz >= n2))) continue;
-                const int crow = yy + n1 * zz;
-                const int lo = std::max(start[(size_t)crow * n0 + std::max(cx - 1, 0)], 0);
-                for (int q = 0; q < W; ++q) {
-                    unsigned w = words[(size_t)(r * W + q) * ctx->cap + i];
-                    for (int k = 32 * q; w; ++k, w >>= 1) {
-                        if (!(w & 1u)) continue;
-                        const int j = lo + k;
-                        if (j >= n_alive)
-                            return fail(ctx, EPP_ERR_DEVICE_STATUS, "mask bit %d of particle %d: index %d", k, i, j);
-                        if (k_out < max_nb) ids[(size_t)k_out * ld + row] = id[j] + 1;
-                        ++k_out;
-                    }
-                }
-            }
-            continue;
-        }
         if (cnt[i] > lcap) continue;   // beyond the list's capacity: read from its stencil, not stored
         const int kept = std::min(cnt[i], (int)max_nb);
         for (int k = 0; k < kept; ++k) {
@@ -1766,10 +1701,9 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     const int g0 = lanes_per_particle;
-    if (g0 != 0 && g0 != 1 && g0 != 2 && g0 != 4 && g0 != 8 && g0 != 16 && g0 != 32 && g0 != EPP_TUNING_LISTS &&
-        g0 != EPP_TUNING_MASKS)
-        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pair-pass family %d not in {0,1,2,4,8,16,32,64,65}", g0);
-    const bool fam0 = g0 == EPP_TUNING_LISTS || g0 == EPP_TUNING_MASKS;
+    if (g0 != 0 && g0 != 1 && g0 != 2 && g0 != 4 && g0 != 8 && g0 != 16 && g0 != 32 && g0 != EPP_TUNING_LISTS)
+        return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "pair-pass family %d not in {0,1,2,4,8,16,32,64}", g0);
+    const bool fam0 = g0 == EPP_TUNING_LISTS;
     const int g = fam0 ? 0 : g0;
     const int store = fam0 ? g0 : 0;
     if (g != 0 && ctx->n_inst > 1)

@@ -1,0 +1,243 @@
+// epp_window.cuh -- the 2D search pass over per-particle stencil-row windows, with the search
+// action folded in.
+//
+// A particle's 3x3 cell stencil is three stencil rows (dy = -1, 0, +1); in each row its
+// candidates are one contiguous cell-order range, cells cx-1 .. cx+1 (its "window", about 27
+// particles at h = 1.5 dx).  The list search pass (k_build) tests, in lockstep, every candidate of
+// the warp's union of stencils against every lane -- about 190 per particle; here each lane tests
+// only its own window, 81 candidates.
+//
+// A warp takes 32 consecutive particles in cell order.  When their cells lie in one cell row, the
+// union of their windows in a stencil row is one contiguous range; the warp stages the three union
+// rows (up to 64 candidates each) in shared memory in one round -- position and h, the list entry
+// (index and tag) in the unused z lane, and the search action's neighbour record -- and every lane
+// reads its own window from there.  For each 32-candidate chunk of a window the lane builds one
+// acceptance word with the reference's IEEE criterion (and the active-pair matrix, applied from
+// per-row tag bitmaps), then walks its set bits in ascending order: it appends the neighbour to its
+// list (the lists the momentum, filter and extrapolation passes read; same layout and order as
+// k_build's: stencil rows, then cell order, then id order inside a cell) and adds the search
+// action's term -- the continuity rate -- from the staged record, so no separate continuity pass
+// walks the neighbours again.  Warps that cross a cell-row end, and union rows longer than 64,
+// read the candidates from global memory instead.
+#pragma once
+#include "epp_tile.cuh"
+
+namespace epp {
+
+struct RowWin {
+    int lo, hi;   // candidate range [lo, hi) in cell order
+};
+
+// Linear cell row of stencil row r (0, 1, 2 for dy = -1, 0, +1) of the cell row `rid` (y + n1 k;
+// k is the instance of a batch), or -1 when y + dy is outside the grid.
+__device__ __forceinline__ int stencil_row2(const PairArgs& A, int rid, int r) {
+    const int yy = rid % A.dom.n[1] + r - 1;
+    return (yy >= 0 && yy < A.dom.n[1]) ? rid + r - 1 : -1;
+}
+
+// Candidates of cells xa .. xb (clamped to the grid) of linear cell row `row` (-1: none).
+__device__ __forceinline__ RowWin row_range(const PairArgs& A, int row, int xa, int xb) {
+    RowWin w{0, 0};
+    if (row < 0) return w;
+    const int n0 = A.dom.n[0];
+    xa = max(xa, 0);
+    xb = min(xb, n0 - 1);
+    if (xa > xb) return w;
+    const int l = max(A.start[row * n0 + xa], 0);
+    const int h = min(A.start[row * n0 + xb + 1], A.n_max);
+    w.lo = l;
+    w.hi = max(h, l);
+    return w;
+}
+
+template <class Act>
+struct Stage2 {
+    float4 x[3 * 64];                 // (x, y, list entry as bits, h)
+    typename Act::Nb nb[3 * 64];
+};
+
+// Stages union rows u[0..2] (each at most 64 candidates) and records, per row, the union slots
+// whose tag this lane's row of the active-pair matrix allows and whether every candidate of the
+// row has one h (one_h, h0).  A tag outside 1..n_tags sets EPP_STATUS_BAD_TAG.  Warp-collective.
+template <class Act, bool FETCH>
+__device__ __forceinline__ void stage_rows2(const PairArgs& A, const Act& act, Stage2<Act>& S, const RowWin (&u)[3],
+                                            unsigned amask, int lane, unsigned& st, unsigned long long (&allowed)[3],
+                                            bool (&one_h)[3], float (&h0)[3]) {
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        allowed[r] = 0ull;
+        one_h[r] = true;
+        h0[r] = 0.0f;
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            if (u[r].lo + part * 32 >= u[r].hi) break;   // warp-uniform: nothing left in this row
+            const int k = part * 32 + lane;
+            const int j = u[r].lo + k;
+            const bool real = j < u[r].hi;
+            const float4 xj = real ? A.s.xh[j] : make_float4(1e30f, 1e30f, 0.0f, 0.0f);
+            const int tj = real ? tag_of(A.s.tagm[j]) : 0;
+            S.x[64 * r + k] = make_float4(xj.x, xj.y, __int_as_float(list_entry(j, tj >= 1 ? tj : 1)), xj.w);
+            if (FETCH && real) S.nb[64 * r + k] = act.fetch(j, 0, tj);
+            if (__ballot_sync(0xffffffffu, real && (tj < 1 || tj > A.n_tags))) st |= EPP_STATUS_BAD_TAG;
+            for (int t = 1; t <= A.n_tags; ++t) {
+                const unsigned b = __ballot_sync(0xffffffffu, real && tj == t);
+                if ((amask >> (t - 1)) & 1u) allowed[r] |= (unsigned long long)b << (part * 32);
+            }
+            const float hf = __shfl_sync(0xffffffffu, xj.w, 0);
+            if (part == 0) h0[r] = hf;
+            one_h[r] = __all_sync(0xffffffffu, !real || xj.w == h0[r]) && one_h[r];
+        }
+    }
+    __syncwarp();
+}
+
+// Acceptance bits of staged candidates [k0, k1) (k1 - k0 <= 32) of a lane's window starting at
+// slot `off`: bit k - k0 set when candidate k is within the criterion's radius, by the reference's
+// IEEE arithmetic.  `uniform`: every candidate has the lane's h (or the default criterion), so one
+// exact bound `r2u` serves; otherwise the bound is looked up per candidate.
+__device__ __forceinline__ unsigned window_bits(const float4* sx, int off, int k0, int k1, float4 xi, bool uniform,
+                                                float r2u, float h2sq, bool dflt, float gap_square) {
+    unsigned word = 0u;
+    if (uniform) {
+        // dr2 <= R2 as integers: non-negative floats order like their bit patterns, so
+        // bits(dr2) - bits(R2) - 1 is negative exactly for the accepted candidates
+        const int nR2 = -__float_as_int(r2u) - 1;
+        for (int k = k1 - 1; k >= k0; --k) {
+            const float4 xj = sx[off + k];
+            const float dx = __fsub_rn(xi.x, xj.x);
+            const float dy = __fsub_rn(xi.y, xj.y);
+            const float d = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+            word = (word << 1) | ((unsigned)(__float_as_int(d) + nR2) >> 31);
+        }
+        return word;
+    }
+    float hc = xi.w, rc = dflt ? gap_square : h2sq;
+    for (int k = k1 - 1; k >= k0; --k) {
+        const float4 xj = sx[off + k];
+        const float dx = __fsub_rn(xi.x, xj.x);
+        const float dy = __fsub_rn(xi.y, xj.y);
+        const float d = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        if (xj.w != hc) {
+            hc = xj.w;
+            rc = dflt ? gap_square : (hc == xi.w ? h2sq : pair_r2(xi.w, hc));
+        }
+        word = (word << 1) | (d <= rc ? 1u : 0u);
+    }
+    return word;
+}
+
+// The 2D search pass: neighbour lists and nCount, and the search action of `Act` over the accepted
+// neighbours in list order (CPCont: continuity + density preview; CPCount: the count only).  A
+// particle with more neighbours than a list keeps has only those stored (the pair passes read its
+// stencil); its search action still covers all of them.
+template <class Act>
+__global__ void __launch_bounds__(128) k_win_build(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M,
+                                                   const __grid_constant__ Act act, unsigned long long* pairs) {
+    __shared__ Stage2<Act> stage[4];
+    const int lane = threadIdx.x & 31;
+    Stage2<Act>& S = stage[threadIdx.x >> 5];
+    const int n_alive = min(A.start[A.dom.n_cells], A.n_max);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int w0 = i - lane;
+    int cnt = 0;
+    if (w0 < n_alive) {   // warp-uniform
+        const bool on = i < n_alive;
+        const int n0 = A.dom.n[0];
+        const int c_first = A.s.cell[w0];
+        const int c_last = A.s.cell[min(w0 + 31, n_alive - 1)];
+        EPP_CHECK(c_first >= 0 && c_last >= c_first && c_last < A.dom.n_cells, 34, c_last);
+        const int rid0 = c_first / n0;
+        const bool tiled = rid0 == c_last / n0;
+        const int c = A.s.cell[min(i, n_alive - 1)];
+        const int rid = c / n0, cx = c - rid * n0;
+        const float4 xi = on ? A.s.xh[i] : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        const int ti = on ? tag_of(A.s.tagm[i]) : 0;
+        const bool valid = on && ti >= 1 && ti <= A.n_tags;
+        unsigned st = (on && !valid) ? EPP_STATUS_BAD_TAG : 0u;
+        const unsigned amask = valid ? A.adj[ti - 1] : 0u;
+        const TargetConst tc = target_const<2>(on ? xi.w : 1.0f);
+        const bool dflt = A.crit == EPP_CRITERION_DEFAULT;
+        RowWin win[3], u[3];
+        bool staged = tiled;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            win[r] = row_range(A, stencil_row2(A, rid, r), cx - 1, cx + 1);
+            u[r] = RowWin{0, 0};
+            if (tiled) {
+                u[r] = row_range(A, stencil_row2(A, rid0, r), c_first - rid0 * n0 - 1, c_last - rid0 * n0 + 1);
+                staged = staged && u[r].hi - u[r].lo <= 64;   // warp-uniform
+            }
+        }
+        unsigned long long allowed[3];
+        bool one_h[3];
+        float h0[3];
+        if (staged) stage_rows2<Act, Act::NC != 0>(A, act, S, u, amask, lane, st, allowed, one_h, h0);
+        ListWriter<2> L = list_writer<2>(M, min(i, n_alive - 1));
+        float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (valid) {
+            typename Act::Self me = act.self(i);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int len = win[r].hi - win[r].lo;
+                const int woff = win[r].lo - u[r].lo;   // the window's first slot in its staged row
+                const bool uniform = staged && one_h[r] && (dflt || h0[r] == xi.w);
+                for (int k0 = 0; k0 < len; k0 += 32) {   // windows beyond 32 candidates in chunks
+                    const int k1 = min(len, k0 + 32);
+                    unsigned word;
+                    if (staged) {
+                        word = window_bits(S.x, 64 * r + woff, k0, k1, xi, uniform, dflt ? A.dom.gap_square : tc.h2sq,
+                                           tc.h2sq, dflt, A.dom.gap_square);
+                        word &= (unsigned)(allowed[r] >> (woff + k0));
+                    } else {
+                        word = 0u;
+                        for (int k = k1 - 1; k >= k0; --k) {
+                            const int j = win[r].lo + k;
+                            word = (word << 1) | (accept<2>(A, i, xi, amask, tc.h2sq, j, A.s.xh[j], st) ? 1u : 0u);
+                        }
+                    }
+                    if (k1 - k0 < 32) word &= (1u << (k1 - k0)) - 1u;
+                    if (r == 1) {   // not its own neighbour
+                        const int ks = i - win[1].lo - k0;
+                        if (ks >= 0 && ks < 32) word &= ~(1u << ks);
+                    }
+                    while (word) {   // append and run the search action, in candidate order
+                        const int k = k0 + __ffs(word) - 1;
+                        word &= word - 1u;
+                        float4 xj;
+                        int e, tj;
+                        typename Act::Nb nb;
+                        if (staged) {
+                            const float4 xs = S.x[64 * r + woff + k];
+                            e = __float_as_int(xs.z);
+                            xj = make_float4(xs.x, xs.y, 0.0f, xs.w);
+                            tj = entry_tag(e);
+                            if (Act::NC != 0) nb = S.nb[64 * r + woff + k];
+                        } else {
+                            const int j = win[r].lo + k;
+                            xj = A.s.xh[j];
+                            tj = tag_of(A.s.tagm[j]);
+                            e = list_entry(j, tj);
+                            if (Act::NC != 0) nb = act.fetch(j, ti, tj);
+                        }
+                        L.put(cnt++, e);
+                        if (Act::NC != 0) {
+                            const float4 t = act.term(me, nb, ti, tj, xj, geometry<2>(xi, xj), tc);
+                            sum.x += t.x;
+                            sum.y += t.y;
+                        }
+                    }
+                }
+            }
+            L.flush(cnt);
+        }
+        if (on) {
+            if (!valid) act.end_idle(i, ti);
+            else act.end(i, ti, sum, cnt);
+        }
+        if (st) atomicOr(A.status, st);
+    }
+    count_pairs(pairs, cnt);
+}
+
+}  // namespace epp

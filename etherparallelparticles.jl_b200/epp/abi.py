@@ -6,8 +6,7 @@ the header cites the reference interface each entry point replaces.
 import ctypes as C
 
 EPP_ABI_VERSION = 4
-EPP_TUNING_LISTS = 64   # epp_set_tuning: family 0 with neighbour lists
-EPP_TUNING_MASKS = 65   # epp_set_tuning: family 0 with stencil-row masks (the 2D default)
+EPP_TUNING_LISTS = 64   # epp_set_tuning: family 0 with the lockstep list search + continuity pass (2D)
 EPP_MAX_TAGS = 16
 
 # epp_status

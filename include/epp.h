@@ -251,15 +251,14 @@ int32_t epp_integrals_wait(epp_ctx* ctx, int64_t ticket, epp_integrals* out);
 int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t* sorted_ids,
                        int32_t* n_cells);
 
-/* Parity access to the neighbours the default pair passes (family 0) read, as the search pass
- * recorded them at the last epp_search or epp_step (2D stencil-row masks, 3D or EPP_TUNING_LISTS
- * neighbour lists): counts[row] = nCount of the particle in caller row `row` (0 for particles not
- * alive), and ids[k * ld + row] for k < min(counts[row], max_nb) = the 1-based id of its k-th
- * neighbour in list order (stencil rows, then cell order, then id order inside a cell).  A
- * particle whose neighbours are not stored -- more than 32 candidates in a 2D stencil row, more
- * than 160 neighbours in a 3D list; its pair passes read its stencil instead -- has its ids left
- * as they were.  ids may be NULL.  Replaces reading the nCount / nIndex columns of the reference's
- * particle system after search! (NeighbourSearch.jl:166-227). */
+/* Parity access to the neighbour lists the default pair passes (family 0) read, as the search pass
+ * built them at the last epp_search or epp_step: counts[row] = nCount of the particle in caller row
+ * `row` (0 for particles not alive), and ids[k * ld + row] for k < min(counts[row], max_nb) = the
+ * 1-based id of its k-th neighbour in list order (stencil rows, then cell order, then id order
+ * inside a cell).  A particle with more neighbours than a list keeps (64 in 2D, 160 in 3D; its
+ * pair passes read its stencil instead) has its ids left as they were.  ids may be NULL.
+ * Replaces reading the nCount / nIndex columns of the reference's particle system after search!
+ * (NeighbourSearch.jl:166-227). */
 int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t ld, int32_t max_nb);
 
 /* Waits for the context stream; returns EPP_ERR_DEVICE_STATUS when a device check failed
@@ -296,13 +295,12 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
  * neighbour list that the momentum pass reuses; 1 = one warp per occupied cell with a compacted
  * pair queue; 2, 4, 8, 16 or 32 = that many lanes of a warp per particle.  Chosen by the
  * autotuner; results change only at the FP32 rounding level (neighbour sets are identical).
- * In 2D, family 0 keeps per-particle stencil-row masks (one 32-bit word per stencil row: which
- * candidates of the row are neighbours) in place of lists, and its search pass runs the search
- * action; in 3D it keeps neighbour lists.  EPP_TUNING_LISTS and EPP_TUNING_MASKS select family 0
- * with lists or masks (two words per row in 3D) in either dimension: the same neighbours in the
- * same order, sums equal to FP32 rounding. */
+ * In 2D, family 0's search pass tests each particle's own stencil-row windows (cells cx-1 .. cx+1
+ * of each stencil row, staged per warp in shared memory) and runs the search action (continuity
+ * and the density preview) in the same pass; EPP_TUNING_LISTS selects family 0 with the lockstep
+ * warp-tile search and a separate continuity pass instead (the 3D form): the same neighbour lists,
+ * sums equal to FP32 rounding. */
 #define EPP_TUNING_LISTS 64
-#define EPP_TUNING_MASKS 65
 int32_t epp_set_tuning(epp_ctx* ctx, int32_t lanes_per_particle);
 /* Threads per block of the family-0 search and list passes: 128 (default), 64 or 32.  Smaller
  * blocks spread a small system over more SMs; results do not change (the per-particle order is

@@ -1,12 +1,14 @@
-"""Stencil-row masks (the default family-0 pair passes in 2D, EPP_TUNING_MASKS in 3D) against the
-neighbour-list passes.
+"""The 2D window search (the default family-0 search pass in 2D) against the tiled list build
+(EPP_TUNING_LISTS).
 
-Both forms visit every particle's neighbours in the same order (stencil rows, then cell order,
-then id order inside a cell) with the same pair terms, so the neighbour counts and sets are
+Both build the same neighbour lists in the same order (stencil rows, then cell order, then id order
+inside a cell): the window search tests each particle's own stencil-row windows from cell rows
+staged in shared memory and runs the continuity action while it writes the list, the tiled build
+tests whole tiles and leaves continuity to a list pass.  Neighbour counts and stored lists are
 identical and every sum agrees to FP32 rounding (the compiler may contract a multiply and an add
 into one fused operation differently in the two kernels).  Checked after fused steps and per-call
-actions, on multi-tile grids, warps that cross cell-row ends and particles whose stencil rows hold
-more candidates than a row's words (read from their stencil)."""
+actions, on multi-tile grids, warps that cross cell-row ends and particles with more neighbours than
+a list keeps (read from their stencil)."""
 import numpy as np
 import pytest
 
@@ -21,9 +23,9 @@ FIELDS = ("PositionVec", "VelocityVec", "Density", "dDensity", "Pressure", "Volu
 
 
 def pair_of_contexts(case):
-    """(masks, lists) contexts of the same case."""
+    """(window search, tiled list build) contexts of the same case."""
     out = []
-    for tuning in (abi.EPP_TUNING_MASKS, abi.EPP_TUNING_LISTS):
+    for tuning in (0, abi.EPP_TUNING_LISTS):
         ns = NeighbourSystem(case.domain, casegen.DAM_BREAK_ACTIVE_PAIRS, max_neighbour_number=1)
         d = DeviceParticleSystem(case.ps, ns)
         d.ctx.set_tuning(tuning)
@@ -53,17 +55,14 @@ def assert_same(a, b, what):
         assert err <= 1e-5, (what, k, err, int(np.sum(x != y)))
 
 
-def case_of(dim, dx, h_factor):
-    if dim == 2:
-        return casegen.dam_break_2d(dx=dx, h_factor=h_factor, max_neighbour_number=1)
-    return casegen.dam_break_3d(dx=dx, tank=(0.6, 0.3, 0.4), column=(0.2, 0.3, 0.24), h_factor=h_factor,
-                                max_neighbour_number=1)
+def case_of(dx, h_factor):
+    return casegen.dam_break_2d(dx=dx, h_factor=h_factor, max_neighbour_number=1)
 
 
-@pytest.mark.parametrize("dim,dx,h_factor,steps", [(2, 0.04, 1.5, 20), (2, 0.02, 1.5, 10), (2, 0.04, 3.0, 4),
-                                                   (3, 0.02, 1.3, 8), (3, 0.01, 1.3, 3), (3, 0.02, 2.0, 3)])
-def test_fused_steps_match(dim, dx, h_factor, steps):
-    case = case_of(dim, dx, h_factor)
+@pytest.mark.parametrize("dx,h_factor,steps", [(0.04, 1.5, 20), (0.02, 1.5, 10), (0.005, 1.5, 3),
+                                               (0.04, 3.0, 4), (0.02, 2.2, 3)])
+def test_fused_steps_match(dx, h_factor, steps):
+    case = case_of(dx, h_factor)
     phys = case.physics
     m, l = pair_of_contexts(case)
     for d in (m, l):
@@ -73,23 +72,23 @@ def test_fused_steps_match(dim, dx, h_factor, steps):
     a, b = host_fields(m), host_fields(l)
     assert_same(a, b, "fused steps")
     n = case.n
-    ca, ia = m.ctx.neighbour_lists(n, 160)
-    cb, ib = l.ctx.neighbour_lists(n, 160)
+    ca, ia = m.ctx.neighbour_lists(n, 64)
+    cb, ib = l.ctx.neighbour_lists(n, 64)
     assert np.array_equal(ca, cb)
-    stored = ia[:, 0] != 0
-    if h_factor >= 2:   # stencil rows beyond a row's words: read from the stencil, not stored
-        assert stored.sum() < n
-    keep = stored & (ib[:, 0] != 0)
-    assert np.array_equal(ia[keep], ib[keep])
+    stored = (ca > 0) & (ca <= 64)
+    if h_factor >= 3:   # more neighbours than a list keeps: read from the stencil, not stored
+        assert stored.sum() < n and np.all(ia[ca > 64] == 0) and np.all(ib[cb > 64] == 0)
+    assert np.all(ia[stored, 0] != 0)
+    assert np.array_equal(ia[stored], ib[stored])
     for d in (m, l):
         d.close()
 
 
-@pytest.mark.parametrize("dim", [2, 3])
-def test_per_call_actions_match(dim):
+@pytest.mark.parametrize("h_factor", [1.5, 3.0])
+def test_per_call_actions_match(h_factor):
     """search! (count only and continuity), interaction! (momentum, neighbour count, kernel filter,
     pressure extrapolation) and selfaction! on both forms."""
-    case = case_of(dim, 0.04 if dim == 2 else 0.02, 1.5 if dim == 2 else 1.3)
+    case = case_of(0.04, h_factor)
     phys = case.physics
     m, l = pair_of_contexts(case)
     for d in (m, l):
