@@ -98,31 +98,33 @@ __device__ __forceinline__ void stage_rows2(const PairArgs& A, const Act& act, S
 // exact bound `r2u` serves; otherwise the bound is looked up per candidate.
 __device__ __forceinline__ unsigned window_bits(const float4* sx, int off, int k0, int k1, float4 xi, bool uniform,
                                                 float r2u, float h2sq, bool dflt, float gap_square) {
+    // (dx, dy) and (dx^2, dy^2) on the packed f32x2 pipe (each half rounds like __fsub_rn /
+    // __fmul_rn), the sum scalar
+    const f32x2 XY = f2_pack(xi.x, xi.y);
     unsigned word = 0u;
     if (uniform) {
         // dr2 <= R2 as integers: non-negative floats order like their bit patterns, so
         // bits(dr2) - bits(R2) - 1 is negative exactly for the accepted candidates
         const int nR2 = -__float_as_int(r2u) - 1;
         for (int k = k1 - 1; k >= k0; --k) {
-            const float4 xj = sx[off + k];
-            const float dx = __fsub_rn(xi.x, xj.x);
-            const float dy = __fsub_rn(xi.y, xj.y);
-            const float d = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-            word = (word << 1) | ((unsigned)(__float_as_int(d) + nR2) >> 31);
+            const f32x2 d = f2_sub(XY, *reinterpret_cast<const f32x2*>(&sx[off + k]));
+            float dx2, dy2;
+            f2_unpack(f2_mul(d, d), dx2, dy2);
+            word = (word << 1) | ((unsigned)(__float_as_int(__fadd_rn(dx2, dy2)) + nR2) >> 31);
         }
         return word;
     }
     float hc = xi.w, rc = dflt ? gap_square : h2sq;
     for (int k = k1 - 1; k >= k0; --k) {
-        const float4 xj = sx[off + k];
-        const float dx = __fsub_rn(xi.x, xj.x);
-        const float dy = __fsub_rn(xi.y, xj.y);
-        const float d = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-        if (xj.w != hc) {
-            hc = xj.w;
+        const float hj = sx[off + k].w;
+        const f32x2 d = f2_sub(XY, *reinterpret_cast<const f32x2*>(&sx[off + k]));
+        float dx2, dy2;
+        f2_unpack(f2_mul(d, d), dx2, dy2);
+        if (hj != hc) {
+            hc = hj;
             rc = dflt ? gap_square : (hc == xi.w ? h2sq : pair_r2(xi.w, hc));
         }
-        word = (word << 1) | (d <= rc ? 1u : 0u);
+        word = (word << 1) | (__fadd_rn(dx2, dy2) <= rc ? 1u : 0u);
     }
     return word;
 }
@@ -175,14 +177,77 @@ __global__ void __launch_bounds__(128) k_win_build(const __grid_constant__ PairA
         if (staged) stage_rows2<Act, Act::NC != 0>(A, act, S, u, amask, lane, st, allowed, one_h, h0);
         ListWriter<2> L = list_writer<2>(M, min(i, n_alive - 1));
         float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (valid) {
-            typename Act::Self me = act.self(i);
+        const bool fits = win[0].hi - win[0].lo <= 32 && win[1].hi - win[1].lo <= 32 && win[2].hi - win[2].lo <= 32;
+        if (valid && fits) {
+            // every window in one word: the three words first, then one walk over all of them,
+            // so a warp iterates as often as its busiest lane's neighbour count (not the sum over
+            // rows of each row's busiest lane)
+            unsigned w[3];
+            int off[3];
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
                 const int len = win[r].hi - win[r].lo;
                 const int woff = win[r].lo - u[r].lo;   // the window's first slot in its staged row
+                off[r] = staged ? 64 * r + woff : win[r].lo;
+                unsigned word = 0u;
+                if (len > 0) {
+                    if (staged) {
+                        const bool uniform = one_h[r] && (dflt || h0[r] == xi.w);
+                        word = window_bits(S.x, off[r], 0, len, xi, uniform, dflt ? A.dom.gap_square : tc.h2sq,
+                                           tc.h2sq, dflt, A.dom.gap_square);
+                        word &= (unsigned)(allowed[r] >> woff);
+                    } else {
+                        for (int k = len - 1; k >= 0; --k) {
+                            const int j = win[r].lo + k;
+                            word = (word << 1) | (accept<2>(A, i, xi, amask, tc.h2sq, j, A.s.xh[j], st) ? 1u : 0u);
+                        }
+                    }
+                    if (len < 32) word &= (1u << len) - 1u;
+                }
+                if (r == 1) word &= ~(1u << (i - win[1].lo));   // not its own neighbour
+                w[r] = word;
+            }
+            typename Act::Self me = act.self(i);
+            unsigned a = w[0], b = w[1], c2 = w[2];
+            while (a | b | c2) {   // append and run the search action, in list order
+                const int r = a ? 0 : (b ? 1 : 2);
+                const unsigned cur = a ? a : (b ? b : c2);
+                const int slot = (r == 0 ? off[0] : (r == 1 ? off[1] : off[2])) + __ffs(cur) - 1;
+                const unsigned rest = cur & (cur - 1u);
+                if (r == 0) a = rest;
+                else if (r == 1) b = rest;
+                else c2 = rest;
+                float4 xj;
+                int e, tj;
+                typename Act::Nb nb;
+                if (staged) {
+                    const float4 xs = S.x[slot];
+                    e = __float_as_int(xs.z);
+                    xj = make_float4(xs.x, xs.y, 0.0f, xs.w);
+                    tj = entry_tag(e);
+                    if (Act::NC != 0) nb = S.nb[slot];
+                } else {
+                    xj = A.s.xh[slot];
+                    tj = tag_of(A.s.tagm[slot]);
+                    e = list_entry(slot, tj);
+                    if (Act::NC != 0) nb = act.fetch(slot, ti, tj);
+                }
+                L.put(cnt++, e);
+                if (Act::NC != 0) {
+                    const float4 t = act.term(me, nb, ti, tj, xj, geometry<2>(xi, xj), tc);
+                    sum.x += t.x;
+                    sum.y += t.y;
+                }
+            }
+            L.flush(cnt);
+        } else if (valid) {   // a window beyond 32 candidates (dense neighbourhoods): row by row in chunks
+            typename Act::Self me = act.self(i);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int len = win[r].hi - win[r].lo;
+                const int woff = win[r].lo - u[r].lo;
                 const bool uniform = staged && one_h[r] && (dflt || h0[r] == xi.w);
-                for (int k0 = 0; k0 < len; k0 += 32) {   // windows beyond 32 candidates in chunks
+                for (int k0 = 0; k0 < len; k0 += 32) {
                     const int k1 = min(len, k0 + 32);
                     unsigned word;
                     if (staged) {
@@ -201,7 +266,7 @@ __global__ void __launch_bounds__(128) k_win_build(const __grid_constant__ PairA
                         const int ks = i - win[1].lo - k0;
                         if (ks >= 0 && ks < 32) word &= ~(1u << ks);
                     }
-                    while (word) {   // append and run the search action, in candidate order
+                    while (word) {
                         const int k = k0 + __ffs(word) - 1;
                         word &= word - 1u;
                         float4 xj;
