@@ -63,8 +63,8 @@ template <int D, bool GEN>
 __device__ __forceinline__ float pair_dwr(int kernel, float q, float hinv, float kdw) {
     if (!GEN || kernel == EPP_KERNEL_WENDLAND_C2) {
         if (!(q < 2.0f)) return 0.0f;   // W = dW = 0 at q >= 2 (WendlandC2.jl:23,44)
-        const float u = 2.0f - q;
-        return kdw * (u * u * u);
+        const float u = __fsub_rn(2.0f, q);
+        return __fmul_rn(kdw, __fmul_rn(__fmul_rn(u, u), u));
     }
     return kern_dwr<D>(kernel, q, hinv);
 }
@@ -144,16 +144,18 @@ struct CPCont {
         const bool fw = ti == P.fluid && tj == P.wall;
         const bool wf = ti == P.wall && tj == P.fluid;
         if (!(ff || fw || wf)) return out;
+        // every operation rounded on its own (no contraction into fused multiply-adds), so the term
+        // is the same bit for bit wherever a pass evaluates it
         const float r = sqrtf(g.dr2);
         float hinv, kdw, hh;
         pair_consts<D>(tc, xj.w, hinv, kdw, hh);
-        const float dwr = pair_dwr<D, GEN>(P.kernel, r * hinv, hinv, kdw);
+        const float dwr = pair_dwr<D, GEN>(P.kernel, __fmul_rn(r, hinv), hinv, kdw);
         if (dwr == 0.0f) return out;
-        float vdx = g.dx * (me.v.x - nb.v.x);
-        vdx += g.dy * (me.v.y - nb.v.y);
-        if (D == 3) vdx += g.dz * (me.v.z - nb.v.z);
-        if (ff) out.x = nb.v.w * vdx * dwr;                     // iClassicContinuity!
-        else out.x = me.rho * vol_of(nb) * vdx * dwr;           // iBalancedContinuity!
+        float vdx = __fmul_rn(g.dx, __fsub_rn(me.v.x, nb.v.x));
+        vdx = __fadd_rn(vdx, __fmul_rn(g.dy, __fsub_rn(me.v.y, nb.v.y)));
+        if (D == 3) vdx = __fadd_rn(vdx, __fmul_rn(g.dz, __fsub_rn(me.v.z, nb.v.z)));
+        if (ff) out.x = __fmul_rn(__fmul_rn(nb.v.w, vdx), dwr);                              // iClassicContinuity!
+        else out.x = __fmul_rn(__fmul_rn(__fmul_rn(me.rho, vol_of(nb)), vdx), dwr);         // iBalancedContinuity!
         return out;
     }
     __device__ __forceinline__ float4 contrib(int i, int j, int ti, int tj, float4 xi, float4 xj,

@@ -17,8 +17,8 @@
 // list (the lists the momentum, filter and extrapolation passes read; same layout and order as
 // k_build's: stencil rows, then cell order, then id order inside a cell) and adds the search
 // action's term -- the continuity rate -- from the staged record, so no separate continuity pass
-// walks the neighbours again.  Warps that cross a cell-row end, and union rows longer than 64,
-// read the candidates from global memory instead.
+// walks the neighbours again.  A warp that crosses a cell-row end takes one such round per cell
+// row of its particles; union rows longer than 64 are read from global memory instead.
 #pragma once
 #include "epp_tile.cuh"
 
@@ -129,12 +129,95 @@ __device__ __forceinline__ unsigned window_bits(const float4* sx, int off, int k
     return word;
 }
 
+// What the general per-lane search hands back to the search pass.
+struct WinOut {
+    int cnt;
+    float sx, sy;
+    unsigned st;
+};
+
+// The per-lane search of the 2D search pass in its general form: windows of any length, row by
+// row 32 candidates at a time, from the staged union rows u[] or, when `staged` is false, from
+// global memory.  Only dense neighbourhoods (a window beyond 32 candidates) and union rows beyond
+// the staging area come here, so it stays out of line and leaves the common path its registers.
+// uniform_rows: bit r set when every candidate of staged row r has the lane's h (or the default
+// criterion), so one exact bound serves the row.
+template <class Act>
+__device__ __noinline__ WinOut win_lane_general(const PairArgs& A, const TileMask& M, const Act& act,
+                                                const Stage2<Act>& S, bool staged, RowWin u0, RowWin u1, RowWin u2,
+                                                unsigned long long al0, unsigned long long al1, unsigned long long al2,
+                                                unsigned uniform_rows, int i, int ti, float4 xi, unsigned amask,
+                                                int rid, int cx) {
+    const TargetConst tc = target_const<2>(xi.w);
+    const bool dflt = A.crit == EPP_CRITERION_DEFAULT;
+    typename Act::Self me = act.self(i);
+    ListWriter<2> L = list_writer<2>(M, i);
+    WinOut o{0, 0.0f, 0.0f, 0u};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const RowWin win = row_range(A, stencil_row2(A, rid, r), cx - 1, cx + 1);
+        const RowWin u = r == 0 ? u0 : (r == 1 ? u1 : u2);
+        const unsigned long long allowed = r == 0 ? al0 : (r == 1 ? al1 : al2);
+        const int len = win.hi - win.lo;
+        const int woff = win.lo - u.lo;
+        const bool uniform = staged && ((uniform_rows >> r) & 1u);
+        for (int k0 = 0; k0 < len; k0 += 32) {
+            const int k1 = min(len, k0 + 32);
+            unsigned word;
+            if (staged) {
+                word = window_bits(S.x, 64 * r + woff, k0, k1, xi, uniform, dflt ? A.dom.gap_square : tc.h2sq,
+                                   tc.h2sq, dflt, A.dom.gap_square);
+                word &= (unsigned)(allowed >> (woff + k0));
+            } else {
+                word = 0u;
+                for (int k = k1 - 1; k >= k0; --k) {
+                    const int j = win.lo + k;
+                    word = (word << 1) | (accept<2>(A, i, xi, amask, tc.h2sq, j, A.s.xh[j], o.st) ? 1u : 0u);
+                }
+            }
+            if (k1 - k0 < 32) word &= (1u << (k1 - k0)) - 1u;
+            if (r == 1) {   // not its own neighbour
+                const int ks = i - win.lo - k0;
+                if (ks >= 0 && ks < 32) word &= ~(1u << ks);
+            }
+            while (word) {   // append and run the search action, in list order
+                const int k = k0 + __ffs(word) - 1;
+                word &= word - 1u;
+                float4 xj;
+                int e, tj;
+                typename Act::Nb nb;
+                if (staged) {
+                    const float4 xs = S.x[64 * r + woff + k];
+                    e = __float_as_int(xs.z);
+                    xj = make_float4(xs.x, xs.y, 0.0f, xs.w);
+                    tj = entry_tag(e);
+                    if (Act::NC != 0) nb = S.nb[64 * r + woff + k];
+                } else {
+                    const int j = win.lo + k;
+                    xj = A.s.xh[j];
+                    tj = tag_of(A.s.tagm[j]);
+                    e = list_entry(j, tj);
+                    if (Act::NC != 0) nb = act.fetch(j, ti, tj);
+                }
+                L.put(o.cnt++, e);
+                if (Act::NC != 0) {
+                    const float4 t = act.term(me, nb, ti, tj, xj, geometry<2>(xi, xj), tc);
+                    o.sx = __fadd_rn(o.sx, t.x);
+                    o.sy = __fadd_rn(o.sy, t.y);
+                }
+            }
+        }
+    }
+    L.flush(o.cnt);
+    return o;
+}
+
 // The 2D search pass: neighbour lists and nCount, and the search action of `Act` over the accepted
 // neighbours in list order (CPCont: continuity + density preview; CPCount: the count only).  A
 // particle with more neighbours than a list keeps has only those stored (the pair passes read its
 // stencil); its search action still covers all of them.
 template <class Act>
-__global__ void __launch_bounds__(128) k_win_build(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M,
+__global__ void __launch_bounds__(128, 6) k_win_build(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M,
                                                    const __grid_constant__ Act act, unsigned long long* pairs) {
     __shared__ Stage2<Act> stage[4];
     const int lane = threadIdx.x & 31;
@@ -146,68 +229,80 @@ __global__ void __launch_bounds__(128) k_win_build(const __grid_constant__ PairA
     if (w0 < n_alive) {   // warp-uniform
         const bool on = i < n_alive;
         const int n0 = A.dom.n[0];
-        const int c_first = A.s.cell[w0];
-        const int c_last = A.s.cell[min(w0 + 31, n_alive - 1)];
-        EPP_CHECK(c_first >= 0 && c_last >= c_first && c_last < A.dom.n_cells, 34, c_last);
-        const int rid0 = c_first / n0;
-        const bool tiled = rid0 == c_last / n0;
         const int c = A.s.cell[min(i, n_alive - 1)];
+        EPP_CHECK(!__any_sync(0xffffffffu, c < 0 || c >= A.dom.n_cells), 34, c);
         const int rid = c / n0, cx = c - rid * n0;
         const float4 xi = on ? A.s.xh[i] : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         const int ti = on ? tag_of(A.s.tagm[i]) : 0;
         const bool valid = on && ti >= 1 && ti <= A.n_tags;
         unsigned st = (on && !valid) ? EPP_STATUS_BAD_TAG : 0u;
         const unsigned amask = valid ? A.adj[ti - 1] : 0u;
-        const TargetConst tc = target_const<2>(on ? xi.w : 1.0f);
-        const bool dflt = A.crit == EPP_CRITERION_DEFAULT;
-        RowWin win[3], u[3];
-        bool staged = tiled;
+        float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        // One round per cell row among the warp's particles (cell order keeps each row's lanes
+        // contiguous): a warp inside one cell row -- all but about 2% -- takes one round; a warp
+        // that crosses a row end stages the union rows of each part in turn instead of reading
+        // candidates from global memory one dependent load at a time.
+        unsigned pending = __ballot_sync(0xffffffffu, on);
+        while (pending) {   // warp-uniform
+            const int lead = __ffs(pending) - 1;
+            const int rid_g = __shfl_sync(0xffffffffu, rid, lead);
+            const bool mine = ((pending >> lane) & 1u) && rid == rid_g;
+            const unsigned members = __ballot_sync(0xffffffffu, mine);
+            const int xa = __shfl_sync(0xffffffffu, cx, lead) - 1;
+            const int xb = __shfl_sync(0xffffffffu, cx, 31 - __clz(members)) + 1;
+            pending &= ~members;
+            RowWin u[3];
+            bool staged = true;
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            win[r] = row_range(A, stencil_row2(A, rid, r), cx - 1, cx + 1);
-            u[r] = RowWin{0, 0};
-            if (tiled) {
-                u[r] = row_range(A, stencil_row2(A, rid0, r), c_first - rid0 * n0 - 1, c_last - rid0 * n0 + 1);
+            for (int r = 0; r < 3; ++r) {
+                u[r] = row_range(A, stencil_row2(A, rid_g, r), xa, xb);
                 staged = staged && u[r].hi - u[r].lo <= 64;   // warp-uniform
             }
-        }
-        unsigned long long allowed[3];
-        bool one_h[3];
-        float h0[3];
-        if (staged) stage_rows2<Act, Act::NC != 0>(A, act, S, u, amask, lane, st, allowed, one_h, h0);
-        ListWriter<2> L = list_writer<2>(M, min(i, n_alive - 1));
-        float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        const bool fits = win[0].hi - win[0].lo <= 32 && win[1].hi - win[1].lo <= 32 && win[2].hi - win[2].lo <= 32;
-        if (valid && fits) {
-            // every window in one word: the three words first, then one walk over all of them,
-            // so a warp iterates as often as its busiest lane's neighbour count (not the sum over
-            // rows of each row's busiest lane)
+            unsigned long long allowed[3] = {0ull, 0ull, 0ull};
+            bool one_h[3] = {false, false, false};
+            float h0[3] = {0.0f, 0.0f, 0.0f};
+            if (staged) stage_rows2<Act, Act::NC != 0>(A, act, S, u, amask, lane, st, allowed, one_h, h0);
+            if (!(mine && valid)) continue;
+            const bool dflt = A.crit == EPP_CRITERION_DEFAULT;
+            RowWin win[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) win[r] = row_range(A, stencil_row2(A, rid, r), cx - 1, cx + 1);
+            unsigned uniform_rows = 0u;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                if (one_h[r] && (dflt || h0[r] == xi.w)) uniform_rows |= 1u << r;
+            if (!staged || win[0].hi - win[0].lo > 32 || win[1].hi - win[1].lo > 32 || win[2].hi - win[2].lo > 32) {
+                const WinOut o = win_lane_general<Act>(A, M, act, S, staged, u[0], u[1], u[2], allowed[0], allowed[1],
+                                                       allowed[2], uniform_rows, i, ti, xi, amask, rid, cx);
+                cnt = o.cnt;
+                sum.x = o.sx;
+                sum.y = o.sy;
+                st |= o.st;
+                continue;
+            }
+            // every window in one word: the three words first, then one walk over all of them, so
+            // a warp iterates as often as its busiest lane's neighbour count (not the sum over rows
+            // of each row's busiest lane)
+            const TargetConst tc = target_const<2>(xi.w);
             unsigned w[3];
             int off[3];
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
                 const int len = win[r].hi - win[r].lo;
                 const int woff = win[r].lo - u[r].lo;   // the window's first slot in its staged row
-                off[r] = staged ? 64 * r + woff : win[r].lo;
+                off[r] = 64 * r + woff;
                 unsigned word = 0u;
                 if (len > 0) {
-                    if (staged) {
-                        const bool uniform = one_h[r] && (dflt || h0[r] == xi.w);
-                        word = window_bits(S.x, off[r], 0, len, xi, uniform, dflt ? A.dom.gap_square : tc.h2sq,
-                                           tc.h2sq, dflt, A.dom.gap_square);
-                        word &= (unsigned)(allowed[r] >> woff);
-                    } else {
-                        for (int k = len - 1; k >= 0; --k) {
-                            const int j = win[r].lo + k;
-                            word = (word << 1) | (accept<2>(A, i, xi, amask, tc.h2sq, j, A.s.xh[j], st) ? 1u : 0u);
-                        }
-                    }
+                    word = window_bits(S.x, off[r], 0, len, xi, (uniform_rows >> r) & 1u,
+                                       dflt ? A.dom.gap_square : tc.h2sq, tc.h2sq, dflt, A.dom.gap_square);
+                    word &= (unsigned)(allowed[r] >> woff);
                     if (len < 32) word &= (1u << len) - 1u;
                 }
                 if (r == 1) word &= ~(1u << (i - win[1].lo));   // not its own neighbour
                 w[r] = word;
             }
             typename Act::Self me = act.self(i);
+            ListWriter<2> L = list_writer<2>(M, i);
             unsigned a = w[0], b = w[1], c2 = w[2];
             while (a | b | c2) {   // append and run the search action, in list order
                 const int r = a ? 0 : (b ? 1 : 2);
@@ -217,81 +312,15 @@ __global__ void __launch_bounds__(128) k_win_build(const __grid_constant__ PairA
                 if (r == 0) a = rest;
                 else if (r == 1) b = rest;
                 else c2 = rest;
-                float4 xj;
-                int e, tj;
-                typename Act::Nb nb;
-                if (staged) {
-                    const float4 xs = S.x[slot];
-                    e = __float_as_int(xs.z);
-                    xj = make_float4(xs.x, xs.y, 0.0f, xs.w);
-                    tj = entry_tag(e);
-                    if (Act::NC != 0) nb = S.nb[slot];
-                } else {
-                    xj = A.s.xh[slot];
-                    tj = tag_of(A.s.tagm[slot]);
-                    e = list_entry(slot, tj);
-                    if (Act::NC != 0) nb = act.fetch(slot, ti, tj);
-                }
+                const float4 xs = S.x[slot];
+                const int e = __float_as_int(xs.z);
                 L.put(cnt++, e);
                 if (Act::NC != 0) {
-                    const float4 t = act.term(me, nb, ti, tj, xj, geometry<2>(xi, xj), tc);
-                    sum.x += t.x;
-                    sum.y += t.y;
-                }
-            }
-            L.flush(cnt);
-        } else if (valid) {   // a window beyond 32 candidates (dense neighbourhoods): row by row in chunks
-            typename Act::Self me = act.self(i);
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                const int len = win[r].hi - win[r].lo;
-                const int woff = win[r].lo - u[r].lo;
-                const bool uniform = staged && one_h[r] && (dflt || h0[r] == xi.w);
-                for (int k0 = 0; k0 < len; k0 += 32) {
-                    const int k1 = min(len, k0 + 32);
-                    unsigned word;
-                    if (staged) {
-                        word = window_bits(S.x, 64 * r + woff, k0, k1, xi, uniform, dflt ? A.dom.gap_square : tc.h2sq,
-                                           tc.h2sq, dflt, A.dom.gap_square);
-                        word &= (unsigned)(allowed[r] >> (woff + k0));
-                    } else {
-                        word = 0u;
-                        for (int k = k1 - 1; k >= k0; --k) {
-                            const int j = win[r].lo + k;
-                            word = (word << 1) | (accept<2>(A, i, xi, amask, tc.h2sq, j, A.s.xh[j], st) ? 1u : 0u);
-                        }
-                    }
-                    if (k1 - k0 < 32) word &= (1u << (k1 - k0)) - 1u;
-                    if (r == 1) {   // not its own neighbour
-                        const int ks = i - win[1].lo - k0;
-                        if (ks >= 0 && ks < 32) word &= ~(1u << ks);
-                    }
-                    while (word) {
-                        const int k = k0 + __ffs(word) - 1;
-                        word &= word - 1u;
-                        float4 xj;
-                        int e, tj;
-                        typename Act::Nb nb;
-                        if (staged) {
-                            const float4 xs = S.x[64 * r + woff + k];
-                            e = __float_as_int(xs.z);
-                            xj = make_float4(xs.x, xs.y, 0.0f, xs.w);
-                            tj = entry_tag(e);
-                            if (Act::NC != 0) nb = S.nb[64 * r + woff + k];
-                        } else {
-                            const int j = win[r].lo + k;
-                            xj = A.s.xh[j];
-                            tj = tag_of(A.s.tagm[j]);
-                            e = list_entry(j, tj);
-                            if (Act::NC != 0) nb = act.fetch(j, ti, tj);
-                        }
-                        L.put(cnt++, e);
-                        if (Act::NC != 0) {
-                            const float4 t = act.term(me, nb, ti, tj, xj, geometry<2>(xi, xj), tc);
-                            sum.x += t.x;
-                            sum.y += t.y;
-                        }
-                    }
+                    const int tj = entry_tag(e);
+                    const float4 xj = make_float4(xs.x, xs.y, 0.0f, xs.w);
+                    const float4 t = act.term(me, S.nb[slot], ti, tj, xj, geometry<2>(xi, xj), tc);
+                    sum.x = __fadd_rn(sum.x, t.x);
+                    sum.y = __fadd_rn(sum.y, t.y);
                 }
             }
             L.flush(cnt);
