@@ -1,6 +1,6 @@
 """Checkpoint / resume with the raw writer's datasets (raw/int_properties, raw/float_properties,
-appendix/*): an exact round trip of the alive rows on the host, and (GPU) a run resumed from a
-checkpoint staying with the uninterrupted run."""
+appendix/*) in its JLD2 files (and the .npz alternative): an exact round trip of the alive rows on
+the host, and (GPU) a run resumed from a checkpoint staying with the uninterrupted run."""
 import numpy as np
 import pytest
 
@@ -9,13 +9,14 @@ from epp.algorithm import DeviceParticleSystem
 from epp.classes import NeighbourSystem
 
 
-def test_round_trip_alive_rows(tmp_path):
+@pytest.mark.parametrize("suffix", [".jld2", ".npz"])
+def test_round_trip_alive_rows(tmp_path, suffix):
     case = casegen.dam_break_2d(dx=0.04, max_neighbour_number=8)
     ps = case.ps
     ps["Density"] = np.linspace(990, 1010, ps.n_particles).astype(np.float32)
     ps.is_alive[[3, 10]] = 0
-    path = checkpoint.file_name(str(tmp_path), 7)
-    assert path.endswith("result_0007.npz")
+    path = checkpoint.file_name(str(tmp_path), 7, suffix=suffix)
+    assert path.endswith("result_0007" + suffix)
     checkpoint.save(ps, path, checkpoint.appendix(step=7, time_value=0.25, write_step=2))
     fresh = casegen.dam_break_2d(dx=0.04, max_neighbour_number=8).ps
     app = checkpoint.load(fresh, path)
@@ -30,7 +31,7 @@ def test_round_trip_alive_rows(tmp_path):
 
 def test_load_rejects_other_layout(tmp_path):
     a = casegen.dam_break_2d(dx=0.04, max_neighbour_number=8)
-    path = checkpoint.save(a.ps, str(tmp_path / "c.npz"))
+    path = checkpoint.save(a.ps, str(tmp_path / "c.jld2"))
     b = casegen.dam_break_2d(dx=0.04, max_neighbour_number=40)
     with pytest.raises(ValueError):
         checkpoint.load(b.ps, path)
@@ -52,7 +53,7 @@ def test_resume_follows_uninterrupted_run(tmp_path):
     da = system(a)
     da.ctx.step(10, phys)
     da.asyncto()
-    path = checkpoint.save(a.ps, str(tmp_path / "result_0010.npz"), checkpoint.appendix(step=10))
+    path = checkpoint.save(a.ps, checkpoint.file_name(str(tmp_path), 10), checkpoint.appendix(step=10))
     da.ctx.step(10, phys)
     da.asyncto()
     b = casegen.dam_break_2d(dx=0.04, max_neighbour_number=1)
