@@ -17,6 +17,7 @@ neighbour lists, bucket cell list, one pass per reference launch) on the host co
 import argparse
 import json
 import os
+import re
 import statistics
 import sys
 import threading
@@ -52,6 +53,14 @@ KERNEL_OF_STAGE = {"momentum_integrate_bin": "k_list<CPMom> (momentum + integrat
                    "rank_gather": "k_rank_gather (rank by id + state gather + density update)",
                    "search": "k_build (neighbour lists + nCount)",
                    "continuity": "k_list<CPCont> (continuity + density preview, fused)"}
+
+
+def kernel_key(name):
+    """(kernel, first type argument) of a kernel label or an ncu kernel name:
+    "k_list<CPMom> (...)" and "k_list<2, CPMom<2, 1, 0>, 1>" both give ("k_list", "CPMom")."""
+    head = name.split(" (")[0]
+    m = re.search(r"[<,]\s*([A-Za-z_]\w*)", head)
+    return head.split("<")[0], m.group(1) if m else None
 
 
 def parse():
@@ -683,6 +692,7 @@ def main():
         b_alg["continuity"][dim] = 0.0
         if windows:
             kernel_of["search"] = "k_win_build<CPCont> (window search + lists + continuity + density preview)"
+            kernel_of["continuity"] = "(none: the continuity action runs inside the window search)"
     # roofline of the dominant kernel: the longest of the step's kernels
     dom_stage = max(STAGES, key=lambda k: stage[STAGES.index(k)])
     dom_ms = float(stage[STAGES.index(dom_stage)])
@@ -699,10 +709,9 @@ def main():
     tr_case = {}
     try:   # DRAM bytes of one launch of that kernel from an ncu capture of the same workload
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            base = lambda name: name.split(" ")[0].split("<")[0]  # noqa: E731
-            # only captures of the kernels this run launches
+            # only captures of the kernels this run launches (same kernel, same pair action)
             tr_case = {k: v for k, v in json.load(f).get(args.case, {}).items()
-                       if k in kernel_of and base(v.get("kernel", "")) == base(kernel_of[k])}
+                       if k in kernel_of and kernel_key(v.get("kernel", "")) == kernel_key(kernel_of[k])}
             if tr_case.get(dom_stage):
                 traffic = tr_case[dom_stage]["bytes_per_launch"]
     except Exception:
