@@ -139,11 +139,12 @@ struct WinOut {
 // The per-lane search of the 2D search pass in its general form: windows of any length, row by
 // row 32 candidates at a time, from the staged union rows u[] or, when `staged` is false, from
 // global memory.  Only dense neighbourhoods (a window beyond 32 candidates) and union rows beyond
-// the staging area come here, so it stays out of line and leaves the common path its registers.
+// the staging area come here.  Inlined: as an out-of-line call it cost the kernel registers (the
+// values live across the call) and 13% of its time.
 // uniform_rows: bit r set when every candidate of staged row r has the lane's h (or the default
 // criterion), so one exact bound serves the row.
 template <class Act>
-__device__ __noinline__ WinOut win_lane_general(const PairArgs& A, const TileMask& M, const Act& act,
+__device__ __forceinline__ WinOut win_lane_general(const PairArgs& A, const TileMask& M, const Act& act,
                                                 const Stage2<Act>& S, bool staged, RowWin u0, RowWin u1, RowWin u2,
                                                 unsigned long long al0, unsigned long long al1, unsigned long long al2,
                                                 unsigned uniform_rows, int i, int ti, float4 xi, unsigned amask,
@@ -217,7 +218,7 @@ __device__ __noinline__ WinOut win_lane_general(const PairArgs& A, const TileMas
 // particle with more neighbours than a list keeps has only those stored (the pair passes read its
 // stencil); its search action still covers all of them.
 template <class Act>
-__global__ void __launch_bounds__(128, 6) k_win_build(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M,
+__global__ void __launch_bounds__(128, 7) k_win_build(const __grid_constant__ PairArgs A, const __grid_constant__ TileMask M,
                                                    const __grid_constant__ Act act, unsigned long long* pairs) {
     __shared__ Stage2<Act> stage[4];
     const int lane = threadIdx.x & 31;
