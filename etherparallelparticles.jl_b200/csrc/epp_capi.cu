@@ -95,7 +95,7 @@ struct epp_ctx {
     unsigned long long* scan_state = nullptr;
     unsigned* status = nullptr;
     unsigned long long* pairs = nullptr;
-    int* ncount = nullptr;
+    int* ncnt[2] = {nullptr, nullptr};   // nCount of each state set (what the last search of that set found)
     float* stage_f = nullptr;
     int* stage_i = nullptr;
     double* ipartial = nullptr;
@@ -163,6 +163,13 @@ struct epp_ctx {
     long long islot_ticket[EPP_INTEGRALS_SLOTS]{-1, -1, -1, -1};
     float islot_c0[EPP_INTEGRALS_SLOTS]{};
     float islot_cfl[EPP_INTEGRALS_SLOTS]{};
+    // ... which run on a second stream beside the next epp_step: they read only the state set they
+    // were asked for (positions, velocities, density, tags, its nCount and cell offsets), which the
+    // next step reads but does not write; `idone[k]` marks the integrals of set k done
+    cudaStream_t istream = nullptr;
+    cudaEvent_t iready = nullptr;
+    cudaEvent_t idone[2]{};
+    bool ipending[2]{};
     bool timed = false;
     std::string err;
 };
@@ -191,6 +198,18 @@ int fail(epp_ctx* c, int code, const char* fmt, ...) {
 
 #define CK_LAUNCH() CK(cudaGetLastError())
 
+// Makes the context's stream wait for integrals still running beside it on set k (both sets when
+// k < 0).  Every entry point that may overwrite a state set, or run the integrals' reduction
+// itself, calls it before enqueueing work.
+int join_integrals(epp_ctx* ctx, int k = -1) {
+    for (int s = 0; s < 2; ++s)
+        if (ctx->ipending[s] && (k < 0 || k == s)) {
+            CK(cudaStreamWaitEvent(ctx->stream, ctx->idone[s], 0));
+            ctx->ipending[s] = false;
+        }
+    return EPP_OK;
+}
+
 size_t state_bytes(int cap) {
     // xh, vm, dv, comp, rp4 (float4) + rho, drho, vol, p, tagm, id, cell (4 B), aligned
     return (size_t)cap * (5 * 16 + 7 * 4) + 12 * 256;
@@ -205,7 +224,7 @@ size_t arena_bytes(int cap, int n_cells, int D, int n_tiles) {
     b += (size_t)(n_tiles + 1) * 8 + 256;                // scan state
     b += 2 * ((size_t)(n_cells + 1) * 4 + 256 + 256);    // occ[2], meta[2]
     b += 256 * 3;                                        // status, pairs
-    b += (size_t)cap * 4 + 256;                          // ncount
+    b += 2 * ((size_t)cap * 4 + 256);                    // nCount of each set
     b += (size_t)cap * 4 * (3 * D + 6) + 256;            // stage_f
     b += (size_t)cap * 4 * SI_COUNT + 256;               // stage_i
     b += (size_t)kIntegralBlocks * 8 * 8 + 8 * 8 + 4 * 256;
@@ -393,11 +412,11 @@ int launch_win_build(epp_ctx* ctx, int set, int crit, const Act& act, unsigned l
 template <int D>
 int launch_build(epp_ctx* ctx, int set, int crit, unsigned long long* pairs) {
     if constexpr (D == 2) {
-        if (uses_windows(ctx)) return launch_win_build(ctx, set, crit, CPCount<2>{ctx->ncount}, pairs);
+        if (uses_windows(ctx)) return launch_win_build(ctx, set, crit, CPCount<2>{ctx->ncnt[set]}, pairs);
     }
     PairArgs A = pair_args(ctx, set, crit);
     TileMask M{ctx->cap, ctx->nlist};
-    k_build<D><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(A, M, ctx->ncount, pairs);
+    k_build<D><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(A, M, ctx->ncnt[set], pairs);
     CK_LAUNCH();
     return EPP_OK;
 }
@@ -408,7 +427,7 @@ int launch_list(epp_ctx* ctx, int set, int crit, const Act& act) {
     PairArgs A = pair_args(ctx, set, crit);
     TileMask M{ctx->cap, ctx->nlist};
     k_list<D, Act, EPI><<<blocks_for(ctx->n, ctx->pass_threads), ctx->pass_threads, 0, ctx->stream>>>(
-        A, M, ctx->ncount, act, ctx->scan_state, ctx->n_tiles + 1);
+        A, M, ctx->ncnt[set], act, ctx->scan_state, ctx->n_tiles + 1);
     CK_LAUNCH();
     return EPP_OK;
 }
@@ -556,10 +575,10 @@ int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_ph
         // the emitted list keeps the reference's neighbour order: one thread per particle
         const int grid = blocks_for(ctx->n);
         if (cont) {
-            ActSearch<D, true, true, false> act{ctx->S[set], ctx->L, P, ctx->ncount, ctx->status};
+            ActSearch<D, true, true, false> act{ctx->S[set], ctx->L, P, ctx->ncnt[set], ctx->status};
             k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, ctx->pairs);
         } else {
-            ActSearch<D, true, false, false> act{ctx->S[set], ctx->L, P, ctx->ncount, ctx->status};
+            ActSearch<D, true, false, false> act{ctx->S[set], ctx->L, P, ctx->ncnt[set], ctx->status};
             k_pair<D><<<grid, kThreads, 0, ctx->stream>>>(A, act, ctx->pairs);
         }
         CK_LAUNCH();
@@ -570,34 +589,34 @@ int launch_search_pass(epp_ctx* ctx, int set, int crit, int action, const epp_ph
         int rc;
         auto cont_pass = [&](auto G) {
             constexpr bool GG = decltype(G)::value;
-            if (fused) return launch_pass<D, true>(ctx, set, crit, CPCont<D, true, GG>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
-            return launch_pass<D, true>(ctx, set, crit, CPCont<D, false, GG>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+            if (fused) return launch_pass<D, true>(ctx, set, crit, CPCont<D, true, GG>{ctx->S[set], P, ctx->ncnt[set]}, ctx->pairs);
+            return launch_pass<D, true>(ctx, set, crit, CPCont<D, false, GG>{ctx->S[set], P, ctx->ncnt[set]}, ctx->pairs);
         };
         if (fused || cont) rc = gen ? cont_pass(std::true_type{}) : cont_pass(std::false_type{});
-        else rc = launch_pass<D, true>(ctx, set, crit, CPCount<D>{ctx->ncount}, ctx->pairs);
+        else rc = launch_pass<D, true>(ctx, set, crit, CPCount<D>{ctx->ncnt[set]}, ctx->pairs);
         ctx->nlist_valid = rc == EPP_OK;
         return rc;
     }
     ctx->nlist_valid = false;
     if (ctx->lanes >= 2) {   // lane-group kernels (tuning alternative)
         if (fused) {
-            ActContG<D, true, true> act{ctx->S[set], P, ctx->ncount};
+            ActContG<D, true, true> act{ctx->S[set], P, ctx->ncnt[set]};
             return launch_pair_g<D, decltype(act), false>(ctx, A, act, ctx->pairs, ctx->n);
         }
         if (cont) {
-            ActContG<D, true, false> act{ctx->S[set], P, ctx->ncount};
+            ActContG<D, true, false> act{ctx->S[set], P, ctx->ncnt[set]};
             return launch_pair_g<D, decltype(act), false>(ctx, A, act, ctx->pairs, ctx->n);
         }
-        ActContG<D, false, false> act{ctx->S[set], P, ctx->ncount};
+        ActContG<D, false, false> act{ctx->S[set], P, ctx->ncnt[set]};
         return launch_pair_g<D, decltype(act), false>(ctx, A, act, ctx->pairs, ctx->n);
     }
     if (gen) {
-        if (fused) return launch_cellpair<D>(ctx, set, crit, CPCont<D, true, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
-        if (cont) return launch_cellpair<D>(ctx, set, crit, CPCont<D, false, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
+        if (fused) return launch_cellpair<D>(ctx, set, crit, CPCont<D, true, true>{ctx->S[set], P, ctx->ncnt[set]}, ctx->pairs);
+        if (cont) return launch_cellpair<D>(ctx, set, crit, CPCont<D, false, true>{ctx->S[set], P, ctx->ncnt[set]}, ctx->pairs);
     }
-    if (fused) return launch_cellpair<D>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
-    if (cont) return launch_cellpair<D>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncount}, ctx->pairs);
-    return launch_cellpair<D>(ctx, set, crit, CPCount<D>{ctx->ncount}, ctx->pairs);
+    if (fused) return launch_cellpair<D>(ctx, set, crit, CPCont<D, true>{ctx->S[set], P, ctx->ncnt[set]}, ctx->pairs);
+    if (cont) return launch_cellpair<D>(ctx, set, crit, CPCont<D, false>{ctx->S[set], P, ctx->ncnt[set]}, ctx->pairs);
+    return launch_cellpair<D>(ctx, set, crit, CPCount<D>{ctx->ncnt[set]}, ctx->pairs);
 }
 
 template <int D>
@@ -687,9 +706,9 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
     EPP_MARK(4);
     int rc;
     if (ctx->lanes == 0 && uses_windows(ctx)) {   // 2D windows: one search pass with the continuity action
-        rc = gen ? launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], Pn, ctx->ncount},
+        rc = gen ? launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], Pn, ctx->ncnt[to]},
                                         ctx->pairs)
-                 : launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], Pn, ctx->ncount},
+                 : launch_pass<D, true>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], Pn, ctx->ncnt[to]},
                                         ctx->pairs);
         if (rc) return rc;
         EPP_MARK(5);
@@ -697,8 +716,8 @@ int enqueue_fused_step(epp_ctx* ctx, int c, const epp_physics& phys, cudaEvent_t
         rc = launch_build<D>(ctx, to, EPP_CRITERION_SYMMETRY, ctx->pairs);
         if (rc) return rc;
         EPP_MARK(5);
-        rc = gen ? launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], Pn, ctx->ncount})
-                 : launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], Pn, ctx->ncount});
+        rc = gen ? launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true, true>{ctx->S[to], Pn, ctx->ncnt[to]})
+                 : launch_list<D>(ctx, to, EPP_CRITERION_SYMMETRY, CPCont<D, true>{ctx->S[to], Pn, ctx->ncnt[to]});
         if (rc) return rc;
     } else {
         rc = launch_search_pass<D>(ctx, to, EPP_CRITERION_SYMMETRY, EPP_ACTION_DAMBREAK_CONTINUITY, &phys, false,
@@ -863,6 +882,7 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     if (cfl) ensure_cfl_tables(ctx, phys);
     if (ctx->dv_dirty) {
         // the first step goes through the per-call kernels, which honour a non-zero dVelocity
+        if ((rc = join_integrals(ctx))) return rc;
         rc = run_selfaction<D>(ctx, EPP_ACTION_DAMBREAK_DENSITY, &phys);
         if (!rc && phys.wall_pressure == EPP_WALL_PRESSURE_EXTRAPOLATE) {
             rc = run_interaction<D>(ctx, EPP_ACTION_EXTRAPOLATE_PRESSURE, &phys);
@@ -908,6 +928,7 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
         ctx->rpn_walls = false;
     }
     if (ctx->last_crit != EPP_CRITERION_SYMMETRY) ctx->nlist_valid = false;
+    if (ctx->lanes == 0 && !ctx->nlist_valid && (rc = join_integrals(ctx, ctx->cur))) return rc;   // rewrites nCount
     rc = ensure_nlist<D>(ctx);
     if (rc) return rc;
     if (extrap && !ctx->rpn_walls) {   // the first step's wall pressure (later steps: the graph's tail)
@@ -923,6 +944,8 @@ int run_step(epp_ctx* ctx, int n_steps, const epp_physics& phys, bool accel) {
     for (int s = 0; s < n_steps; ++s) {
         ++ctx->step_count;
         const bool f = phys.filter_interval > 0 && ctx->step_count % phys.filter_interval == 0;
+        // a step reads set cur and writes set 1 - cur: integrals still reading set cur run on
+        if ((rc = join_integrals(ctx, 1 - ctx->cur))) return rc;
         CK(cudaGraphLaunch(f ? ctx->graph_f[ctx->cur] : ctx->graph[ctx->cur], ctx->stream));
         ctx->cur = 1 - ctx->cur;
     }
@@ -1062,7 +1085,8 @@ int32_t epp_create(const epp_config* cfg, epp_ctx** out) {
     ctx->scan_state = a.take<unsigned long long>(ctx->n_tiles + 1);
     ctx->status = a.take<unsigned>(1);
     ctx->pairs = a.take<unsigned long long>(1);
-    ctx->ncount = a.take<int>(ctx->cap);
+    ctx->ncnt[0] = a.take<int>(ctx->cap);
+    ctx->ncnt[1] = a.take<int>(ctx->cap);
     ctx->stage_f = a.take<float>((size_t)ctx->cap * (3 * D + 6));
     ctx->stage_i = a.take<int>((size_t)ctx->cap * SI_COUNT);
     ctx->ipartial = a.take<double>(kIntegralBlocks * 8);
@@ -1121,6 +1145,7 @@ int32_t epp_destroy(epp_ctx* ctx) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->istream) cudaStreamSynchronize(ctx->istream);
     ctx->stream = ctx->own_stream;   // the frees below are ordered on the context's own stream
     drop_graphs(ctx);
     dev_free(ctx, ctx->accel);
@@ -1140,6 +1165,10 @@ int32_t epp_destroy(epp_ctx* ctx) {
     for (int k = 0; k < EPP_INTEGRALS_SLOTS; ++k)
         if (ctx->iev[k]) cudaEventDestroy(ctx->iev[k]);
     if (ctx->ihost) cudaFreeHost(ctx->ihost);
+    if (ctx->iready) cudaEventDestroy(ctx->iready);
+    for (int k = 0; k < 2; ++k)
+        if (ctx->idone[k]) cudaEventDestroy(ctx->idone[k]);
+    if (ctx->istream) cudaStreamDestroy(ctx->istream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return EPP_OK;
@@ -1155,6 +1184,7 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
         return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "Tag and PositionVec columns are required");
     if (ldi < n || ldf < n) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "leading dimension < n");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     const int D = ctx->D;
     const bool same_n = n == ctx->n;
     ctx->n = n;
@@ -1227,7 +1257,7 @@ int32_t epp_upload(epp_ctx* ctx, int32_t n, const int32_t* is_alive, const int32
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;
         k_unpack<DD><<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->stage_f, ctx->stage_i,
-                                                                  ctx->S[0], ctx->ncount);
+                                                                  ctx->S[0], ctx->ncnt[0]);
     };
     if (D == 2) launch(std::integral_constant<int, 2>{});
     else launch(std::integral_constant<int, 3>{});
@@ -1263,13 +1293,14 @@ int32_t epp_download(epp_ctx* ctx, int32_t* is_alive, int32_t* cell_index, int32
                      float* fp, int64_t ldf, const epp_column_map* m) {
     if (!ctx || !m) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     const int D = ctx->D, n = ctx->n;
     if (n == 0) return EPP_OK;
     if ((ip && ldi < n) || (fp && ldf < n)) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "leading dimension < n");
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;
         k_pack<DD><<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->n_cells, ctx->stage_f, ctx->stage_i,
-                                                                ctx->S[ctx->cur], ctx->ncount);
+                                                                ctx->S[ctx->cur], ctx->ncnt[ctx->cur]);
     };
     if (D == 2) launch(std::integral_constant<int, 2>{});
     else launch(std::integral_constant<int, 3>{});
@@ -1319,7 +1350,7 @@ int32_t epp_download(epp_ctx* ctx, int32_t* is_alive, int32_t* cell_index, int32
         auto launch2 = [&](auto Dt) {
             constexpr int DD = decltype(Dt)::value;
             k_pack_lists<DD><<<blocks_for(n), kThreads, 0, ctx->stream>>>(n, ctx->L, ctx->S[ctx->cur].id,
-                                                                          ctx->ncount, nidx, nrvec, nr, nw, ndw, nh);
+                                                                          ctx->ncnt[ctx->cur], nidx, nrvec, nr, nw, ndw, nh);
         };
         if (D == 2) launch2(std::integral_constant<int, 2>{});
         else launch2(std::integral_constant<int, 3>{});
@@ -1358,6 +1389,7 @@ int32_t epp_search(epp_ctx* ctx, int32_t criterion, int32_t action, const epp_ph
     if (ctx->extrap_pending)
         return fail(ctx, EPP_ERR_STATE, "extrapolation sums pending: selfaction!(EXTRAPOLATE_PRESSURE_SELF) first");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     if (ctx->n == 0) return EPP_OK;
     const bool emit = (flags & EPP_SEARCH_EMIT_LIST) != 0;
     return ctx->D == 2 ? run_search<2>(ctx, criterion, action, phys, emit)
@@ -1376,6 +1408,7 @@ int32_t epp_interaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (!ctx->searched)
         return fail(ctx, EPP_ERR_STATE, "interaction! needs a search! at the current positions");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     if (ctx->n == 0) return EPP_OK;
     ctx->dv_dirty = true;
     return ctx->D == 2 ? run_interaction<2>(ctx, action, phys) : run_interaction<3>(ctx, action, phys);
@@ -1394,6 +1427,7 @@ int32_t epp_selfaction(epp_ctx* ctx, int32_t action, const epp_physics* phys) {
     if (!ctx->sorted_once)
         return fail(ctx, EPP_ERR_STATE, "selfaction! runs on the cell-sorted state: call search! first");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     if (ctx->n == 0) return EPP_OK;
     int rc = ctx->D == 2 ? run_selfaction<2>(ctx, action, phys) : run_selfaction<3>(ctx, action, phys);
     if (action == EPP_ACTION_DAMBREAK_INTEGRATE) {
@@ -1433,14 +1467,14 @@ int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys) {
 
 namespace {
 
-// k_integrals on the context's stream: the 8 results land in ctx->iresult.
-int launch_integrals(epp_ctx* ctx, const epp_physics* phys) {
+// k_integrals of the current set on stream `st`: the 8 results land in ctx->iresult.
+int launch_integrals(epp_ctx* ctx, const epp_physics* phys, cudaStream_t st) {
     IntegralsOut O{ctx->ipartial, ctx->iresult, ctx->iticket};
     DevPhys P = dev_phys(ctx, *phys);
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;
-        k_integrals<DD><<<kIntegralBlocks, 256, 0, ctx->stream>>>(
-            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], ctx->ncount, P, phys->rho0, phys->c0,
+        k_integrals<DD><<<kIntegralBlocks, 256, 0, st>>>(
+            ctx->start[ctx->cur], ctx->n_cells, ctx->n, ctx->S[ctx->cur], ctx->ncnt[ctx->cur], P, phys->rho0, phys->c0,
             phys->gamma, phys->p0,
             phys->gravity[0], phys->gravity[1], phys->gravity[2], O);
     };
@@ -1467,10 +1501,11 @@ void fill_integrals(epp_integrals* out, const double* r, int n_alive, float c0, 
 int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out) {
     if (!ctx || !phys || !out) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     std::memset(out, 0, sizeof *out);
     if (ctx->n == 0) return EPP_OK;
     if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
-    if (const int rc = launch_integrals(ctx, phys)) return rc;
+    if (const int rc = launch_integrals(ctx, phys, ctx->stream)) return rc;
     double r[8];
     int n_alive = 0;
     CK(cudaMemcpyAsync(r, ctx->iresult, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1489,21 +1524,33 @@ int32_t epp_integrals_async(epp_ctx* ctx, const epp_physics* phys, int64_t* tick
     const int slot = (int)(t % EPP_INTEGRALS_SLOTS);
     if (ctx->islot_ticket[slot] >= 0)
         return fail(ctx, EPP_ERR_STATE, "%d integrals tickets outstanding: wait for one first", EPP_INTEGRALS_SLOTS);
-    if (!ctx->ihost) {   // pinned slots on first use (the copies below then run asynchronously)
+    if (!ctx->ihost) {   // pinned slots, the second stream and its events on first use
         CK(cudaMallocHost(reinterpret_cast<void**>(&ctx->ihost), sizeof(double) * 9 * EPP_INTEGRALS_SLOTS));
         for (int k = 0; k < EPP_INTEGRALS_SLOTS; ++k) CK(cudaEventCreateWithFlags(&ctx->iev[k], cudaEventDisableTiming));
+        int prio = 0;
+        CK(cudaStreamGetPriority(ctx->stream, &prio));
+        CK(cudaStreamCreateWithPriority(&ctx->istream, cudaStreamNonBlocking, prio));
+        CK(cudaEventCreateWithFlags(&ctx->iready, cudaEventDisableTiming));
+        for (int k = 0; k < 2; ++k) CK(cudaEventCreateWithFlags(&ctx->idone[k], cudaEventDisableTiming));
     }
     double* h = ctx->ihost + 9 * slot;
+    // the second stream starts once the state is complete on the context's stream, and the next
+    // epp_step runs meanwhile (it reads this set and writes the other)
+    dev_phys(ctx, *phys);   // any table upload it needs goes first, on the context's stream
+    CK(cudaEventRecord(ctx->iready, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->istream, ctx->iready, 0));
     if (ctx->n == 0) {
         for (int k = 0; k < 9; ++k) h[k] = 0.0;
         h[6] = 1e300;
     } else {
-        if (const int rc = launch_integrals(ctx, phys)) return rc;
-        CK(cudaMemcpyAsync(h, ctx->iresult, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        if (const int rc = launch_integrals(ctx, phys, ctx->istream)) return rc;
+        CK(cudaMemcpyAsync(h, ctx->iresult, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->istream));
         CK(cudaMemcpyAsync(h + 8, ctx->start[ctx->cur] + ctx->n_cells, sizeof(int), cudaMemcpyDeviceToHost,
-                           ctx->stream));
+                           ctx->istream));
+        CK(cudaEventRecord(ctx->idone[ctx->cur], ctx->istream));
+        ctx->ipending[ctx->cur] = true;
     }
-    CK(cudaEventRecord(ctx->iev[slot], ctx->stream));
+    CK(cudaEventRecord(ctx->iev[slot], ctx->istream));
     ctx->islot_ticket[slot] = t;
     ctx->islot_c0[slot] = phys->c0;
     ctx->islot_cfl[slot] = phys->cfl;
@@ -1534,6 +1581,7 @@ int32_t epp_cell_stats(epp_ctx* ctx, int32_t* counts, int32_t* offsets, int32_t*
     if (!counts && !offsets && !sorted_ids) return EPP_OK;
     if (!ctx->searched) return fail(ctx, EPP_ERR_STATE, "no cell list: call search! first");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     std::vector<int> st(ctx->n_cells + 2);
     CK(cudaMemcpyAsync(st.data(), ctx->start[ctx->cur], sizeof(int) * (ctx->n_cells + 1), cudaMemcpyDeviceToHost,
                        ctx->stream));
@@ -1556,6 +1604,7 @@ int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t
     if (ctx->lanes != 0 || !ctx->nlist_valid)
         return fail(ctx, EPP_ERR_STATE, "no neighbour lists of the search pass (family 0, after a search or step)");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     const int n = ctx->n;
     if (n == 0) return EPP_OK;
     const int lcap = ctx->D == 2 ? ListConf<2>::LCAP : ListConf<3>::LCAP;
@@ -1569,7 +1618,7 @@ int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t
     std::vector<int> list((size_t)lcap * ctx->cap);
     if (n_alive > 0) {
         CK(cudaMemcpyAsync(id.data(), ctx->S[ctx->cur].id, sizeof(int) * n_alive, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(cnt.data(), ctx->ncount, sizeof(int) * n_alive, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(cnt.data(), ctx->ncnt[ctx->cur], sizeof(int) * n_alive, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaMemcpyAsync(list.data(), ctx->nlist, sizeof(int) * list.size(), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     }
@@ -1594,6 +1643,7 @@ int32_t epp_neighbour_lists(epp_ctx* ctx, int32_t* counts, int32_t* ids, int64_t
 int32_t epp_synchronize(epp_ctx* ctx, uint32_t* device_status) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     CK(cudaStreamSynchronize(ctx->stream));
     unsigned st = 0;
     CK(cudaMemcpy(&st, ctx->status, sizeof st, cudaMemcpyDeviceToHost));
@@ -1609,6 +1659,7 @@ int32_t epp_step_dt(epp_ctx* ctx, const epp_physics* phys, int32_t n, float* nex
     if (n != ctx->n_inst) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "n = %d, context has %d instances", n, ctx->n_inst);
     if (const int prc = check_physics(ctx, phys)) return prc;
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     if (next_dt) {
         if (phys->cfl > 0.0f && ctx->n > 0) {
             if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "the CFL time step needs a search! first");
@@ -1669,11 +1720,12 @@ int32_t epp_get_instance_integrals(epp_ctx* ctx, const epp_physics* phys, epp_in
     if (n != ctx->n_inst) return fail(ctx, EPP_ERR_INVALID_ARGUMENT, "n = %d, context has %d instances", n, ctx->n_inst);
     if (!ctx->sorted_once) return fail(ctx, EPP_ERR_STATE, "integrals need a search! first");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     DevPhys P = dev_phys(ctx, *phys);
     auto launch = [&](auto Dt) {
         constexpr int DD = decltype(Dt)::value;
         k_integrals_inst<DD><<<ctx->n_inst, 256, 0, ctx->stream>>>(
-            ctx->start[ctx->cur], ctx->dom, ctx->n, ctx->S[ctx->cur], ctx->ncount, P, phys->rho0, phys->gamma,
+            ctx->start[ctx->cur], ctx->dom, ctx->n, ctx->S[ctx->cur], ctx->ncnt[ctx->cur], P, phys->rho0, phys->gamma,
             phys->p0, phys->gravity[0], phys->gravity[1], phys->gravity[2], ctx->inst_out);
     };
     if (ctx->D == 2) launch(std::integral_constant<int, 2>{});
@@ -1753,7 +1805,8 @@ int32_t epp_context_bytes(const epp_config* cfg, int64_t* bytes) {
 
 int32_t epp_query(epp_ctx* ctx, int32_t* done) {
     if (!ctx || !done) return EPP_ERR_INVALID_ARGUMENT;
-    const cudaError_t e = cudaStreamQuery(ctx->stream);
+    cudaError_t e = cudaStreamQuery(ctx->stream);
+    if (e == cudaSuccess && ctx->istream) e = cudaStreamQuery(ctx->istream);   // integrals beside the step
     if (e == cudaErrorNotReady) {
         *done = 0;
         return EPP_OK;
@@ -1766,6 +1819,7 @@ int32_t epp_query(epp_ctx* ctx, int32_t* done) {
 int32_t epp_set_priority(epp_ctx* ctx, int32_t priority, int32_t* applied) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     int lo = 0, hi = 0;   // numerically: hi (greatest priority) <= lo
     CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     const int p = priority < hi ? hi : priority > lo ? lo : priority;
@@ -1783,6 +1837,7 @@ int32_t epp_set_priority(epp_ctx* ctx, int32_t priority, int32_t* applied) {
 int32_t epp_set_stream(epp_ctx* ctx, void* stream) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
     return EPP_OK;
@@ -1792,6 +1847,7 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
     if (!ctx || !phys || !stage_ms) return EPP_ERR_INVALID_ARGUMENT;
     if (!ctx->searched) return fail(ctx, EPP_ERR_STATE, "epp_profile_step needs an initial search!");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     if (ctx->n == 0) return EPP_OK;
     if (ctx->dv_dirty) {
         int rc = epp_step(ctx, 1, phys);   // settles dVelocity through the per-call path
@@ -1836,6 +1892,7 @@ int32_t epp_profile_step(epp_ctx* ctx, const epp_physics* phys, float* stage_ms)
 int32_t epp_set_accel_output(epp_ctx* ctx, int32_t enable) {
     if (!ctx) return EPP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     if (enable && !ctx->accel) {
         CK(dev_alloc(ctx, &ctx->accel, sizeof(float4) * ctx->cap));
         CK(cudaMemsetAsync(ctx->accel, 0, sizeof(float4) * ctx->cap, ctx->stream));
@@ -1851,6 +1908,7 @@ int32_t epp_get_accel(epp_ctx* ctx, float* out, int32_t n) {
     if (!ctx || !out || n != ctx->n) return EPP_ERR_INVALID_ARGUMENT;
     if (!ctx->accel) return fail(ctx, EPP_ERR_STATE, "accel output disabled");
     cudaSetDevice(ctx->dev);
+    if (const int rc_ = join_integrals(ctx)) return rc_;
     // accel is indexed by the order before the last gather; the permutation is cs/perm.  Copy
     // with the id array of that order (the other ping-pong set).
     std::vector<float4> a(ctx->n);

@@ -237,10 +237,11 @@ int32_t epp_step(epp_ctx* ctx, int32_t n_steps, const epp_physics* phys);
 int32_t epp_get_integrals(epp_ctx* ctx, const epp_physics* phys, epp_integrals* out);
 
 /* The same reductions without blocking: epp_integrals_async enqueues them for the current state
- * on the context's stream (their copy to the host included) and returns a ticket;
- * epp_integrals_wait(ticket) waits for that point of the stream and fills `out`.  Work queued in
- * between (the next epp_step) runs meanwhile.  At most EPP_INTEGRALS_SLOTS tickets may be
- * outstanding (EPP_ERR_STATE beyond). */
+ * (their copy to the host included) on a second stream of the context, once the work queued
+ * before has finished, and returns a ticket; epp_integrals_wait(ticket) waits for them and fills
+ * `out`.  The next epp_step runs beside them (it reads the state they reduce and writes the
+ * other buffer set); any other call that could change that state waits for them first.  At most
+ * EPP_INTEGRALS_SLOTS tickets may be outstanding (EPP_ERR_STATE beyond). */
 #define EPP_INTEGRALS_SLOTS 4
 int32_t epp_integrals_async(epp_ctx* ctx, const epp_physics* phys, int64_t* ticket);
 int32_t epp_integrals_wait(epp_ctx* ctx, int64_t ticket, epp_integrals* out);
