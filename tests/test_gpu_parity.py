@@ -356,6 +356,46 @@ def test_integrals_async_matches_blocking():
         d2.ctx.integrals_wait(t)
 
 
+def test_integrals_beside_steps_and_calls():
+    """The async integrals run on a second stream beside the following steps: with several tickets
+    outstanding and per-call work (a download, a self action, a blocking reduction) queued in
+    between, every ticket gives the values the blocking call gives at the same point, and the
+    trajectory is the one of a run that never asked for integrals."""
+    case = make_case(2, 0.04)
+    phys = case.physics
+    sym, cont = abi.EPP_CRITERION_SYMMETRY, abi.EPP_ACTION_DAMBREAK_CONTINUITY
+    a, _ = pair(case, 40)
+    a.ctx.search(sym, cont, phys, 0)
+    b, _ = pair(make_case(2, 0.04), 40)
+    b.ctx.search(sym, cont, phys, 0)
+    c, _ = pair(make_case(2, 0.04), 40)
+    c.ctx.search(sym, cont, phys, 0)
+    expect, tickets = [], []
+    for k in range(12):
+        a.ctx.step(1, phys)
+        expect.append(a.ctx.integrals(phys))
+        b.ctx.step(1, phys)
+        tickets.append(b.ctx.integrals_async(phys))
+        c.ctx.step(1, phys)
+        if k == 5:   # calls that must wait for the integrals still running on the other stream
+            b.asyncto()
+            assert b.ctx.integrals(phys) == expect[-1]
+        if len(tickets) == abi.EPP_INTEGRALS_SLOTS:
+            got = [b.ctx.integrals_wait(t) for t in tickets]
+            assert got == expect[len(expect) - len(got):]
+            tickets = []
+    got = [b.ctx.integrals_wait(t) for t in tickets]
+    assert got == expect[len(expect) - len(got):]
+    a.asyncto()
+    b.asyncto()
+    c.asyncto()
+    for k in ("PositionVec", "VelocityVec", "Density", "nCount"):
+        assert np.array_equal(a.host[k], b.host[k]), k
+        assert np.array_equal(a.host[k], c.host[k]), k
+    for d in (a, b, c):
+        d.close()
+
+
 def test_out_of_domain_killed():
     """NeighbourSearch.jl:41-43: particles outside the domain are killed (is_alive = 0, cell 0)."""
     case = make_case(2, 0.04)
