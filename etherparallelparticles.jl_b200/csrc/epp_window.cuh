@@ -28,10 +28,11 @@ struct RowWin {
     int lo, hi;   // candidate range [lo, hi) in cell order
 };
 
-// Linear cell row of stencil row r (0, 1, 2 for dy = -1, 0, +1) of the cell row `rid` (y + n1 k;
-// k is the instance of a batch), or -1 when y + dy is outside the grid.
-__device__ __forceinline__ int stencil_row2(const PairArgs& A, int rid, int r) {
-    const int yy = rid % A.dom.n[1] + r - 1;
+// Linear cell row of stencil row r (0, 1, 2 for dy = -1, 0, +1) of the cell row `rid` = y + n1 k
+// (k is the instance of a batch; the caller passes y = rid mod n1), or -1 when y + dy is outside
+// the grid.
+__device__ __forceinline__ int stencil_row2(const PairArgs& A, int rid, int y, int r) {
+    const int yy = y + r - 1;
     return (yy >= 0 && yy < A.dom.n[1]) ? rid + r - 1 : -1;
 }
 
@@ -156,7 +157,7 @@ __device__ __forceinline__ WinOut win_lane_general(const PairArgs& A, const Tile
     WinOut o{0, 0.0f, 0.0f, 0u};
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-        const RowWin win = row_range(A, stencil_row2(A, rid, r), cx - 1, cx + 1);
+        const RowWin win = row_range(A, stencil_row2(A, rid, rid % A.dom.n[1], r), cx - 1, cx + 1);
         const RowWin u = r == 0 ? u0 : (r == 1 ? u1 : u2);
         const unsigned long long allowed = r == 0 ? al0 : (r == 1 ? al1 : al2);
         const int len = win.hi - win.lo;
@@ -233,6 +234,7 @@ __global__ void __launch_bounds__(128, 7) k_win_build(const __grid_constant__ Pa
         const int c = A.s.cell[min(i, n_alive - 1)];
         EPP_CHECK(!__any_sync(0xffffffffu, c < 0 || c >= A.dom.n_cells), 34, c);
         const int rid = c / n0, cx = c - rid * n0;
+        const int y = rid % A.dom.n[1];
         const float4 xi = on ? A.s.xh[i] : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         const int ti = on ? tag_of(A.s.tagm[i]) : 0;
         const bool valid = on && ti >= 1 && ti <= A.n_tags;
@@ -247,6 +249,7 @@ __global__ void __launch_bounds__(128, 7) k_win_build(const __grid_constant__ Pa
         while (pending) {   // warp-uniform
             const int lead = __ffs(pending) - 1;
             const int rid_g = __shfl_sync(0xffffffffu, rid, lead);
+            const int y_g = __shfl_sync(0xffffffffu, y, lead);
             const bool mine = ((pending >> lane) & 1u) && rid == rid_g;
             const unsigned members = __ballot_sync(0xffffffffu, mine);
             const int xa = __shfl_sync(0xffffffffu, cx, lead) - 1;
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(128, 7) k_win_build(const __grid_constant__ Pa
             bool staged = true;
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
-                u[r] = row_range(A, stencil_row2(A, rid_g, r), xa, xb);
+                u[r] = row_range(A, stencil_row2(A, rid_g, y_g, r), xa, xb);
                 staged = staged && u[r].hi - u[r].lo <= 64;   // warp-uniform
             }
             unsigned long long allowed[3] = {0ull, 0ull, 0ull};
@@ -267,7 +270,7 @@ __global__ void __launch_bounds__(128, 7) k_win_build(const __grid_constant__ Pa
             const bool dflt = A.crit == EPP_CRITERION_DEFAULT;
             RowWin win[3];
 #pragma unroll
-            for (int r = 0; r < 3; ++r) win[r] = row_range(A, stencil_row2(A, rid, r), cx - 1, cx + 1);
+            for (int r = 0; r < 3; ++r) win[r] = row_range(A, stencil_row2(A, rid, y, r), cx - 1, cx + 1);
             unsigned uniform_rows = 0u;
 #pragma unroll
             for (int r = 0; r < 3; ++r)
