@@ -11,13 +11,14 @@
 // union of their windows in a stencil row is one contiguous range; the warp stages the three union
 // rows (up to 64 candidates each) in shared memory in one round -- position and h, the list entry
 // (index and tag) in the unused z lane, and the search action's neighbour record -- and every lane
-// reads its own window from there.  For each 32-candidate chunk of a window the lane builds one
-// acceptance word with the reference's IEEE criterion (and the active-pair matrix, applied from
-// per-row tag bitmaps), then walks its set bits in ascending order: it appends the neighbour to its
-// list (the lists the momentum, filter and extrapolation passes read; same layout and order as
+// reads its own window from there.  The lane builds one acceptance word per stencil row with the
+// reference's IEEE criterion (and the active-pair matrix, applied from per-row tag bitmaps), then
+// walks the set bits of the three words in list order, in one loop: it appends the neighbour to
+// its list (the lists the momentum, filter and extrapolation passes read; same layout and order as
 // k_build's: stencil rows, then cell order, then id order inside a cell) and adds the search
 // action's term -- the continuity rate -- from the staged record, so no separate continuity pass
-// walks the neighbours again.  A warp that crosses a cell-row end takes one such round per cell
+// walks the neighbours again.  Windows beyond 32 candidates (dense neighbourhoods) go row by row
+// in 32-candidate chunks.  A warp that crosses a cell-row end takes one such round per cell
 // row of its particles; union rows longer than 64 are read from global memory instead.
 #pragma once
 #include "epp_tile.cuh"
