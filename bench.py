@@ -1147,7 +1147,7 @@ def compute_roof(tr_case, stage, fp32_peak, clk, kernel_of=None):
 
 
 def energy_drift_fp64(case, steps, device=0):
-    """North-star check on this workload: relative energy drift (kinetic + potential + internal,
+    """Energy check on this workload: relative energy drift (kinetic + potential + internal,
     FP64 integrals) over `steps` fused steps, the FP32 CUDA path against the FP64 oracle from the
     same initial state; the bar is |drift_gpu - drift_fp64| <= 1e-4."""
     from epp import abi, casegen
