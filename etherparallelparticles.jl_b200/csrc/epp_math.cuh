@@ -80,7 +80,7 @@ struct NeighbourList {   // EPP_SEARCH_EMIT_LIST output, column-major [k * cap +
 };
 
 // tagm = tag | movable << 8 | instance << 9
-// EPP_CHECKED builds: every index read from the cell offsets, lists and masks is checked before
+// EPP_CHECKED builds: every index read from the cell offsets and lists is checked before
 // the access; a bad one is recorded (site, index) in epp_check_slot and the access is skipped.
 #ifdef EPP_CHECKED
 __device__ int epp_check_slot[4];
