@@ -160,7 +160,8 @@ __device__ __forceinline__ ListWriter<D> list_writer(const TileMask& M, int i) {
 // Reads a particle's list in order, the next entries already in flight: 2D (column-major) one
 // entry at a time through next(), with streaming loads (each entry is read once: evicted first,
 // so the neighbour records the pass gathers keep the L1; momentum -1.7%); 3D (row-major) rows are
-// read four entries at a time by k_list from the two groups start() loads.
+// read four entries at a time by k_list from the two groups start() loads, as ordinary loads (a
+// row's next group shares its line: streaming loads there cost the 3D list passes 5-9%).
 template <int D>
 struct ListReader {
     const int* base;
